@@ -1,0 +1,409 @@
+#!/usr/bin/env python3
+"""Benchmark: AV1 post-filter chain (deblock -> CDEF -> loop restoration) on B200.
+
+Workload (the post-filter stage micro-benchmark configuration): a batch of 64
+frames of 1920x1080 8-bit 4:2:0 synthetic decoder state per GPU — planes from a
+bilinearly upsampled 16x16 uniform field plus uniform noise in [-12, 12],
+legal per-4x4 transform sizes, deblock levels 0..63 with sharpness 0..7,
+per-64x64 CDEF strengths (cdef_bits 3, damping 3..6) and 64x64 restoration
+units split Wiener / self-guided.  One step = the whole chain over the batch,
+one launch per stage across the 64 frames.  `--bit-depth 10` runs the 10-bit
+variant.
+
+Printed JSON (rank 0): `value` is whole-job frames/s with inputs resident in
+HBM; `e2e` is the same metric through the C-ABI with the inputs copied from
+pinned host memory and the restored frames copied back every step; `roofline`
+is the dominant kernel's algorithmic bytes per launch over its CUDA-event
+duration against the measured HBM copy bandwidth; `cpu_baseline` is the CPU
+oracle (a C restatement of the reference's CPU path) on a bounded sample.
+
+`--impl reference` times the reference's CPU implementation of the path (the
+same C restatement — the Rust crate does not build here) on all host cores.
+"""
+import argparse
+import concurrent.futures as cf
+import ctypes as C
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+PKG_DIR = ROOT / "oxideav-av1_b200"
+
+
+def load_package():
+    if "oxideav_av1_b200" in sys.modules:
+        return sys.modules["oxideav_av1_b200"]
+    spec = importlib.util.spec_from_file_location("oxideav_av1_b200", PKG_DIR / "__init__.py",
+                                                  submodule_search_locations=[str(PKG_DIR)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["oxideav_av1_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+load_package()
+sys.path.insert(0, str(ROOT))
+
+from oxideav_av1_b200 import abi, synth  # noqa: E402
+
+WIDTH, HEIGHT = 1920, 1080
+METRIC = "decoded frames/s"
+UNIT = "frames/s"
+
+
+def frame_seed(rank, i):
+    return 1_000_003 * (rank + 1) + i
+
+
+def make_frames(rank, n, bit_depth):
+    return [synth.make_frame(frame_seed(rank, i), WIDTH, HEIGHT, bit_depth=bit_depth) for i in range(n)]
+
+
+def algorithmic_bytes(frame):
+    """Per-frame algorithmic bytes of each stage (the path's roofline model).
+
+    S bytes/sample, P samples of the cropped frame, M mi cells, U LR units:
+      deblock  2*P*S + 10*M      (planes read+write; ~10 B of mi side data per 4x4)
+      cdef     2*P*S + M + 64*SB (planes read+write; skip flags; one index per 64x64)
+      lr       2*P*S + P*S/16 + 10*U (CDEF frame read, output write, 2+2 deblocked rows
+                                    per 64-row stripe, unit parameters)
+    """
+    h = frame.hdr
+    S = 2 if h.bit_depth > 8 else 1
+    P = sum(frame.out_dims(p)[0] * frame.out_dims(p)[1] for p in range(h.num_planes))
+    M = h.mi_rows * h.mi_cols
+    SB = ((h.mi_rows + 15) // 16) * ((h.mi_cols + 15) // 16)
+    U = sum(frame.lr_grid(p)[0] * frame.lr_grid(p)[1] for p in range(h.num_planes))
+    return {"deblock": 2 * P * S + 10 * M, "cdef": 2 * P * S + M + 64 * SB, "lr": 2 * P * S + P * S // 16 + 10 * U}
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def dram_traffic(kernel, workload):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, or None."""
+    p = ROOT / "profiles" / "dram_traffic.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 3 and not line.startswith("#") and parts[0] == kernel and parts[1] == workload:
+            return int(parts[2])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------
+# reference arm and CPU baseline: the C oracle on host cores
+# ----------------------------------------------------------------------------
+
+def cpu_time_frames(frames, threads):
+    import oracle
+    oracle.load()
+    t0 = time.perf_counter()
+    if threads == 1:
+        for f in frames:
+            oracle.postfilter_frame(f)
+    else:
+        with cf.ThreadPoolExecutor(threads) as ex:  # ctypes releases the GIL during the C call
+            list(ex.map(oracle.postfilter_frame, frames))
+    return time.perf_counter() - t0
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    frames = make_frames(0, threads, args.bit_depth)
+    for _ in range(args.warmup):
+        cpu_time_frames(frames[:threads], threads)
+    dt = 0.0
+    for _ in range(args.steps):
+        dt += cpu_time_frames(frames, threads)
+    value = len(frames) * args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8" if args.bit_depth == 8 else "u16",
+        "data": "synthetic",
+        "config": config_block(args, frames_per_step=len(frames)),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{len(frames)} frames of the workload per step, one frame per thread, "
+                                   "full deblock+CDEF+LR chain (C restatement of the reference CPU path)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def config_block(args, frames_per_step):
+    return {"workload": f"post-filter chain (deblock+CDEF+loop restoration), {frames_per_step} x "
+                        f"{WIDTH}x{HEIGHT} {args.bit_depth}-bit 4:2:0 frames per GPU per step",
+            "frames_per_step_per_gpu": frames_per_step, "resolution": f"{WIDTH}x{HEIGHT}",
+            "bit_depth": args.bit_depth, "chroma": "4:2:0", "stages": ["deblock", "cdef", "lr"],
+            "launch": "one launch per stage across the batch",
+            "parallelism": f"independent frame batches per GPU (replicas, no collective), {args.gpus} GPU(s)",
+            "l2": "inputs larger than L2 (each step reads ~200 MB of planes per GPU)"}
+
+
+# ----------------------------------------------------------------------------
+# GPU arm
+# ----------------------------------------------------------------------------
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+    from oxideav_av1_b200 import postfilter
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    abi.load()
+    frames = make_frames(rank, args.frames, args.bit_depth)
+    dframes = [postfilter.DeviceFrame(f, device=dev) for f in frames]
+    jobs = postfilter.jobs_array(dframes)
+    lib = abi.load()
+    stream = torch.cuda.Stream(device=dev)
+    sp = C.c_void_p(stream.cuda_stream)
+    n = len(dframes)
+    stages = [("deblock", lib.av1g_run_deblock), ("cdef", lib.av1g_run_cdef), ("lr", lib.av1g_run_lr)]
+
+    def step(events=None):
+        for i, (_, fn) in enumerate(stages):
+            abi.check(fn(jobs, n, sp))
+            if events is not None:
+                events[i].record(stream)
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 3)):
+            step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev_start = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev_stage = [[torch.cuda.Event(enable_timing=True) for _ in stages] for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                ev_start[k].record(stream)
+                step(ev_stage[k])
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    stage_ms = {name: 0.0 for name, _ in stages}
+    total_ms = 0.0
+    for k in range(args.steps):
+        prev = ev_start[k]
+        for i, (name, _) in enumerate(stages):
+            d = prev.elapsed_time(ev_stage[k][i])
+            stage_ms[name] += d
+            total_ms += d
+            prev = ev_stage[k][i]
+    t = torch.tensor([total_ms], device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * n / (ms_per_step / 1e3)
+
+    # plain one-frame-per-launch path (same kernels, a launch per stage per frame)
+    with torch.cuda.stream(stream):
+        postfilter.run_postfilter(dframes, mode=abi.MODE_PER_FRAME, stream=stream, jobs=jobs)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            postfilter.run_postfilter(dframes, mode=abi.MODE_PER_FRAME, stream=stream, jobs=jobs)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    per_frame_ms = e0.elapsed_time(e1) / args.steps
+
+    e2e = run_e2e(args, frames, dframes, jobs, stream, dev, world)
+
+    # roofline of the dominant kernel
+    ab = algorithmic_bytes(frames[0])
+    dom = max(stage_ms, key=stage_ms.get)
+    launch_ms = stage_ms[dom] / args.steps
+    achieved = ab[dom] * n / (launch_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    kernel_name = {"deblock": "deblock_kernel", "cdef": "cdef_kernel", "lr": "lr_kernel"}[dom]
+    workload = f"{WIDTH}x{HEIGHT}x{args.bit_depth}b"
+    traffic = dram_traffic(kernel_name, workload)
+    if traffic is not None:
+        traffic = traffic * n  # summary holds bytes per frame
+    stage_frac = {}
+    for name in stage_ms:
+        a = ab[name] * n / (stage_ms[name] / args.steps / 1e3) / 1e9
+        stage_frac[name] = {"ms_per_launch": stage_ms[name] / args.steps, "achieved_gbs": a, "frac": a / peak}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8" if args.bit_depth == 8 else "u16", "data": "synthetic",
+        "config": config_block(args, n),
+        "roofline": {"bound": "hbm", "kernel": kernel_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                     if peak_kind == "measured" else "fallback 6650 GB/s"},
+        "stages": stage_frac,
+        "per_frame_path": {"value": world * n / (per_frame_ms / 1e3), "unit": UNIT, "ms_per_step": per_frame_ms,
+                           "launches_per_step": None},
+        "e2e": e2e,
+        "gpu_launches": len(stages) * args.steps,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        k = args.cpu_sample
+        dt = cpu_time_frames(frames[:k], 1)
+        line["cpu_baseline"] = {"value": k / dt, "unit": UNIT, "cores": 1, "kind": "port",
+                                "sample": f"{k} of the {n} workload frames through the full chain, one thread"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def run_e2e(args, frames, dframes, jobs, stream, dev, world):
+    """Frames/s through the C-ABI with host buffers: inputs H2D from pinned memory
+    and the restored (cropped) planes D2H every step."""
+    import torch
+    from oxideav_av1_b200 import postfilter
+
+    lib = abi.load()
+    sp = C.c_void_p(stream.cuda_stream)
+    n = len(dframes)
+    # pinned host copies of every input the chain reads, and of every output
+    h_in, d_in, h_out, d_out = [], [], [], []
+    for f, d in zip(frames, dframes):
+        for p, pl in enumerate(d.recon):
+            h_in.append(pl.t.cpu().pin_memory())
+            d_in.append(pl.t)
+        for k in d.GRID_KEYS:
+            h_in.append(d.grid[k].cpu().pin_memory())
+            d_in.append(d.grid[k])
+        h_in.append(d.cdef_idx.cpu().pin_memory())
+        d_in.append(d.cdef_idx)
+        for u in d.lr_units:
+            if u is not None:
+                h_in.append(u.cpu().pin_memory())
+                d_in.append(u)
+        for p, pl in enumerate(d.stage_planes()["lr"]):
+            h_out.append(torch.empty_like(pl.t, device="cpu").pin_memory())
+            d_out.append(pl.t)
+    h2d = sum(t.numel() * t.element_size() for t in h_in)
+    d2h = sum(t.numel() * t.element_size() for t in h_out)
+
+    def step():
+        for h, d in zip(h_in, d_in):
+            d.copy_(h, non_blocking=True)
+        abi.check(lib.av1g_run_postfilter(jobs, n, abi.MODE_BATCHED, sp, None))
+        for h, d in zip(h_out, d_out):
+            h.copy_(d, non_blocking=True)
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 3)):
+            step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    t = torch.tensor([ms], device=dev)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    return {"value": world * n / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "ms_per_step": ms, "path": "av1g_run_postfilter with pinned-host inputs/outputs copied every step"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--frames", type=int, default=64)
+    ap.add_argument("--bit-depth", type=int, default=8, choices=[8, 10])
+    ap.add_argument("--cpu-sample", type=int, default=6)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

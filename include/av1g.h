@@ -1,0 +1,262 @@
+/*
+ * av1g.h — C ABI of the B200 AV1 reconstruction + post-filter engine.
+ *
+ * The engine replaces the pixel stages of the reference decoder's frame
+ * driver: everything in `decode_frame_spec_tiles` after the tile walk has
+ * parsed the symbols (src/decoder/frame_driver.rs:790-1116 — deblock, CDEF,
+ * superres, loop restoration, crop, pre-grain reference store, film grain,
+ * narrow) plus the per-TU dequant / inverse transform / reconstruction merge
+ * that the walker interleaves with parsing (src/cdf.rs:32482-32973).
+ *
+ * Conventions
+ *  - Plain C types only; no CUDA or torch types appear in signatures.  Where a
+ *    CUDA stream is accepted it is passed as `void*` (a cudaStream_t, NULL =
+ *    legacy default stream).
+ *  - Every entry point returns an av1g_status; nothing aborts the process.  A
+ *    malformed descriptor yields AV1G_EINVAL, mirroring the reference's
+ *    "typed error, never panic" contract (src/lib.rs:1937).
+ *  - Sample planes hold 8-bit content as uint8_t and 10/12-bit content as
+ *    uint16_t (little-endian), the same layout the reference surfaces
+ *    (frame_driver.rs:1101-1116).  Strides are in bytes.
+ *  - Per-mi grids are row-major MiRows x MiCols with stride MiCols, one entry
+ *    per 4x4 luma cell, as the tile walker stores them (cdf.rs:15391-15940).
+ */
+#ifndef AV1G_H
+#define AV1G_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AV1G_ABI_VERSION 1
+
+typedef enum av1g_status {
+    AV1G_OK = 0,
+    AV1G_EINVAL = 1,         /* malformed descriptor or argument            */
+    AV1G_ENOMEM_BUDGET = 2,  /* admission would exceed the engine HBM budget */
+    AV1G_EBUSY = 3,          /* no free slot; retry after a poll/fetch       */
+    AV1G_TIMEOUT = 4,        /* bounded wait expired                         */
+    AV1G_EDEVICE = 5,        /* CUDA error (launch, copy, allocation)        */
+    AV1G_EPARITY = 6,        /* debug self-check mismatch                    */
+    AV1G_ENOTSUP = 7,        /* feature not handled by this build            */
+    AV1G_ENOTREADY = 8       /* ticket not finished yet (non-blocking poll)  */
+} av1g_status;
+
+/* ---------------------------------------------------------------------
+ * Frame-level parameters (resolved header state)
+ * ------------------------------------------------------------------- */
+
+/* Film grain parameters after §5.9.30 resolution (the `update_grain == 0`
+ * predicted path already applied by the caller, frame_driver.rs:1060-1075).
+ * Field meaning follows FilmGrainParams (src/uncompressed_header_tail.rs:1763):
+ * grain_scaling is GrainScaling (8..11), ar_coeff_shift is ArCoeffShift
+ * (6..9). */
+typedef struct av1g_film_grain {
+    uint8_t apply_grain;
+    uint8_t chroma_scaling_from_luma;
+    uint16_t grain_seed;
+    uint8_t num_y_points;
+    uint8_t point_y_value[14];
+    uint8_t point_y_scaling[14];
+    uint8_t num_cb_points;
+    uint8_t point_cb_value[10];
+    uint8_t point_cb_scaling[10];
+    uint8_t num_cr_points;
+    uint8_t point_cr_value[10];
+    uint8_t point_cr_scaling[10];
+    uint8_t grain_scaling;
+    uint8_t ar_coeff_lag;
+    uint8_t ar_coeffs_y_plus_128[24];
+    uint8_t ar_coeffs_cb_plus_128[25];
+    uint8_t ar_coeffs_cr_plus_128[25];
+    uint8_t ar_coeff_shift;
+    uint8_t grain_scale_shift;
+    uint8_t cb_mult;
+    uint8_t cb_luma_mult;
+    uint8_t cr_mult;
+    uint8_t cr_luma_mult;
+    uint8_t overlap_flag;
+    uint8_t clip_to_restricted_range;
+    uint16_t cb_offset;
+    uint16_t cr_offset;
+} av1g_film_grain;
+
+/* Everything the post-filter chain reads from the sequence and frame
+ * headers.  Names follow the spec / reference structs:
+ *   sizes            — FrameSize (frame_header.rs), MiRows/MiCols
+ *   loop filter      — LoopFilterParams (uncompressed_header_tail.rs:261)
+ *   segmentation     — the SEG_LVL_ALT_LF_* features (1..4) of
+ *                      SegmentationParams (uncompressed_header_tail.rs:554)
+ *   cdef             — CdefParams (uncompressed_header_tail.rs:876); the
+ *                      secondary strengths are the adjusted {0,1,2,4} values
+ *   restoration      — LrParams (uncompressed_header_tail.rs:1079)
+ *   film grain       — av1g_film_grain above. */
+typedef struct av1g_frame_header {
+    int32_t frame_width;      /* FrameWidth (post superres downscale)      */
+    int32_t frame_height;     /* FrameHeight                               */
+    int32_t upscaled_width;   /* UpscaledWidth (== frame_width w/o superres) */
+    int32_t mi_rows;          /* MiRows                                    */
+    int32_t mi_cols;          /* MiCols                                    */
+    uint8_t bit_depth;        /* 8, 10 or 12                               */
+    uint8_t subsampling_x;
+    uint8_t subsampling_y;
+    uint8_t num_planes;       /* 1 (monochrome) or 3                       */
+    uint8_t matrix_coefficients;
+    uint8_t use_superres;
+    uint8_t coded_lossless;
+    uint8_t allow_intrabc;
+    uint8_t enable_cdef;      /* sequence header enable_cdef               */
+    /* §5.9.11 loop filter */
+    uint8_t lf_level[4];
+    uint8_t lf_sharpness;
+    uint8_t lf_delta_enabled;
+    uint8_t delta_lf_multi;
+    int8_t lf_ref_deltas[8];
+    int8_t lf_mode_deltas[2];
+    /* §5.9.14 segmentation, loop-filter features only: [segment][i] for
+     * feature SEG_LVL_ALT_LF_Y_V + i, i = 0..3 */
+    uint8_t seg_lf_active[8][4];
+    int16_t seg_lf_data[8][4];
+    /* §5.9.19 cdef */
+    uint8_t cdef_short_circuited;
+    uint8_t cdef_damping;
+    uint8_t cdef_bits;
+    uint8_t cdef_y_pri[8];
+    uint8_t cdef_y_sec[8];
+    uint8_t cdef_uv_pri[8];
+    uint8_t cdef_uv_sec[8];
+    /* §5.9.20 loop restoration: FrameRestorationType (0 none, 1 wiener,
+     * 2 sgrproj, 3 switchable) and LoopRestorationSize per plane */
+    uint8_t uses_lr;
+    uint8_t lr_type[3];
+    int32_t lr_unit_size[3];
+    av1g_film_grain film_grain;
+} av1g_frame_header;
+
+/* Per-unit loop-restoration parameters (LrUnit, src/cdf.rs:15225).
+ * type: 0 RESTORE_NONE, 1 RESTORE_WIENER, 2 RESTORE_SGRPROJ.
+ * wiener[pass][i]: pass 0 vertical, pass 1 horizontal coefficients. */
+typedef struct av1g_lr_unit {
+    uint8_t type;
+    uint8_t sgr_set;
+    int8_t wiener[2][3];
+    int16_t sgr_xqd[2];
+} av1g_lr_unit;
+
+/* Per-mi decode grids the post filters read (cdf.rs:15391-15940).  Each
+ * pointer addresses mi_rows * mi_cols entries (delta_lf: 4 per cell). */
+typedef struct av1g_mi_grid {
+    const uint8_t* mi_size;       /* MiSizes, BLOCK_* ordinal               */
+    const uint8_t* skip;          /* Skips                                  */
+    const uint8_t* is_inter;      /* IsInters                               */
+    const int8_t* ref_frame0;     /* RefFrames[.][.][0] (0 = INTRA_FRAME)   */
+    const uint8_t* y_mode;        /* YModes                                 */
+    const int8_t* segment_id;     /* SegmentIds (-1 = none)                 */
+    const int8_t* delta_lf;       /* DeltaLFs[.][.][0..3]                   */
+    const uint8_t* tx_size;       /* TxSizes (intra cells)                  */
+    const uint8_t* inter_tx_size; /* InterTxSizes (inter cells)             */
+} av1g_mi_grid;
+
+/* One sample plane.  data is a device pointer for the av1g_run_* entry
+ * points and a host pointer for av1g_submit_frame / av1g_fetch_output. */
+typedef struct av1g_plane {
+    void* data;
+    int32_t stride;   /* bytes between rows                               */
+    int32_t width;    /* samples                                          */
+    int32_t height;   /* rows                                             */
+} av1g_plane;
+
+/* A frame's post-filter work in device memory.  The chain reads `recon`
+ * (CurrFrame at the padded mi extent, (MiCols*4 >> ssx) x (MiRows*4 >> ssy))
+ * and writes the intermediate planes named below.  Stages that the header
+ * gates off (frame_driver.rs:832-836, 870, 906, 971, 1060) are skipped and the
+ * next stage reads the previous stage's buffer instead.
+ *   deblocked    — §7.14 output (padded extent)
+ *   cdef         — §7.15 output (padded extent)
+ *   up_deblocked — §7.16 upscale of `deblocked` (UpscaledWidth x FrameHeight)
+ *   up_cdef      — §7.16 upscale of `cdef`      (UpscaledWidth x FrameHeight)
+ *   lr           — §7.17 output; its crop to UpscaledWidth x FrameHeight is
+ *                  the §7.20 reference payload (pre grain)
+ *   out          — §7.18.3 film grain applied to the cropped frame
+ * Buffers a frame does not need may be left NULL. */
+typedef struct av1g_frame_job {
+    const av1g_frame_header* hdr;   /* host pointer                        */
+    av1g_mi_grid grid;              /* device pointers                     */
+    const int8_t* cdef_idx;         /* device; cdef_idx per 64x64 luma
+                                       block, ceil(MiRows/16) rows x
+                                       ceil(MiCols/16) cols, -1 = off      */
+    const av1g_lr_unit* lr_units[3]; /* device; unit_rows x unit_cols each  */
+    av1g_plane recon[3];
+    av1g_plane deblocked[3];
+    av1g_plane cdef[3];
+    av1g_plane up_deblocked[3];
+    av1g_plane up_cdef[3];
+    av1g_plane lr[3];
+    av1g_plane out[3];
+} av1g_frame_job;
+
+/* Launch modes for av1g_run_postfilter. */
+#define AV1G_MODE_BATCHED 0     /* one launch per stage across all jobs    */
+#define AV1G_MODE_PER_FRAME 1   /* one launch per stage per frame          */
+
+/* ---------------------------------------------------------------------
+ * Library
+ * ------------------------------------------------------------------- */
+
+/* ABI version of the loaded library (AV1G_ABI_VERSION at build time). */
+int32_t av1g_abi_version(void);
+
+/* sizeof() of a public struct by name ("av1g_frame_header", ...), or -1.
+ * Lets bindings in other languages verify their struct mirrors. */
+int32_t av1g_struct_size(const char* name);
+
+/* Human-readable text of the last error on this thread. */
+const char* av1g_last_error(void);
+
+/* Number of units an LR plane of `plane_size` samples holds at
+ * `unit_size` (§5.9.20 count_units_in_frame, loop_restoration.rs:888). */
+int32_t av1g_lr_units_in_frame(int32_t unit_size, int32_t plane_size);
+
+/* ---------------------------------------------------------------------
+ * Stage entry points on device-resident frames.  Each runs one stage for
+ * `n` jobs as one launch (or one launch per plane group) on `stream`.
+ * ------------------------------------------------------------------- */
+
+/* §7.14 deblock: recon -> deblocked.  Replaces loop_filter_frame
+ * (src/loop_filter.rs:271) as driven by loop_filter_frame_from_grid
+ * (src/cdf.rs:20449). */
+av1g_status av1g_run_deblock(const av1g_frame_job* jobs, int32_t n, void* stream);
+
+/* §7.15 CDEF: deblocked -> cdef.  Replaces cdef_frame (src/cdef.rs:180) as
+ * driven by cdef_frame_from_idx (src/cdf.rs:20300). */
+av1g_status av1g_run_cdef(const av1g_frame_job* jobs, int32_t n, void* stream);
+
+/* §7.16 superres: deblocked -> up_deblocked and cdef -> up_cdef.
+ * Replaces upscale_frame (src/superres.rs:282) as called at
+ * frame_driver.rs:906-966. */
+av1g_status av1g_run_superres(const av1g_frame_job* jobs, int32_t n, void* stream);
+
+/* §7.17 loop restoration: (up_)cdef + (up_)deblocked -> lr.  Replaces
+ * loop_restoration_frame (src/loop_restoration.rs:268) as driven by
+ * loop_restore_frame_from_grid (src/cdf.rs:20624). */
+av1g_status av1g_run_lr(const av1g_frame_job* jobs, int32_t n, void* stream);
+
+/* §7.18.3 film grain: lr (cropped) -> out.  Replaces film_grain_synthesis
+ * (src/film_grain.rs:848) as called at frame_driver.rs:1060-1096. */
+av1g_status av1g_run_film_grain(const av1g_frame_job* jobs, int32_t n, void* stream);
+
+/* The whole §7.4 chain of frame_driver.rs:830-1096 for `n` jobs:
+ * deblock, CDEF, superres, loop restoration, film grain, with the
+ * reference's gating.  mode = AV1G_MODE_BATCHED or AV1G_MODE_PER_FRAME.
+ * *launches (optional) receives the number of kernels launched. */
+av1g_status av1g_run_postfilter(const av1g_frame_job* jobs, int32_t n, int32_t mode,
+                                void* stream, int32_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AV1G_H */

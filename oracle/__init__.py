@@ -1,0 +1,186 @@
+"""CPU parity oracle — TEST INFRASTRUCTURE ONLY.
+
+A C restatement of the reference decoder's pixel path (see oracle.h), built
+with gcc into ``liboxav1_oracle.so`` and driven through ctypes.  Only the test
+suite, the smoke check and the bench's CPU-baseline / reference arms use it;
+the engine never imports it.
+"""
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parent
+LIB = HERE / "liboxav1_oracle.so"
+SOURCES = sorted(HERE.glob("*.c"))
+HEADERS = [HERE / "oracle.h", REPO / "include" / "av1g.h",
+           REPO / "oxideav-av1_b200" / "csrc" / "av1_spec_tables.h"]
+
+_lib = None
+
+
+def build(force=False):
+    srcs = sorted(HERE.glob("*.c"))
+    newest = max(p.stat().st_mtime for p in srcs + HEADERS)
+    if force or not LIB.exists() or LIB.stat().st_mtime < newest:
+        cmd = ["gcc", "-O2", "-fPIC", "-shared", "-Wall", "-Wno-missing-braces", "-std=gnu11",
+               "-I" + str(REPO / "include"), "-I" + str(REPO / "oxideav-av1_b200" / "csrc"),
+               *map(str, srcs), "-o", str(LIB), "-lm"]
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+class OraPlane(C.Structure):
+    _fields_ = [("s", C.POINTER(C.c_int32)), ("rows", C.c_int32), ("cols", C.c_int32)]
+
+
+def load():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = C.CDLL(str(LIB))
+        _lib.ora_postfilter_frame.restype = C.c_int
+        _lib.ora_random_next.restype = C.c_uint32
+        _lib.ora_random_next.argtypes = [C.POINTER(C.c_uint16), C.c_int]
+    return _lib
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def _grid_struct(frame, keep):
+    from_abi = _abi_module()
+    g = from_abi.MiGrid()
+    for k in ["mi_size", "skip", "is_inter", "ref_frame0", "y_mode", "segment_id", "delta_lf", "tx_size",
+              "inter_tx_size"]:
+        a = np.ascontiguousarray(frame.grid[k])
+        keep.append(a)
+        setattr(g, k, a.ctypes.data)
+    return g
+
+
+def _abi_module():
+    import sys
+    return sys.modules["oxideav_av1_b200.abi"]
+
+
+def _units(frame, keep):
+    arr = (C.c_void_p * 3)()
+    for p in range(3):
+        u = frame.lr_units[p]
+        if u is not None:
+            a = np.ascontiguousarray(u)
+            keep.append(a)
+            arr[p] = a.ctypes.data
+    return arr
+
+
+def postfilter_frame(frame):
+    """Full §7.4 chain on the CPU; returns (ref_planes, out_planes) as int32 arrays."""
+    lib = load()
+    keep = []
+    h = frame.hdr
+    grid = _grid_struct(frame, keep)
+    idx = np.ascontiguousarray(frame.cdef_idx)
+    units = _units(frame, keep)
+    recon = [_i32(frame.recon[p]) for p in range(h.num_planes)]
+    rec_p = (C.POINTER(C.c_int32) * 3)(*[_ptr(r) for r in recon])
+    refs, outs = [], []
+    for p in range(h.num_planes):
+        oh, ow = frame.out_dims(p)
+        refs.append(np.zeros((oh, ow), np.int32))
+        outs.append(np.zeros((oh, ow), np.int32))
+    ref_p = (C.POINTER(C.c_int32) * 3)(*[_ptr(r) for r in refs])
+    out_p = (C.POINTER(C.c_int32) * 3)(*[_ptr(r) for r in outs])
+    rc = lib.ora_postfilter_frame(C.byref(h), C.byref(grid), idx.ctypes.data_as(C.c_void_p), units, rec_p,
+                                  ref_p, out_p)
+    if rc != 0:
+        raise RuntimeError(f"oracle rejected the frame ({rc})")
+    return refs, outs
+
+
+def _planes(arrs):
+    ps = (OraPlane * 3)()
+    for i, a in enumerate(arrs):
+        ps[i] = OraPlane(_ptr(a), a.shape[0], a.shape[1])
+    return ps
+
+
+def loop_filter(frame, planes):
+    """§7.14 on int32 planes (modified in place)."""
+    lib = load()
+    keep = []
+    grid = _grid_struct(frame, keep)
+    lib.ora_loop_filter_frame(C.byref(frame.hdr), C.byref(grid), _planes(planes))
+    return planes
+
+
+def cdef(frame, src):
+    lib = load()
+    keep = []
+    grid = _grid_struct(frame, keep)
+    dst = [np.zeros_like(s) for s in src]
+    idx = np.ascontiguousarray(frame.cdef_idx)
+    lib.ora_cdef_frame(C.byref(frame.hdr), C.byref(grid), idx.ctypes.data_as(C.c_void_p), _planes(src),
+                       _planes(dst))
+    return dst
+
+
+def upscale(frame, src):
+    lib = load()
+    dst = [np.zeros(frame.out_dims(p), np.int32) for p in range(frame.hdr.num_planes)]
+    rc = lib.ora_upscale_frame(C.byref(frame.hdr), _planes(src), _planes(dst))
+    if rc:
+        raise RuntimeError("oracle upscale rejected the frame")
+    return dst
+
+
+def loop_restoration(frame, curr, cdef_planes):
+    lib = load()
+    keep = []
+    units = _units(frame, keep)
+    rows = (C.c_int32 * 3)()
+    cols = (C.c_int32 * 3)()
+    for p in range(frame.hdr.num_planes):
+        rows[p], cols[p] = frame.lr_grid(p)
+    lr = [np.zeros_like(c) for c in cdef_planes]
+    lib.ora_lr_frame(C.byref(frame.hdr), units, rows, cols, _planes(curr), _planes(cdef_planes), _planes(lr))
+    return lr
+
+
+def film_grain(frame, planes):
+    lib = load()
+    h = frame.hdr
+    lib.ora_film_grain(C.byref(h.film_grain), h.bit_depth, h.num_planes, h.subsampling_x, h.subsampling_y,
+                       h.matrix_coefficients, _planes(planes))
+    return planes
+
+
+def generate_grain(fg, bit_depth, ssx, ssy):
+    lib = load()
+    luma = np.zeros((73, 82), np.int32)
+    cw, ch = (44 if ssx else 82), (38 if ssy else 73)
+    cb = np.zeros((ch, cw), np.int32)
+    cr = np.zeros((ch, cw), np.int32)
+    lib.ora_generate_grain(C.byref(fg), bit_depth, ssx, ssy, _ptr(luma), _ptr(cb), _ptr(cr))
+    return luma, cb, cr
+
+
+def scaling_lut(fg, num_planes):
+    lib = load()
+    lut = np.zeros((3, 256), np.uint8)
+    lib.ora_scaling_lookup_init(C.byref(fg), num_planes, lut.ctypes.data_as(C.c_void_p))
+    return lut
+
+
+def random_draws(seed, bits, count):
+    lib = load()
+    st = C.c_uint16(seed)
+    return [lib.ora_random_next(C.byref(st), bits) for _ in range(count)]

@@ -1,0 +1,81 @@
+/*
+ * oracle.h — CPU restatement of the reference decoder's pixel path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the parity oracle for the CUDA
+ * engine: tests, the smoke check and the bench's CPU-baseline arm call it to
+ * produce the expected output on the same inputs.  The engine never links,
+ * loads or calls it.
+ *
+ * Every function restates the reference crate's CPU code (Rust, not buildable
+ * here: no rustc/cargo and the `oxideav-core` dependency is not vendored) in
+ * the reference's own per-sample formulation, with the file:line it follows
+ * cited at each definition.  Planes are int32 row-major, like the reference's
+ * `PlaneBuffer` (src/loop_filter.rs:119-126).
+ */
+#ifndef AV1_ORACLE_H
+#define AV1_ORACLE_H
+
+#include <stdint.h>
+#include "av1g.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ora_plane {
+    int32_t* s;
+    int32_t rows;
+    int32_t cols;
+} ora_plane;
+
+/* §7.14 — loop_filter_frame (src/loop_filter.rs:271) driven by
+ * loop_filter_frame_from_grid (src/cdf.rs:20449).  In place. */
+void ora_loop_filter_frame(const av1g_frame_header* hdr, const av1g_mi_grid* grid,
+                           ora_plane planes[3]);
+
+/* §7.15 — cdef_frame (src/cdef.rs:180) driven by cdef_frame_from_idx
+ * (src/cdf.rs:20300).  cdef_idx per 64x64: ceil(mi_rows/16) x ceil(mi_cols/16). */
+void ora_cdef_frame(const av1g_frame_header* hdr, const av1g_mi_grid* grid,
+                    const int8_t* cdef_idx, const ora_plane src[3], ora_plane dst[3]);
+
+/* §7.16 — upscale_frame (src/superres.rs:282).  Returns 0 on success. */
+int ora_upscale_frame(const av1g_frame_header* hdr, const ora_plane in[3], ora_plane out[3]);
+
+/* §7.17 — loop_restoration_frame (src/loop_restoration.rs:268) driven by
+ * loop_restore_frame_from_grid (src/cdf.rs:20624). */
+void ora_lr_frame(const av1g_frame_header* hdr, const av1g_lr_unit* const units[3],
+                  const int32_t unit_rows[3], const int32_t unit_cols[3],
+                  const ora_plane curr[3], const ora_plane cdef[3], ora_plane lr[3]);
+
+/* §7.18.3 — film_grain_synthesis (src/film_grain.rs:848), in place on the
+ * cropped output planes. */
+void ora_film_grain(const av1g_film_grain* fg, int bit_depth, int num_planes, int sub_x,
+                    int sub_y, int matrix_coefficients, ora_plane out[3]);
+
+/* §7.18.3.3 generate_grain (src/film_grain.rs:230) — exposed for the
+ * template-level known-answer tests.  luma: 73x82, cb/cr: chroma_h x chroma_w. */
+void ora_generate_grain(const av1g_film_grain* fg, int bit_depth, int sub_x, int sub_y,
+                        int32_t* luma, int32_t* cb, int32_t* cr);
+
+/* §7.18.3.4 scaling_lookup_init (src/film_grain.rs:418): 3 x 256 table. */
+void ora_scaling_lookup_init(const av1g_film_grain* fg, int num_planes, uint8_t lut[3][256]);
+
+/* §7.18.3.2 RandomRegister::next (src/film_grain.rs:119). */
+uint32_t ora_random_next(uint16_t* state, int bits);
+
+/* The §7.4 chain of decode_frame_spec_tiles (src/decoder/frame_driver.rs:
+ * 790-1116): deblock, CDEF, superres, LR, crop, pre-grain store, grain.
+ * recon: padded-extent planes (not modified).  ref_out / out: cropped
+ * UpscaledWidth x FrameHeight planes (chroma subsampled), row stride = width;
+ * ref_out is the §7.20 pre-grain payload, out the post-grain output.
+ * Returns 0 on success, nonzero on a malformed header. */
+int ora_postfilter_frame(const av1g_frame_header* hdr, const av1g_mi_grid* grid,
+                         const int8_t* cdef_idx, const av1g_lr_unit* const units[3],
+                         const int32_t* const recon[3], int32_t* ref_out[3],
+                         int32_t* out[3]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

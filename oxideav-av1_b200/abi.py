@@ -1,0 +1,146 @@
+"""ctypes mirror of ``include/av1g.h`` and the loader of the CUDA library.
+
+The structures below are field-for-field copies of the C structs; the loader
+checks their sizes against ``av1g_struct_size`` exported by the library so a
+drift between the header and this file fails at load time rather than
+corrupting a launch.  There is no CPU fallback: if the library is missing or
+fails to load, ``load()`` raises.
+"""
+import ctypes as C
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "liboxav1_b200.so"
+
+AV1G_OK = 0
+AV1G_EINVAL = 1
+AV1G_ENOMEM_BUDGET = 2
+AV1G_EBUSY = 3
+AV1G_TIMEOUT = 4
+AV1G_EDEVICE = 5
+AV1G_EPARITY = 6
+AV1G_ENOTSUP = 7
+AV1G_ENOTREADY = 8
+STATUS_NAMES = {0: "OK", 1: "EINVAL", 2: "ENOMEM_BUDGET", 3: "EBUSY", 4: "TIMEOUT", 5: "EDEVICE",
+                6: "EPARITY", 7: "ENOTSUP", 8: "ENOTREADY"}
+
+MODE_BATCHED = 0
+MODE_PER_FRAME = 1
+
+
+class FilmGrain(C.Structure):
+    _fields_ = [
+        ("apply_grain", C.c_uint8), ("chroma_scaling_from_luma", C.c_uint8), ("grain_seed", C.c_uint16),
+        ("num_y_points", C.c_uint8), ("point_y_value", C.c_uint8 * 14), ("point_y_scaling", C.c_uint8 * 14),
+        ("num_cb_points", C.c_uint8), ("point_cb_value", C.c_uint8 * 10), ("point_cb_scaling", C.c_uint8 * 10),
+        ("num_cr_points", C.c_uint8), ("point_cr_value", C.c_uint8 * 10), ("point_cr_scaling", C.c_uint8 * 10),
+        ("grain_scaling", C.c_uint8), ("ar_coeff_lag", C.c_uint8),
+        ("ar_coeffs_y_plus_128", C.c_uint8 * 24), ("ar_coeffs_cb_plus_128", C.c_uint8 * 25),
+        ("ar_coeffs_cr_plus_128", C.c_uint8 * 25), ("ar_coeff_shift", C.c_uint8), ("grain_scale_shift", C.c_uint8),
+        ("cb_mult", C.c_uint8), ("cb_luma_mult", C.c_uint8), ("cr_mult", C.c_uint8), ("cr_luma_mult", C.c_uint8),
+        ("overlap_flag", C.c_uint8), ("clip_to_restricted_range", C.c_uint8),
+        ("cb_offset", C.c_uint16), ("cr_offset", C.c_uint16),
+    ]
+
+
+class FrameHeader(C.Structure):
+    _fields_ = [
+        ("frame_width", C.c_int32), ("frame_height", C.c_int32), ("upscaled_width", C.c_int32),
+        ("mi_rows", C.c_int32), ("mi_cols", C.c_int32),
+        ("bit_depth", C.c_uint8), ("subsampling_x", C.c_uint8), ("subsampling_y", C.c_uint8),
+        ("num_planes", C.c_uint8), ("matrix_coefficients", C.c_uint8), ("use_superres", C.c_uint8),
+        ("coded_lossless", C.c_uint8), ("allow_intrabc", C.c_uint8), ("enable_cdef", C.c_uint8),
+        ("lf_level", C.c_uint8 * 4), ("lf_sharpness", C.c_uint8), ("lf_delta_enabled", C.c_uint8),
+        ("delta_lf_multi", C.c_uint8), ("lf_ref_deltas", C.c_int8 * 8), ("lf_mode_deltas", C.c_int8 * 2),
+        ("seg_lf_active", (C.c_uint8 * 4) * 8), ("seg_lf_data", (C.c_int16 * 4) * 8),
+        ("cdef_short_circuited", C.c_uint8), ("cdef_damping", C.c_uint8), ("cdef_bits", C.c_uint8),
+        ("cdef_y_pri", C.c_uint8 * 8), ("cdef_y_sec", C.c_uint8 * 8),
+        ("cdef_uv_pri", C.c_uint8 * 8), ("cdef_uv_sec", C.c_uint8 * 8),
+        ("uses_lr", C.c_uint8), ("lr_type", C.c_uint8 * 3), ("lr_unit_size", C.c_int32 * 3),
+        ("film_grain", FilmGrain),
+    ]
+
+
+class LrUnit(C.Structure):
+    _fields_ = [("type", C.c_uint8), ("sgr_set", C.c_uint8), ("wiener", (C.c_int8 * 3) * 2),
+                ("sgr_xqd", C.c_int16 * 2)]
+
+
+class MiGrid(C.Structure):
+    _fields_ = [
+        ("mi_size", C.c_void_p), ("skip", C.c_void_p), ("is_inter", C.c_void_p), ("ref_frame0", C.c_void_p),
+        ("y_mode", C.c_void_p), ("segment_id", C.c_void_p), ("delta_lf", C.c_void_p), ("tx_size", C.c_void_p),
+        ("inter_tx_size", C.c_void_p),
+    ]
+
+
+class Plane(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("stride", C.c_int32), ("width", C.c_int32), ("height", C.c_int32)]
+
+
+class FrameJob(C.Structure):
+    _fields_ = [
+        ("hdr", C.POINTER(FrameHeader)), ("grid", MiGrid), ("cdef_idx", C.c_void_p),
+        ("lr_units", C.c_void_p * 3),
+        ("recon", Plane * 3), ("deblocked", Plane * 3), ("cdef", Plane * 3), ("up_deblocked", Plane * 3),
+        ("up_cdef", Plane * 3), ("lr", Plane * 3), ("out", Plane * 3),
+    ]
+
+
+_STRUCTS = {"av1g_film_grain": FilmGrain, "av1g_frame_header": FrameHeader, "av1g_lr_unit": LrUnit,
+            "av1g_mi_grid": MiGrid, "av1g_plane": Plane, "av1g_frame_job": FrameJob}
+
+# exported entry points and their ctypes signatures
+_SIGS = {
+    "av1g_abi_version": (C.c_int32, []),
+    "av1g_struct_size": (C.c_int32, [C.c_char_p]),
+    "av1g_last_error": (C.c_char_p, []),
+    "av1g_lr_units_in_frame": (C.c_int32, [C.c_int32, C.c_int32]),
+    "av1g_run_deblock": (C.c_int, [C.POINTER(FrameJob), C.c_int32, C.c_void_p]),
+    "av1g_run_cdef": (C.c_int, [C.POINTER(FrameJob), C.c_int32, C.c_void_p]),
+    "av1g_run_superres": (C.c_int, [C.POINTER(FrameJob), C.c_int32, C.c_void_p]),
+    "av1g_run_lr": (C.c_int, [C.POINTER(FrameJob), C.c_int32, C.c_void_p]),
+    "av1g_run_film_grain": (C.c_int, [C.POINTER(FrameJob), C.c_int32, C.c_void_p]),
+    "av1g_run_postfilter": (C.c_int, [C.POINTER(FrameJob), C.c_int32, C.c_int32, C.c_void_p,
+                                      C.POINTER(C.c_int32)]),
+}
+
+_lib = None
+
+
+class Av1gError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def load(path=None):
+    """Load the CUDA library once; raises if it is absent or inconsistent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(f"CUDA library {p} is not built; run build.py (no CPU fallback exists)")
+    lib = C.CDLL(str(p))
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if lib.av1g_abi_version() != 1:
+        raise RuntimeError("ABI version mismatch")
+    for cname, cls in _STRUCTS.items():
+        n = lib.av1g_struct_size(cname.encode())
+        if n != C.sizeof(cls):
+            raise RuntimeError(f"struct {cname}: library {n} bytes, ctypes {C.sizeof(cls)} bytes")
+    _lib = lib
+    return lib
+
+
+def check(status):
+    if status != AV1G_OK:
+        raise Av1gError(status, _lib.av1g_last_error().decode(errors="replace"))
+
+
+def exported_symbols():
+    return list(_SIGS)

@@ -1,0 +1,319 @@
+// api.cu — the av1g_* C ABI: descriptor validation, stage gating and the
+// batched / per-frame launch of the §7.4 post-filter chain.
+//
+// Gating and buffer flow follow decode_frame_spec_tiles
+// (src/decoder/frame_driver.rs:790-1116):
+//   deblock  iff (lf_level[0] || lf_level[1]) && !CodedLossless && !allow_intrabc   (832-836)
+//   CDEF     iff !CodedLossless && !allow_intrabc && enable_cdef && cdef coded      (870)
+//   superres iff use_superres && UpscaledWidth > FrameWidth                          (906)
+//   LR       iff UsesLr                                                             (971)
+//   grain    iff apply_grain                                                        (1060)
+// A stage that is off forwards its input plane to the next stage (pointer
+// aliasing, no copy), and so does a chroma plane whose deblock level
+// (loop_filter.rs:274-278) or restoration type is zero.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace av1g {
+size_t lr_smem_bytes();
+}
+
+using namespace av1g;
+
+namespace {
+
+thread_local std::string g_err;
+
+av1g_status fail(av1g_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return s;
+}
+
+av1g_status cuda_fail(cudaError_t e, const char* what) {
+    return fail(AV1G_EDEVICE, "%s: %s", what, cudaGetErrorString(e));
+}
+
+int r2u(int x, int n) { return n ? (x + (1 << (n - 1))) >> n : x; }
+
+PlaneDev to_dev(const av1g_plane& p) { return PlaneDev{(uint8_t*)p.data, p.stride, p.width, p.height}; }
+
+bool plane_ok(const av1g_plane& p, int w, int h, int bps) {
+    return p.data && p.width >= w && p.height >= h && p.stride >= w * bps;
+}
+
+int count_units(int us, int sz) {
+    if (us <= 0) return 1;
+    int n = (sz + (us >> 1)) / us;
+    return n > 1 ? n : 1;
+}
+
+// Builds the FrameDev record of one job and validates it.
+av1g_status prepare_frame(const av1g_frame_job& j, FrameDev& F) {
+    if (!j.hdr) return fail(AV1G_EINVAL, "job without header");
+    const av1g_frame_header& h = *j.hdr;
+    memset(&F, 0, sizeof F);
+    F.h = h;
+    if (h.bit_depth != 8 && h.bit_depth != 10 && h.bit_depth != 12)
+        return fail(AV1G_EINVAL, "bit_depth %d", h.bit_depth);
+    if (h.num_planes != 1 && h.num_planes != 3) return fail(AV1G_EINVAL, "num_planes %d", h.num_planes);
+    if (h.subsampling_x > 1 || h.subsampling_y > 1 || (h.subsampling_y && !h.subsampling_x))
+        return fail(AV1G_EINVAL, "subsampling %d,%d", h.subsampling_x, h.subsampling_y);
+    if (h.frame_width <= 0 || h.frame_height <= 0 || h.upscaled_width < h.frame_width)
+        return fail(AV1G_EINVAL, "frame size %dx%d upscaled %d", h.frame_width, h.frame_height, h.upscaled_width);
+    if (h.mi_cols != 2 * ((h.frame_width + 7) >> 3) || h.mi_rows != 2 * ((h.frame_height + 7) >> 3))
+        return fail(AV1G_EINVAL, "MiRows/MiCols %d/%d do not match %dx%d", h.mi_rows, h.mi_cols, h.frame_width,
+                    h.frame_height);
+    if (h.cdef_bits > 3 || h.cdef_damping < 3 || h.cdef_damping > 6)
+        return fail(AV1G_EINVAL, "cdef_bits %d damping %d", h.cdef_bits, h.cdef_damping);
+    const int hbd = h.bit_depth > 8, bps = hbd ? 2 : 1;
+    F.hbd = hbd;
+    F.g = j.grid;
+    F.cdef_idx = j.cdef_idx;
+    const int np = h.num_planes, ssx = h.subsampling_x, ssy = h.subsampling_y;
+    int pw[3], ph[3], uw[3], fh[3];
+    for (int p = 0; p < np; p++) {
+        int sx = p ? ssx : 0, sy = p ? ssy : 0;
+        pw[p] = (h.mi_cols * 4) >> sx;
+        ph[p] = (h.mi_rows * 4) >> sy;
+        uw[p] = r2u(h.upscaled_width, sx);
+        fh[p] = r2u(h.frame_height, sy);
+        if (!plane_ok(j.recon[p], pw[p], ph[p], bps)) return fail(AV1G_EINVAL, "recon plane %d too small", p);
+    }
+    F.do_stage[ST_DEBLOCK] = (h.lf_level[0] || h.lf_level[1]) && !h.coded_lossless && !h.allow_intrabc;
+    F.do_stage[ST_CDEF] = !h.coded_lossless && !h.allow_intrabc && h.enable_cdef && !h.cdef_short_circuited;
+    F.do_stage[ST_SUPERRES] = h.use_superres && h.upscaled_width > h.frame_width;
+    F.do_stage[ST_LR] = h.uses_lr != 0;
+    F.do_stage[ST_GRAIN] = h.film_grain.apply_grain != 0;
+    bool grid_needed = F.do_stage[ST_DEBLOCK] || F.do_stage[ST_CDEF];
+    if (grid_needed && (!j.grid.skip || !j.grid.mi_size))
+        return fail(AV1G_EINVAL, "mi grid missing");
+    if (F.do_stage[ST_DEBLOCK] && (!j.grid.is_inter || !j.grid.ref_frame0 || !j.grid.y_mode || !j.grid.segment_id ||
+                                   !j.grid.delta_lf || !j.grid.tx_size || !j.grid.inter_tx_size))
+        return fail(AV1G_EINVAL, "mi grid incomplete for deblock");
+    if (F.do_stage[ST_CDEF] && !j.cdef_idx) return fail(AV1G_EINVAL, "cdef_idx missing");
+    for (int p = 0; p < np; p++) {
+        F.recon[p] = to_dev(j.recon[p]);
+        bool deb = F.do_stage[ST_DEBLOCK] && (p == 0 || h.lf_level[1 + p] != 0);
+        if (deb && !plane_ok(j.deblocked[p], pw[p], ph[p], bps)) return fail(AV1G_EINVAL, "deblocked plane %d", p);
+        F.deb[p] = deb ? to_dev(j.deblocked[p]) : F.recon[p];
+        if (F.do_stage[ST_CDEF] && !plane_ok(j.cdef[p], pw[p], ph[p], bps)) return fail(AV1G_EINVAL, "cdef plane %d", p);
+        F.cdef[p] = F.do_stage[ST_CDEF] ? to_dev(j.cdef[p]) : F.deb[p];
+        if (F.do_stage[ST_SUPERRES]) {
+            if (!plane_ok(j.up_cdef[p], uw[p], fh[p], bps)) return fail(AV1G_EINVAL, "up_cdef plane %d", p);
+            F.upcdef[p] = to_dev(j.up_cdef[p]);
+            if (F.do_stage[ST_LR]) {
+                if (!plane_ok(j.up_deblocked[p], uw[p], fh[p], bps)) return fail(AV1G_EINVAL, "up_deblocked plane %d", p);
+                F.updeb[p] = to_dev(j.up_deblocked[p]);
+            } else {
+                F.updeb[p] = F.deb[p];
+            }
+        } else {
+            F.upcdef[p] = F.cdef[p];
+            F.updeb[p] = F.deb[p];
+        }
+        bool lr = F.do_stage[ST_LR] && h.lr_type[p] != 0;
+        if (lr) {
+            if (!plane_ok(j.lr[p], uw[p], fh[p], bps)) return fail(AV1G_EINVAL, "lr plane %d", p);
+            if (h.lr_unit_size[p] < 32 || h.lr_unit_size[p] > 256 || (h.lr_unit_size[p] & (h.lr_unit_size[p] - 1)))
+                return fail(AV1G_EINVAL, "lr unit size %d", h.lr_unit_size[p]);
+            F.lr[p] = to_dev(j.lr[p]);
+            F.lr_units[p] = j.lr_units[p];
+            F.lr_unit_rows[p] = count_units(h.lr_unit_size[p], fh[p]);
+            F.lr_unit_cols[p] = count_units(h.lr_unit_size[p], uw[p]);
+        } else {
+            F.lr[p] = F.upcdef[p];
+        }
+        F.lr[p].w = uw[p];  // the cropped view the reference stores (frame_driver.rs:1018-1052)
+        F.lr[p].h = fh[p];
+        if (F.do_stage[ST_GRAIN]) {
+            if (!plane_ok(j.out[p], uw[p], fh[p], bps)) return fail(AV1G_EINVAL, "out plane %d", p);
+            F.out[p] = to_dev(j.out[p]);
+            F.out[p].w = uw[p];
+            F.out[p].h = fh[p];
+        } else {
+            F.out[p] = F.lr[p];
+        }
+    }
+    if (F.do_stage[ST_GRAIN]) {
+        const av1g_film_grain& g = h.film_grain;
+        if (g.num_y_points > 14 || g.num_cb_points > 10 || g.num_cr_points > 10 || g.ar_coeff_lag > 3 ||
+            g.grain_scaling < 8 || g.grain_scaling > 11 || g.ar_coeff_shift < 6 || g.ar_coeff_shift > 9 ||
+            g.grain_scale_shift > 3)
+            return fail(AV1G_EINVAL, "film grain parameters out of range");
+        F.grain_nblocks = ((h.upscaled_width + 1) / 2 + 15) / 16;
+    }
+    return AV1G_OK;
+}
+
+int grain_scratch_bytes(const FrameDev& F) {
+    int nstripes = ((F.h.frame_height + 1) / 2 + 15) / 16;
+    return (3 * 73 * 82 * 2 + 768 + nstripes * F.grain_nblocks + 255) & ~255;
+}
+
+struct Batch {
+    std::vector<FrameDev> frames;
+    // per stage (and the grain template pass, index ST_COUNT) tile counts per frame
+    std::vector<int32_t> tiles[ST_COUNT + 1];
+};
+
+int stage_tiles(const FrameDev& F, int st) {
+    if (st < ST_COUNT && !F.do_stage[st]) return 0;
+    switch (st) {
+        case ST_DEBLOCK: return tiles_deblock(F);
+        case ST_CDEF: return tiles_cdef(F);
+        case ST_SUPERRES: return tiles_superres(F);
+        case ST_LR: return tiles_lr(F);
+        case ST_GRAIN: return tiles_grain_blend(F);
+        default: return F.do_stage[ST_GRAIN] ? 1 : 0;  // template pass
+    }
+}
+
+// Runs `stages` (bit mask over ST_*) for the jobs.
+av1g_status run(const av1g_frame_job* jobs, int n, int stage_mask, int mode, void* stream, int* launches) {
+    g_err.clear();
+    if (launches) *launches = 0;
+    if (n < 0 || (n > 0 && !jobs)) return fail(AV1G_EINVAL, "bad job array");
+    if (n == 0) return AV1G_OK;
+    if (mode != AV1G_MODE_BATCHED && mode != AV1G_MODE_PER_FRAME) return fail(AV1G_EINVAL, "mode %d", mode);
+    cudaStream_t s = (cudaStream_t)stream;
+    Batch b;
+    b.frames.resize(n);
+    for (int i = 0; i < n; i++) {
+        av1g_status st = prepare_frame(jobs[i], b.frames[i]);
+        if (st != AV1G_OK) {
+            std::string m = g_err;
+            return fail(st, "job %d: %s", i, m.c_str());
+        }
+    }
+    // layout: frames | starts (batched: NS x (n+1)) | per-frame starts (n x NS x 2) | grain scratch
+    const int NS = ST_COUNT + 1;
+    size_t off_starts = ((sizeof(FrameDev) * n) + 255) & ~(size_t)255;
+    size_t off_pf = off_starts + sizeof(int32_t) * NS * (n + 1);
+    size_t off_scratch = (off_pf + sizeof(int32_t) * n * NS * 2 + 255) & ~(size_t)255;
+    size_t scratch = 0;
+    std::vector<size_t> scratch_off(n, 0);
+    if (stage_mask & (1 << ST_GRAIN))
+        for (int i = 0; i < n; i++)
+            if (b.frames[i].do_stage[ST_GRAIN]) {
+                scratch_off[i] = off_scratch + scratch;
+                scratch += grain_scratch_bytes(b.frames[i]);
+            }
+    size_t total_bytes = off_scratch + scratch;
+    uint8_t* dev = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&dev, total_bytes, s);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
+    for (int i = 0; i < n; i++)
+        if (scratch_off[i]) {
+            FrameDev& F = b.frames[i];
+            F.grain_tmpl = (int16_t*)(dev + scratch_off[i]);
+            F.grain_lut = (uint8_t*)(dev + scratch_off[i] + 3 * 73 * 82 * 2);
+            F.grain_offs = F.grain_lut + 768;
+        }
+    std::vector<uint8_t> host(off_scratch, 0);
+    memcpy(host.data(), b.frames.data(), sizeof(FrameDev) * n);
+    int32_t* hs = (int32_t*)(host.data() + off_starts);
+    int32_t* hpf = (int32_t*)(host.data() + off_pf);
+    int32_t totals[ST_COUNT + 1];
+    for (int st = 0; st < NS; st++) {
+        int32_t acc = 0;
+        for (int i = 0; i < n; i++) {
+            int c = (stage_mask & (1 << (st < ST_COUNT ? st : ST_GRAIN))) ? stage_tiles(b.frames[i], st) : 0;
+            hs[st * (n + 1) + i] = acc;
+            hpf[(i * NS + st) * 2 + 0] = 0;
+            hpf[(i * NS + st) * 2 + 1] = c;
+            acc += c;
+        }
+        hs[st * (n + 1) + n] = acc;
+        totals[st] = acc;
+    }
+    e = cudaMemcpyAsync(dev, host.data(), off_scratch, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+        cudaFreeAsync(dev, s);
+        return cuda_fail(e, "cudaMemcpyAsync");
+    }
+    const FrameDev* dframes = (const FrameDev*)dev;
+    const int32_t* ds = (const int32_t*)(dev + off_starts);
+    const int32_t* dpf = (const int32_t*)(dev + off_pf);
+    int nl = 0;
+    auto launch_stage = [&](int st, const FrameDev* fr, const int32_t* starts, const int32_t* starts_tmpl, int nn,
+                            int total, int total_tmpl) {
+        switch (st) {
+            case ST_DEBLOCK: if (total) { launch_deblock(fr, starts, nn, total, s); nl++; } break;
+            case ST_CDEF: if (total) { launch_cdef(fr, starts, nn, total, s); nl++; } break;
+            case ST_SUPERRES: if (total) { launch_superres(fr, starts, nn, total, s); nl++; } break;
+            case ST_LR: if (total) { launch_lr(fr, starts, nn, total, s); nl++; } break;
+            case ST_GRAIN:
+                launch_grain(fr, starts_tmpl, starts, nn, total_tmpl, total, s);
+                nl += (total_tmpl > 0) + (total > 0);
+                break;
+        }
+    };
+    for (int st = 0; st < ST_COUNT; st++) {
+        if (!(stage_mask & (1 << st))) continue;
+        if (mode == AV1G_MODE_BATCHED) {
+            launch_stage(st, dframes, ds + st * (n + 1), ds + ST_COUNT * (n + 1), n, totals[st], totals[ST_COUNT]);
+        } else {
+            for (int i = 0; i < n; i++)
+                launch_stage(st, dframes + i, dpf + (i * NS + st) * 2, dpf + (i * NS + ST_COUNT) * 2, 1,
+                             hpf[(i * NS + st) * 2 + 1], hpf[(i * NS + ST_COUNT) * 2 + 1]);
+        }
+    }
+    e = cudaGetLastError();
+    cudaFreeAsync(dev, s);
+    if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+    if (launches) *launches = nl;
+    return AV1G_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t av1g_abi_version(void) { return AV1G_ABI_VERSION; }
+
+int32_t av1g_struct_size(const char* name) {
+    if (!name) return -1;
+    if (!strcmp(name, "av1g_film_grain")) return (int32_t)sizeof(av1g_film_grain);
+    if (!strcmp(name, "av1g_frame_header")) return (int32_t)sizeof(av1g_frame_header);
+    if (!strcmp(name, "av1g_lr_unit")) return (int32_t)sizeof(av1g_lr_unit);
+    if (!strcmp(name, "av1g_mi_grid")) return (int32_t)sizeof(av1g_mi_grid);
+    if (!strcmp(name, "av1g_plane")) return (int32_t)sizeof(av1g_plane);
+    if (!strcmp(name, "av1g_frame_job")) return (int32_t)sizeof(av1g_frame_job);
+    return -1;
+}
+
+const char* av1g_last_error(void) { return g_err.c_str(); }
+
+int32_t av1g_lr_units_in_frame(int32_t unit_size, int32_t plane_size) { return count_units(unit_size, plane_size); }
+
+av1g_status av1g_run_deblock(const av1g_frame_job* jobs, int32_t n, void* stream) {
+    return run(jobs, n, 1 << ST_DEBLOCK, AV1G_MODE_BATCHED, stream, nullptr);
+}
+av1g_status av1g_run_cdef(const av1g_frame_job* jobs, int32_t n, void* stream) {
+    return run(jobs, n, 1 << ST_CDEF, AV1G_MODE_BATCHED, stream, nullptr);
+}
+av1g_status av1g_run_superres(const av1g_frame_job* jobs, int32_t n, void* stream) {
+    return run(jobs, n, 1 << ST_SUPERRES, AV1G_MODE_BATCHED, stream, nullptr);
+}
+av1g_status av1g_run_lr(const av1g_frame_job* jobs, int32_t n, void* stream) {
+    return run(jobs, n, 1 << ST_LR, AV1G_MODE_BATCHED, stream, nullptr);
+}
+av1g_status av1g_run_film_grain(const av1g_frame_job* jobs, int32_t n, void* stream) {
+    return run(jobs, n, 1 << ST_GRAIN, AV1G_MODE_BATCHED, stream, nullptr);
+}
+av1g_status av1g_run_postfilter(const av1g_frame_job* jobs, int32_t n, int32_t mode, void* stream,
+                                int32_t* launches) {
+    return run(jobs, n, (1 << ST_COUNT) - 1, mode, stream, launches);
+}
+
+}  // extern "C"

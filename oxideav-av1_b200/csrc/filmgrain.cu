@@ -1,0 +1,377 @@
+// filmgrain.cu — §7.18.3 film grain synthesis.
+//
+// Replaces film_grain_synthesis / generate_grain / scaling_lookup_init /
+// add_noise_synthesis (src/film_grain.rs:100-873) as called at
+// frame_driver.rs:1060-1096.
+//
+// Two kernels:
+//  * grain_template_kernel — one CTA per frame builds the 82x73 luma and the
+//    chroma grain templates, the three scaling LUTs and the per-stripe random
+//    block offsets into a per-frame scratch area.  The reference draws the
+//    white noise from one 16-bit LFSR in raster order; the LFSR is linear over
+//    GF(2), so the state at the start of row y is M^(W*y) applied to the seed
+//    and every row is generated by its own thread after a jump of at most
+//    seven precomputed matrix-vector products.  The auto-regressive filter
+//    (lag <= 3) reads only earlier rows and earlier samples of the same row,
+//    so samples with equal x + 4y are independent and one warp sweeps the
+//    template in ~350 wavefront steps.
+//  * grain_blend_kernel — every thread owns one chroma-resolution position
+//    and the (1 << ssx) x (1 << ssy) luma samples it covers.  The noise value
+//    of a sample is evaluated in closed form from the template, the random
+//    offsets of the (at most two) 32-sample blocks that wrote it in each
+//    direction and the 27/17, 17/27 and 23/22 overlap blends, which is exactly
+//    what the reference's materialised noise stripes and noise image hold
+//    (film_grain.rs:599-760).  Chroma is blended first from the un-noised
+//    luma, then luma, as the reference orders it (film_grain.rs:758-828).
+#include "common.cuh"
+#include "av1_spec_tables.h"
+
+namespace av1g {
+
+__constant__ AV1T_GAUSSIAN_SEQUENCE_TYPE c_gauss AV1T_GAUSSIAN_SEQUENCE_DIMS = AV1T_GAUSSIAN_SEQUENCE_INIT;
+
+namespace {
+
+constexpr int LW = 82, LH = 73;
+
+// ---- LFSR jump tables: M^(w * 2^b) for row widths 82 and 44 ---------------
+struct Jumps {
+    uint16_t m[2][7][16];  // [width 82 / 44][bit][column]
+};
+
+constexpr uint16_t mat_apply(const uint16_t* cols, uint16_t v) {
+    uint16_t r = 0;
+    for (int k = 0; k < 16; k++)
+        if ((v >> k) & 1) r ^= cols[k];
+    return r;
+}
+
+constexpr uint16_t lfsr_step(uint16_t r) {
+    unsigned bit = (r ^ (r >> 1) ^ (r >> 3) ^ (r >> 12)) & 1;
+    return (uint16_t)((r >> 1) | (bit << 15));
+}
+
+constexpr Jumps make_jumps() {
+    Jumps j{};
+    const int widths[2] = {LW, 44};
+    for (int wi = 0; wi < 2; wi++) {
+        // M^w by stepping each basis vector w times
+        for (int k = 0; k < 16; k++) {
+            uint16_t v = (uint16_t)(1u << k);
+            for (int s = 0; s < widths[wi]; s++) v = lfsr_step(v);
+            j.m[wi][0][k] = v;
+        }
+        for (int b = 1; b < 7; b++)
+            for (int k = 0; k < 16; k++)
+                j.m[wi][b][k] = mat_apply(j.m[wi][b - 1], j.m[wi][b - 1][k]);
+    }
+    return j;
+}
+
+__constant__ Jumps c_jumps = make_jumps();
+
+__device__ __forceinline__ uint16_t row_state(uint16_t seed, int row, int wi) {
+    uint16_t s = seed;
+    for (int b = 0; b < 7; b++)
+        if ((row >> b) & 1) s = mat_apply(c_jumps.m[wi][b], s);
+    return s;
+}
+
+__device__ __forceinline__ int r2(int x, int n) { return n ? (x + (1 << (n - 1))) >> n : x; }
+
+// scaling_lookup_fill (film_grain.rs:490-540)
+__device__ void scaling_fill(uint8_t* t, int np, const uint8_t* xv, const uint8_t* yv) {
+    if (np == 0) {
+        for (int v = 0; v < 256; v++) t[v] = 0;
+        return;
+    }
+    for (int v = 0; v < xv[0]; v++) t[v] = yv[0];
+    for (int i = 0; i + 1 < np; i++) {
+        int dx = xv[i + 1] - xv[i], dy = yv[i + 1] - yv[i];
+        if (dx <= 0) continue;
+        int delta = dy * ((65536 + (dx >> 1)) / dx);
+        for (int x = 0; x < dx; x++) {
+            int idx = xv[i] + x;
+            if (idx < 256) t[idx] = (uint8_t)clip3(0, 255, yv[i] + ((x * delta + 32768) >> 16));
+        }
+    }
+    for (int v = xv[np - 1]; v < 256; v++) t[v] = yv[np - 1];
+}
+
+// AR filter of one template by one warp: wavefront over t = x + 4y.
+__device__ void ar_luma(int16_t* L, const av1g_film_grain& fg, int gmin, int gmax) {
+    int lane = threadIdx.x & 31, lag = fg.ar_coeff_lag;
+    for (int T = 3 + 4 * 3; T <= (LW - 4) + 4 * (LH - 1); T++) {
+        int ylo = max(3, (T - (LW - 4) + 3) >> 2), yhi = min(LH - 1, (T - 3) >> 2);
+        int y = ylo + lane;
+        if (y <= yhi) {
+            int x = T - 4 * y;
+            int s = 0, pos = 0;
+            for (int dr = -lag; dr <= 0; dr++)
+                for (int dc = -lag; dc <= lag; dc++) {
+                    if (dr == 0 && dc == 0) goto done;
+                    s += L[(y + dr) * LW + x + dc] * (fg.ar_coeffs_y_plus_128[pos] - 128);
+                    pos++;
+                }
+        done:
+            L[y * LW + x] = (int16_t)clip3(gmin, gmax, L[y * LW + x] + r2(s, fg.ar_coeff_shift));
+        }
+        __syncwarp();
+    }
+}
+
+__device__ void ar_chroma(int16_t* C, const int16_t* L, const uint8_t* coef, const av1g_film_grain& fg,
+                          int cw, int ch, int ssx, int ssy, int gmin, int gmax) {
+    int lane = threadIdx.x & 31, lag = fg.ar_coeff_lag;
+    for (int T = 3 + 4 * 3; T <= (cw - 4) + 4 * (ch - 1); T++) {
+        int ylo = max(3, (T - (cw - 4) + 3) >> 2), yhi = min(ch - 1, (T - 3) >> 2);
+        for (int y = ylo + lane; y <= yhi; y += 32) {
+            int x = T - 4 * y;
+            int s = 0, pos = 0;
+            for (int dr = -lag; dr <= 0; dr++)
+                for (int dc = -lag; dc <= lag; dc++) {
+                    int c = coef[pos] - 128;
+                    if (dr == 0 && dc == 0) {
+                        if (fg.num_y_points > 0) {
+                            int lx = ((x - 3) << ssx) + 3, ly = ((y - 3) << ssy) + 3, l = 0;
+                            for (int i = 0; i <= ssy; i++)
+                                for (int j = 0; j <= ssx; j++) l += L[(ly + i) * LW + lx + j];
+                            s += r2(l, ssx + ssy) * c;
+                        }
+                        goto done;
+                    }
+                    s += C[(y + dr) * cw + x + dc] * c;
+                    pos++;
+                }
+        done:
+            C[y * cw + x] = (int16_t)clip3(gmin, gmax, C[y * cw + x] + r2(s, fg.ar_coeff_shift));
+        }
+        __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(128) grain_template_kernel(const FrameDev* __restrict__ frames,
+                                                             const int32_t* __restrict__ starts, int n, int total) {
+    __shared__ int16_t T[3][LH * LW];
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        int f = find_frame(starts, n, t);
+        const FrameDev& F = frames[f];
+        const av1g_film_grain& fg = F.h.film_grain;
+        const int bd = F.h.bit_depth, ssx = F.h.subsampling_x, ssy = F.h.subsampling_y;
+        const int center = 128 << (bd - 8), gmin = -center, gmax = (256 << (bd - 8)) - 1 - center;
+        const int shift = 12 - bd + fg.grain_scale_shift;
+        const int cw = ssx ? 44 : 82, ch = ssy ? 38 : 73;
+        __syncthreads();
+        if (threadIdx.x < 3) {
+            int p = threadIdx.x;
+            uint8_t* lut = F.grain_lut + p * 256;
+            if (p < F.h.num_planes) {
+                if (p == 0 || fg.chroma_scaling_from_luma) scaling_fill(lut, fg.num_y_points, fg.point_y_value, fg.point_y_scaling);
+                else if (p == 1) scaling_fill(lut, fg.num_cb_points, fg.point_cb_value, fg.point_cb_scaling);
+                else scaling_fill(lut, fg.num_cr_points, fg.point_cr_value, fg.point_cr_scaling);
+            } else {
+                for (int v = 0; v < 256; v++) lut[v] = 0;
+            }
+        }
+        // white noise (generate_grain, film_grain.rs:245-300)
+        for (int job = threadIdx.x; job < LH + 2 * ch; job += blockDim.x) {
+            int p = job < LH ? 0 : (job < LH + ch ? 1 : 2);
+            int y = p == 0 ? job : (p == 1 ? job - LH : job - LH - ch);
+            int w = p == 0 ? LW : cw;
+            bool on = p == 0 ? fg.num_y_points > 0
+                             : (p == 1 ? (fg.num_cb_points > 0 || fg.chroma_scaling_from_luma)
+                                       : (fg.num_cr_points > 0 || fg.chroma_scaling_from_luma));
+            uint16_t seed = p == 0 ? fg.grain_seed : (uint16_t)(fg.grain_seed ^ (p == 1 ? 0xb524 : 0x49d8));
+            uint16_t s = on ? row_state(seed, y, (p == 0 || cw == LW) ? 0 : 1) : 0;
+            int16_t* row = &T[p][y * w];
+            for (int x = 0; x < w; x++) {
+                int g = 0;
+                if (on) {
+                    s = lfsr_step(s);
+                    g = c_gauss[(s >> 5) & 2047];
+                }
+                row[x] = (int16_t)r2(g, shift);
+            }
+        }
+        __syncthreads();
+        if (fg.num_y_points > 0 && threadIdx.x < 32) ar_luma(T[0], fg, gmin, gmax);
+        __syncthreads();
+        if (fg.chroma_scaling_from_luma || fg.num_cb_points > 0 || fg.num_cr_points > 0) {
+            int warp = threadIdx.x >> 5;
+            if (warp == 0) ar_chroma(T[1], T[0], fg.ar_coeffs_cb_plus_128, fg, cw, ch, ssx, ssy, gmin, gmax);
+            else if (warp == 1) ar_chroma(T[2], T[0], fg.ar_coeffs_cr_plus_128, fg, cw, ch, ssx, ssy, gmin, gmax);
+        }
+        __syncthreads();
+        int16_t* out = F.grain_tmpl;
+        for (int i = threadIdx.x; i < LH * LW; i += blockDim.x) out[i] = T[0][i];
+        for (int i = threadIdx.x; i < ch * cw; i += blockDim.x) {
+            out[LH * LW + i] = T[1][i];
+            out[2 * LH * LW + i] = T[2][i];
+        }
+        // per-stripe block offsets (add_noise_synthesis, film_grain.rs:604-615)
+        const int w = F.out[0].w, h = F.out[0].h;
+        const int nstripes = ((h + 1) / 2 + 15) / 16, nblocks = F.grain_nblocks;
+        for (int s = threadIdx.x; s < nstripes; s += blockDim.x) {
+            uint16_t st = fg.grain_seed;
+            st ^= (uint16_t)((((unsigned)s * 37 + 178) & 255) << 8);
+            st ^= (uint16_t)(((unsigned)s * 173 + 105) & 255);
+            for (int k = 0; k < nblocks; k++) {
+                st = lfsr_step(st);
+                F.grain_offs[s * nblocks + k] = (uint8_t)(st >> 8);
+            }
+        }
+        (void)w;
+    }
+}
+
+// Noise of plane p at (y, x): the materialised noiseImage of the reference.
+struct NoiseCtx {
+    const int16_t* tmpl;
+    const uint8_t* offs;
+    int nblocks, tw;  // template row width
+    int psx, psy, overlap, gmin, gmax;
+    __device__ int g(int s, int k, int i, int j) const {
+        int o = offs[s * nblocks + k];
+        int ox = o >> 4, oy = o & 15;
+        int pox = psx ? 6 + ox : 9 + ox * 2, poy = psy ? 6 + oy : 9 + oy * 2;
+        return __ldg(&tmpl[(poy + i) * tw + pox + j]);
+    }
+    // value of noise stripe s, row i, column x after the horizontal overlap
+    __device__ int stripe(int s, int i, int x) const {
+        int bs = psx ? 4 : 5;
+        int k = x >> bs, j = x & ((1 << bs) - 1);
+        int v = g(s, k, i, j);
+        if (overlap && k > 0) {
+            if (psx == 0 && j < 2) {
+                int old = g(s, k - 1, i, j + 32);
+                v = j == 0 ? old * 27 + v * 17 : old * 17 + v * 27;
+                v = clip3(gmin, gmax, r2(v, 5));
+            } else if (psx && j == 0) {
+                int old = g(s, k - 1, i, 16);
+                v = clip3(gmin, gmax, r2(old * 23 + v * 22, 5));
+            }
+        }
+        return v;
+    }
+    __device__ int noise(int y, int x) const {
+        int bs = psy ? 4 : 5;
+        int s = y >> bs, i = y & ((1 << bs) - 1);
+        int v = stripe(s, i, x);
+        if (overlap && s > 0) {
+            if (psy == 0 && i < 2) {
+                int old = stripe(s - 1, i + 32, x);
+                v = i == 0 ? old * 27 + v * 17 : old * 17 + v * 27;
+                v = clip3(gmin, gmax, r2(v, 5));
+            } else if (psy && i == 0) {
+                int old = stripe(s - 1, 16, x);
+                v = clip3(gmin, gmax, r2(old * 23 + v * 22, 5));
+            }
+        }
+        return v;
+    }
+};
+
+__device__ __forceinline__ int scale_lut(const uint8_t* lut, int index, int bd) {
+    int shift = bd - 8, x = index >> shift;
+    if (bd == 8 || x >= 255) return lut[x < 255 ? x : 255];
+    int rem = index - (x << shift);
+    int a = lut[x], b = lut[x + 1];
+    return a + r2((b - a) * rem, shift);
+}
+
+constexpr int BR = 8, BC = 256;
+
+__global__ void __launch_bounds__(256) grain_blend_kernel(const FrameDev* __restrict__ frames,
+                                                          const int32_t* __restrict__ starts, int n, int total) {
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        int f = find_frame(starts, n, t);
+        const FrameDev& F = frames[f];
+        const av1g_film_grain& fg = F.h.film_grain;
+        const int bd = F.h.bit_depth, hbd = F.hbd;
+        const int ssx = F.h.num_planes > 1 ? F.h.subsampling_x : 0, ssy = F.h.num_planes > 1 ? F.h.subsampling_y : 0;
+        const int w = F.out[0].w, h = F.out[0].h;
+        const int gw = (w + ssx) >> ssx, gh = (h + ssy) >> ssy;
+        const int ntc = (gw + BC - 1) / BC;
+        int local = t - starts[f];
+        int tr = local / ntc, tc = local % ntc;
+        int xc = tc * BC + threadIdx.x;
+        if (xc >= gw) continue;
+        const int center = 128 << (bd - 8), gmin = -center, gmax = (256 << (bd - 8)) - 1 - center;
+        int minv, maxl, maxc;
+        if (fg.clip_to_restricted_range) {
+            minv = 16 << (bd - 8);
+            maxl = 235 << (bd - 8);
+            maxc = F.h.matrix_coefficients == 0 ? maxl : 240 << (bd - 8);
+        } else {
+            minv = 0;
+            maxl = maxc = (256 << (bd - 8)) - 1;
+        }
+        const int cw = F.h.subsampling_x ? 44 : 82;
+        NoiseCtx nl{F.grain_tmpl, F.grain_offs, F.grain_nblocks, LW, 0, 0, fg.overlap_flag, gmin, gmax};
+        const bool chroma = F.h.num_planes >= 3 &&
+                            (fg.num_cb_points > 0 || fg.num_cr_points > 0 || fg.chroma_scaling_from_luma);
+        for (int yc = tr * BR; yc < min(gh, tr * BR + BR); yc++) {
+            int ly = yc << ssy, lx = xc << ssx;
+            if (chroma) {
+                int lnx = min(lx + 1, w - 1);
+                int y0 = ld_px(F.lr[0], hbd, ly, lx);
+                int avg = ssx ? r2(y0 + ld_px(F.lr[0], hbd, ly, lnx), 1) : y0;
+                for (int p = 1; p <= 2; p++) {
+                    int np_ = p == 1 ? fg.num_cb_points : fg.num_cr_points;
+                    if (!(np_ > 0 || fg.chroma_scaling_from_luma)) {
+                        st_px(F.out[p], hbd, yc, xc, ld_px(F.lr[p], hbd, yc, xc));
+                        continue;
+                    }
+                    int orig = ld_px(F.lr[p], hbd, yc, xc);
+                    int merged;
+                    if (fg.chroma_scaling_from_luma) {
+                        merged = avg;
+                    } else {
+                        int lm = p == 1 ? fg.cb_luma_mult : fg.cr_luma_mult;
+                        int m = p == 1 ? fg.cb_mult : fg.cr_mult;
+                        int off = p == 1 ? fg.cb_offset : fg.cr_offset;
+                        int comb = avg * (lm - 128) + orig * (m - 128);
+                        merged = clip3(0, (1 << bd) - 1, (comb >> 6) + (off - 256) * (1 << (bd - 8)));
+                    }
+                    NoiseCtx nc{F.grain_tmpl + p * LH * LW, F.grain_offs, F.grain_nblocks, cw,
+                                F.h.subsampling_x, F.h.subsampling_y, fg.overlap_flag, gmin, gmax};
+                    int nz = r2(scale_lut(F.grain_lut + p * 256, merged, bd) * nc.noise(yc, xc), fg.grain_scaling);
+                    st_px(F.out[p], hbd, yc, xc, clip3(minv, maxc, orig + nz));
+                }
+            } else if (F.h.num_planes >= 3) {
+                for (int p = 1; p <= 2; p++) st_px(F.out[p], hbd, yc, xc, ld_px(F.lr[p], hbd, yc, xc));
+            }
+            for (int dy = 0; dy <= ssy; dy++)
+                for (int dx = 0; dx <= ssx; dx++) {
+                    int y = ly + dy, x = lx + dx;
+                    if (y >= h || x >= w) continue;
+                    int orig = ld_px(F.lr[0], hbd, y, x);
+                    int o = orig;
+                    if (fg.num_y_points > 0) {
+                        int nz = r2(scale_lut(F.grain_lut, orig, bd) * nl.noise(y, x), fg.grain_scaling);
+                        o = clip3(minv, maxl, orig + nz);
+                    }
+                    st_px(F.out[0], hbd, y, x, o);
+                }
+        }
+    }
+}
+
+}  // namespace
+
+int tiles_grain_blend(const FrameDev& f) {
+    int ssx = f.h.num_planes > 1 ? f.h.subsampling_x : 0, ssy = f.h.num_planes > 1 ? f.h.subsampling_y : 0;
+    int gw = (f.out[0].w + ssx) >> ssx, gh = (f.out[0].h + ssy) >> ssy;
+    return ((gh + BR - 1) / BR) * ((gw + BC - 1) / BC);
+}
+
+void launch_grain(const FrameDev* frames, const int32_t* starts_tmpl, const int32_t* starts_blend, int n,
+                  int total_tmpl, int total_blend, cudaStream_t s) {
+    if (total_tmpl > 0) grain_template_kernel<<<total_tmpl, 128, 0, s>>>(frames, starts_tmpl, n, total_tmpl);
+    if (total_blend > 0) {
+        int grid = total_blend < kSMs * 8 ? total_blend : kSMs * 8;
+        grain_blend_kernel<<<grid, 256, 0, s>>>(frames, starts_blend, n, total_blend);
+    }
+}
+
+}  // namespace av1g

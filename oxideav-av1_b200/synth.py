@@ -1,0 +1,308 @@
+"""Seeded synthetic post-filter frames (the decoder's pre-parsed symbol state).
+
+The reference measures its post-filter path on encoder-produced streams that
+cannot be produced in this environment (its Rust encoder does not build here),
+so the workload is generated directly at the seam the engine consumes: a
+frame's reconstructed planes at the padded mi extent plus the per-mi decode
+grids and the frame header fields the §7.14-§7.18 stages read.
+
+Shapes and value distributions follow the post-filter micro-benchmark
+configuration (1920x1080 4:2:0, 8-bit and a 10-bit variant):
+  * planes: a 16x16 uniform random field, bilinearly upsampled, plus uniform
+    noise in [-12, 12] (scaled by 2^(bitdepth-8)), clipped to the sample range;
+  * a random legal partition of every 64x64 superblock (NONE / HORZ / VERT /
+    SPLIT / HORZ_4 / VERT_4), per block a transform size from the legal set
+    (Max_Tx_Size_Rect split 0..2 times), intra/inter, skip, modes, references,
+    segment ids and delta-LF values;
+  * deblock levels uniform 0..63 with sharpness 0..7; per-64x64 CDEF indices
+    uniform over 1 << cdef_bits = 8 strength sets with primary 0..15,
+    secondary {0,1,2,4}, damping 3..6;
+  * 64x64 restoration units, each Wiener (taps uniform within the spec
+    coefficient bounds, chroma tap 0 = 0) or self-guided (set 0..15, projection
+    weights within the spec bounds).
+Superres and film grain are off in that configuration; the generator can turn
+them on for parity cases.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+
+# (w4, h4) in 4x4 units -> BLOCK_* ordinal (spec §3 block size order)
+BLOCK_OF = {(1, 1): 0, (1, 2): 1, (2, 1): 2, (2, 2): 3, (2, 4): 4, (4, 2): 5, (4, 4): 6, (4, 8): 7, (8, 4): 8,
+            (8, 8): 9, (8, 16): 10, (16, 8): 11, (16, 16): 12, (16, 32): 13, (32, 16): 14, (32, 32): 15,
+            (1, 4): 16, (4, 1): 17, (2, 8): 18, (8, 2): 19, (4, 16): 20, (16, 4): 21}
+# Max_Tx_Size_Rect[BLOCK_*] and Split_Tx_Size[TX_*] (spec additional tables)
+MAX_TX_RECT = [0, 5, 6, 1, 7, 8, 2, 9, 10, 3, 11, 12, 4, 4, 4, 4, 13, 14, 15, 16, 17, 18]
+SPLIT_TX = [0, 0, 1, 2, 3, 0, 0, 1, 1, 2, 2, 3, 3, 5, 6, 7, 8, 9, 10]
+
+WIENER_MIN = [-5, -23, -17]
+WIENER_MAX = [10, 8, 46]
+SGR_R = [(2, 1), (2, 1), (2, 1), (2, 1), (2, 1), (2, 1), (2, 1), (2, 1), (2, 1), (2, 1), (0, 1), (0, 1), (0, 1),
+         (0, 1), (2, 0), (2, 0)]
+
+LR_DTYPE = np.dtype([("type", np.uint8), ("sgr_set", np.uint8), ("wiener", np.int8, (2, 3)),
+                     ("sgr_xqd", np.int16, (2,))], align=True)
+assert LR_DTYPE.itemsize == C.sizeof(abi.LrUnit)
+
+
+def _lerp_weights(n):
+    pos = np.linspace(0, 15, n)
+    i0 = np.minimum(pos.astype(np.int64), 14)
+    return i0, pos - i0
+
+
+def _field(rng, h, w, maxv):
+    """16x16 uniform field bilinearly upsampled to h x w."""
+    f = rng.uniform(0, maxv, size=(16, 16))
+    xi, xf = _lerp_weights(w)
+    rows = f[:, xi] * (1 - xf) + f[:, xi + 1] * xf
+    yi, yf = _lerp_weights(h)
+    return rows[yi] * (1 - yf)[:, None] + rows[yi + 1] * yf[:, None]
+
+
+def _plane(rng, h, w, bd):
+    maxv = (1 << bd) - 1
+    base = _field(rng, h, w, maxv)
+    noise = rng.integers(-12, 13, size=(h, w)) * (1 << (bd - 8))
+    v = np.clip(np.rint(base) + noise, 0, maxv)
+    return v.astype(np.uint8 if bd == 8 else np.uint16)
+
+
+class SyntheticFrame:
+    """One frame's post-filter inputs: header, mi grids, CDEF indices, LR units, planes."""
+
+    def __init__(self):
+        self.hdr = abi.FrameHeader()
+        self.grid = {}
+        self.cdef_idx = None
+        self.lr_units = [None, None, None]
+        self.recon = []
+
+    @property
+    def hbd(self):
+        return self.hdr.bit_depth > 8
+
+    def plane_dims(self, p):
+        """padded (height, width) of plane p."""
+        h = self.hdr
+        sx = h.subsampling_x if p else 0
+        sy = h.subsampling_y if p else 0
+        return (h.mi_rows * 4) >> sy, (h.mi_cols * 4) >> sx
+
+    def out_dims(self, p):
+        """cropped (height, width) of output plane p."""
+        h = self.hdr
+        sx = h.subsampling_x if p else 0
+        sy = h.subsampling_y if p else 0
+        return (h.frame_height + sy) >> sy, (h.upscaled_width + sx) >> sx
+
+    def lr_grid(self, p):
+        h = self.hdr
+        sx = h.subsampling_x if p else 0
+        sy = h.subsampling_y if p else 0
+        us = h.lr_unit_size[p]
+        rows = _count_units(us, (h.frame_height + (1 << sy >> 1)) >> sy)
+        cols = _count_units(us, (h.upscaled_width + (1 << sx >> 1)) >> sx)
+        return rows, cols
+
+
+def _count_units(us, size):
+    return max((size + (us >> 1)) // us, 1)
+
+
+def _partition(rng, grid, r, c, n4, mi_rows, mi_cols, depth_bias):
+    """Random legal partition of a square block of n4 x n4 4x4 units at (r, c)."""
+    if r >= mi_rows or c >= mi_cols:
+        return
+    opts = ["NONE"]
+    if n4 > 1:
+        opts += ["HORZ", "VERT", "SPLIT"]
+        if n4 >= 4:
+            opts += ["HORZ_4", "VERT_4"]
+    w = np.array([1.0 if o == "NONE" else (depth_bias if o == "SPLIT" else 0.5) for o in opts])
+    # blocks crossing the frame edge split like the spec's forced partitions
+    if r + n4 > mi_rows or c + n4 > mi_cols:
+        if n4 > 1:
+            opts, w = ["SPLIT"], np.array([1.0])
+    o = opts[rng.choice(len(opts), p=w / w.sum())]
+    if o == "NONE":
+        _leaf(rng, grid, r, c, n4, n4)
+    elif o == "HORZ":
+        _leaf(rng, grid, r, c, n4, n4 // 2)
+        _leaf(rng, grid, r + n4 // 2, c, n4, n4 // 2)
+    elif o == "VERT":
+        _leaf(rng, grid, r, c, n4 // 2, n4)
+        _leaf(rng, grid, r, c + n4 // 2, n4 // 2, n4)
+    elif o == "HORZ_4":
+        for k in range(4):
+            _leaf(rng, grid, r + k * n4 // 4, c, n4, n4 // 4)
+    elif o == "VERT_4":
+        for k in range(4):
+            _leaf(rng, grid, r, c + k * n4 // 4, n4 // 4, n4)
+    else:
+        h = n4 // 2
+        for dr in (0, h):
+            for dc in (0, h):
+                _partition(rng, grid, r + dr, c + dc, h, mi_rows, mi_cols, depth_bias * 0.85)
+
+
+def _leaf(rng, grid, r, c, w4, h4):
+    bs = BLOCK_OF[(w4, h4)]
+    tx = MAX_TX_RECT[bs]
+    for _ in range(rng.integers(0, 3)):
+        tx = SPLIT_TX[tx]
+    inter = rng.random() < 0.5
+    sl = (slice(r, r + h4), slice(c, c + w4))
+    g = grid
+    g["mi_size"][sl] = bs
+    g["skip"][sl] = rng.random() < 0.3
+    g["is_inter"][sl] = inter
+    g["ref_frame0"][sl] = rng.integers(1, 8) if inter else 0
+    g["y_mode"][sl] = rng.integers(14, 26) if inter else rng.integers(0, 13)
+    g["segment_id"][sl] = rng.integers(0, 8) if g["_seg"] else 0
+    g["delta_lf"][sl] = rng.integers(-6, 7, size=4) if g["_dlf"] else 0
+    g["tx_size"][sl] = tx
+    g["inter_tx_size"][sl] = tx
+
+
+def make_frame(seed, width=1920, height=1080, bit_depth=8, ssx=1, ssy=1, mono=False, superres_denom=8,
+               film_grain=False, lr_unit=64, lr_uv_shift=0, lr_types=(3, 3, 3), lr_none_frac=0.0, deblock=True,
+               cdef=True, lr=True, segmentation=True, delta_lf=True):
+    rng = np.random.default_rng(seed)
+    f = SyntheticFrame()
+    h = f.hdr
+    up_w = width
+    fw = (up_w * 8 + superres_denom // 2) // superres_denom if superres_denom != 8 else up_w
+    h.frame_width, h.frame_height, h.upscaled_width = fw, height, up_w
+    h.mi_cols = 2 * ((fw + 7) >> 3)
+    h.mi_rows = 2 * ((height + 7) >> 3)
+    h.bit_depth = bit_depth
+    h.num_planes = 1 if mono else 3
+    h.subsampling_x, h.subsampling_y = (1, 1) if mono else (ssx, ssy)
+    h.matrix_coefficients = int(rng.integers(0, 3))
+    h.use_superres = 1 if superres_denom != 8 else 0
+    h.enable_cdef = 1 if cdef else 0
+    # §5.9.11 loop filter
+    if deblock:
+        for i in range(4):
+            h.lf_level[i] = int(rng.integers(0, 64))
+        h.lf_level[0] = max(h.lf_level[0], 1)
+    h.lf_sharpness = int(rng.integers(0, 8))
+    h.lf_delta_enabled = int(rng.random() < 0.7)
+    h.delta_lf_multi = int(rng.random() < 0.5)
+    for i, d in enumerate([1, 0, 0, 0, -1, 0, -1, -1]):
+        h.lf_ref_deltas[i] = int(np.clip(d + rng.integers(-3, 4), -63, 63))
+    h.lf_mode_deltas[0] = int(rng.integers(-3, 4))
+    h.lf_mode_deltas[1] = int(rng.integers(-3, 4))
+    if segmentation:
+        for s in range(8):
+            for i in range(4):
+                if rng.random() < 0.3:
+                    h.seg_lf_active[s][i] = 1
+                    h.seg_lf_data[s][i] = int(rng.integers(-20, 21))
+    # §5.9.19 cdef
+    h.cdef_short_circuited = 0
+    h.cdef_damping = int(rng.integers(3, 7))
+    h.cdef_bits = 3
+    for i in range(8):
+        h.cdef_y_pri[i] = int(rng.integers(0, 16))
+        h.cdef_y_sec[i] = int(rng.choice([0, 1, 2, 4]))
+        h.cdef_uv_pri[i] = int(rng.integers(0, 16))
+        h.cdef_uv_sec[i] = int(rng.choice([0, 1, 2, 4]))
+    # §5.9.20 restoration
+    h.uses_lr = 1 if lr else 0
+    for p in range(3):
+        h.lr_type[p] = lr_types[p] if lr else 0
+        h.lr_unit_size[p] = lr_unit if p == 0 else lr_unit >> lr_uv_shift
+    # grids
+    mr, mc = h.mi_rows, h.mi_cols
+    g = {
+        "mi_size": np.zeros((mr, mc), np.uint8), "skip": np.zeros((mr, mc), np.uint8),
+        "is_inter": np.zeros((mr, mc), np.uint8), "ref_frame0": np.zeros((mr, mc), np.int8),
+        "y_mode": np.zeros((mr, mc), np.uint8), "segment_id": np.zeros((mr, mc), np.int8),
+        "delta_lf": np.zeros((mr, mc, 4), np.int8), "tx_size": np.zeros((mr, mc), np.uint8),
+        "inter_tx_size": np.zeros((mr, mc), np.uint8), "_seg": segmentation, "_dlf": delta_lf,
+    }
+    for r in range(0, mr, 16):
+        for c in range(0, mc, 16):
+            _partition(rng, g, r, c, 16, mr, mc, 1.6)
+    del g["_seg"], g["_dlf"]
+    f.grid = g
+    cr, cc = (mr + 15) // 16, (mc + 15) // 16
+    idx = rng.integers(0, 8, size=(cr, cc)).astype(np.int8)
+    idx[rng.random((cr, cc)) < 0.05] = -1
+    f.cdef_idx = idx
+    for p in range(h.num_planes):
+        rows, cols = f.lr_grid(p)
+        u = np.zeros((rows, cols), LR_DTYPE)
+        kinds = rng.random((rows, cols))
+        for i in range(rows):
+            for j in range(cols):
+                k = kinds[i, j]
+                if k < lr_none_frac:
+                    continue
+                if k < lr_none_frac + (1 - lr_none_frac) / 2:
+                    u[i, j]["type"] = 1
+                    for ps in range(2):
+                        for t in range(3):
+                            v = int(rng.integers(WIENER_MIN[t], WIENER_MAX[t] + 1))
+                            u[i, j]["wiener"][ps, t] = 0 if (p > 0 and t == 0) else v
+                else:
+                    u[i, j]["type"] = 2
+                    s = int(rng.integers(0, 16))
+                    u[i, j]["sgr_set"] = s
+                    r0, r1 = SGR_R[s]
+                    w0 = int(rng.integers(-96, 32)) if r0 else 0
+                    w1 = int(rng.integers(-32, 96))
+                    if r1 == 0:
+                        w1 = int(np.clip(128 - w0, -32, 95))
+                    u[i, j]["sgr_xqd"] = (w0, w1)
+        f.lr_units[p] = u
+    for p in range(h.num_planes):
+        ph, pw = f.plane_dims(p)
+        f.recon.append(_plane(rng, ph, pw, bit_depth))
+    if film_grain:
+        _film_grain(rng, h.film_grain, bit_depth, mono)
+    return f
+
+
+def _points(rng, n, maxn):
+    n = min(n, maxn)
+    xs = np.sort(rng.choice(np.arange(256), size=n, replace=False)) if n else np.array([], int)
+    ys = rng.integers(0, 256, size=n)
+    return xs, ys
+
+
+def _film_grain(rng, fg, bd, mono):
+    fg.apply_grain = 1
+    fg.grain_seed = int(rng.integers(0, 65536))
+    ny = int(rng.integers(1, 15))
+    xs, ys = _points(rng, ny, 14)
+    fg.num_y_points = len(xs)
+    for i in range(len(xs)):
+        fg.point_y_value[i], fg.point_y_scaling[i] = int(xs[i]), int(ys[i])
+    fg.chroma_scaling_from_luma = 0 if mono else int(rng.random() < 0.25)
+    if not mono and not fg.chroma_scaling_from_luma:
+        for name in ("cb", "cr"):
+            n = int(rng.integers(0, 11))
+            xs, ys = _points(rng, n, 10)
+            setattr(fg, f"num_{name}_points", len(xs))
+            vals, scs = getattr(fg, f"point_{name}_value"), getattr(fg, f"point_{name}_scaling")
+            for i in range(len(xs)):
+                vals[i], scs[i] = int(xs[i]), int(ys[i])
+    fg.grain_scaling = int(rng.integers(8, 12))
+    fg.ar_coeff_lag = int(rng.integers(0, 4))
+    for i in range(24):
+        fg.ar_coeffs_y_plus_128[i] = int(128 + rng.integers(-24, 25))
+    for i in range(25):
+        fg.ar_coeffs_cb_plus_128[i] = int(128 + rng.integers(-24, 25))
+        fg.ar_coeffs_cr_plus_128[i] = int(128 + rng.integers(-24, 25))
+    fg.ar_coeff_shift = int(rng.integers(6, 10))
+    fg.grain_scale_shift = int(rng.integers(0, 4))
+    fg.cb_mult, fg.cb_luma_mult = int(rng.integers(0, 256)), int(rng.integers(0, 256))
+    fg.cr_mult, fg.cr_luma_mult = int(rng.integers(0, 256)), int(rng.integers(0, 256))
+    fg.cb_offset, fg.cr_offset = int(rng.integers(0, 512)), int(rng.integers(0, 512))
+    fg.overlap_flag = int(rng.random() < 0.7)
+    fg.clip_to_restricted_range = int(rng.random() < 0.5)
