@@ -1078,3 +1078,58 @@ int ora_postfilter_frame(const av1g_frame_header* h, const av1g_mi_grid* grid,
         for (size_t i = 0; i < (size_t)o[p].rows * o[p].cols; i++) out[p][i] = clip3(0, maxv, out[p][i]);
     return 0;
 }
+
+/* ===================================================================== */
+/* Internals exposed for the known-answer tests that restate the         */
+/* reference's module unit tests (loop_filter.rs, cdef.rs,               */
+/* loop_restoration.rs tests).                                           */
+/* ===================================================================== */
+
+void ora_lf_strength(const av1g_frame_header* hdr, const av1g_mi_grid* grid, int row, int col, int plane,
+                     int pass, int32_t out[4]) {
+    lf_ctx c = {hdr, grid};
+    lf_strength s = filter_strength(&c, row, col, plane, pass);
+    out[0] = s.lvl;
+    out[1] = s.limit;
+    out[2] = s.blimit;
+    out[3] = s.thresh;
+}
+
+int ora_lf_filter_size(int tx, int prev_tx, int pass, int plane) {
+    int base = pass == 0 ? (TXW[tx] < TXW[prev_tx] ? TXW[tx] : TXW[prev_tx])
+                         : (TXH[tx] < TXH[prev_tx] ? TXH[tx] : TXH[prev_tx]);
+    int cap = plane == 0 ? 16 : 8;
+    return base < cap ? base : cap;
+}
+
+void ora_lf_narrow(ora_plane* p, int x, int y, int dx, int dy, int hev, int bd) {
+    narrow_filter(p, x, y, dx, dy, hev, bd);
+}
+
+void ora_lf_wide(ora_plane* p, int x, int y, int plane, int dx, int dy, int log2_size) {
+    wide_filter(p, x, y, plane, dx, dy, log2_size);
+}
+
+int ora_cdef_constrain(int diff, int threshold, int damping) { return constrain(diff, threshold, damping); }
+
+void ora_cdef_direction(const av1g_frame_header* hdr, const ora_plane* p0, int r, int c, int32_t out[2]) {
+    int d, v;
+    cdef_direction(hdr, p0, r, c, &d, &v);
+    out[0] = d;
+    out[1] = v;
+}
+
+int ora_lr_count_units(int unit_size, int frame_size) { return count_units(unit_size, frame_size); }
+
+void ora_lr_geometry(const av1g_frame_header* hdr, int plane, int row, int col, int32_t out[10]) {
+    lr_geom g = lr_geometry(hdr, plane, row, col);
+    int32_t v[10] = {g.unit_row, g.unit_col, g.x, g.y, g.w, g.h, g.stripe_start, g.stripe_end, g.plane_end_x,
+                     g.plane_end_y};
+    memcpy(out, v, sizeof v);
+}
+
+int ora_lr_source_sample(const av1g_frame_header* hdr, int plane, int row, int col, const ora_plane* curr,
+                         const ora_plane* cdef, int x, int y) {
+    lr_geom g = lr_geometry(hdr, plane, row, col);
+    return source_sample(curr, cdef, x, y, &g);
+}

@@ -45,10 +45,17 @@ av1g_status cuda_fail(cudaError_t e, const char* what) {
 
 int r2u(int x, int n) { return n ? (x + (1 << (n - 1))) >> n : x; }
 
-PlaneDev to_dev(const av1g_plane& p) { return PlaneDev{(uint8_t*)p.data, p.stride, p.width, p.height}; }
+// The kernels see a plane at exactly the extent the reference's buffer has
+// (the padded mi extent, or UpscaledWidth x FrameHeight after superres): the
+// CDEF availability test and every clamp are relative to that extent, so a
+// caller's larger allocation must not widen it.
+PlaneDev to_dev(const av1g_plane& p, int w, int h) { return PlaneDev{(uint8_t*)p.data, p.stride, w, h}; }
 
+// Planes must start on a 16-byte boundary with a stride that is a multiple
+// of 16 bytes: the kernels move samples with 4- and 8-byte vector accesses.
 bool plane_ok(const av1g_plane& p, int w, int h, int bps) {
-    return p.data && p.width >= w && p.height >= h && p.stride >= w * bps;
+    return p.data && ((uintptr_t)p.data & 15) == 0 && (p.stride & 15) == 0 && p.width >= w && p.height >= h &&
+           p.stride >= w * bps;
 }
 
 int count_units(int us, int sz) {
@@ -102,18 +109,18 @@ av1g_status prepare_frame(const av1g_frame_job& j, FrameDev& F) {
         return fail(AV1G_EINVAL, "mi grid incomplete for deblock");
     if (F.do_stage[ST_CDEF] && !j.cdef_idx) return fail(AV1G_EINVAL, "cdef_idx missing");
     for (int p = 0; p < np; p++) {
-        F.recon[p] = to_dev(j.recon[p]);
+        F.recon[p] = to_dev(j.recon[p], pw[p], ph[p]);
         bool deb = F.do_stage[ST_DEBLOCK] && (p == 0 || h.lf_level[1 + p] != 0);
         if (deb && !plane_ok(j.deblocked[p], pw[p], ph[p], bps)) return fail(AV1G_EINVAL, "deblocked plane %d", p);
-        F.deb[p] = deb ? to_dev(j.deblocked[p]) : F.recon[p];
+        F.deb[p] = deb ? to_dev(j.deblocked[p], pw[p], ph[p]) : F.recon[p];
         if (F.do_stage[ST_CDEF] && !plane_ok(j.cdef[p], pw[p], ph[p], bps)) return fail(AV1G_EINVAL, "cdef plane %d", p);
-        F.cdef[p] = F.do_stage[ST_CDEF] ? to_dev(j.cdef[p]) : F.deb[p];
+        F.cdef[p] = F.do_stage[ST_CDEF] ? to_dev(j.cdef[p], pw[p], ph[p]) : F.deb[p];
         if (F.do_stage[ST_SUPERRES]) {
             if (!plane_ok(j.up_cdef[p], uw[p], fh[p], bps)) return fail(AV1G_EINVAL, "up_cdef plane %d", p);
-            F.upcdef[p] = to_dev(j.up_cdef[p]);
+            F.upcdef[p] = to_dev(j.up_cdef[p], uw[p], fh[p]);
             if (F.do_stage[ST_LR]) {
                 if (!plane_ok(j.up_deblocked[p], uw[p], fh[p], bps)) return fail(AV1G_EINVAL, "up_deblocked plane %d", p);
-                F.updeb[p] = to_dev(j.up_deblocked[p]);
+                F.updeb[p] = to_dev(j.up_deblocked[p], uw[p], fh[p]);
             } else {
                 F.updeb[p] = F.deb[p];
             }
@@ -124,9 +131,11 @@ av1g_status prepare_frame(const av1g_frame_job& j, FrameDev& F) {
         bool lr = F.do_stage[ST_LR] && h.lr_type[p] != 0;
         if (lr) {
             if (!plane_ok(j.lr[p], uw[p], fh[p], bps)) return fail(AV1G_EINVAL, "lr plane %d", p);
-            if (h.lr_unit_size[p] < 32 || h.lr_unit_size[p] > 256 || (h.lr_unit_size[p] & (h.lr_unit_size[p] - 1)))
-                return fail(AV1G_EINVAL, "lr unit size %d", h.lr_unit_size[p]);
-            F.lr[p] = to_dev(j.lr[p]);
+            // LoopRestorationSize: 64..256 for luma, halved for 4:2:0 chroma (§5.9.20)
+            int umin = 64 >> (p ? ssy : 0);
+            if (h.lr_unit_size[p] < umin || h.lr_unit_size[p] > 256 || (h.lr_unit_size[p] & (h.lr_unit_size[p] - 1)))
+                return fail(AV1G_EINVAL, "lr unit size %d for plane %d", h.lr_unit_size[p], p);
+            F.lr[p] = to_dev(j.lr[p], uw[p], fh[p]);
             F.lr_units[p] = j.lr_units[p];
             F.lr_unit_rows[p] = count_units(h.lr_unit_size[p], fh[p]);
             F.lr_unit_cols[p] = count_units(h.lr_unit_size[p], uw[p]);
@@ -137,7 +146,7 @@ av1g_status prepare_frame(const av1g_frame_job& j, FrameDev& F) {
         F.lr[p].h = fh[p];
         if (F.do_stage[ST_GRAIN]) {
             if (!plane_ok(j.out[p], uw[p], fh[p], bps)) return fail(AV1G_EINVAL, "out plane %d", p);
-            F.out[p] = to_dev(j.out[p]);
+            F.out[p] = to_dev(j.out[p], uw[p], fh[p]);
             F.out[p].w = uw[p];
             F.out[p].h = fh[p];
         } else {
@@ -200,25 +209,42 @@ av1g_status run(const av1g_frame_job* jobs, int n, int stage_mask, int mode, voi
     size_t off_starts = ((sizeof(FrameDev) * n) + 255) & ~(size_t)255;
     size_t off_pf = off_starts + sizeof(int32_t) * NS * (n + 1);
     size_t off_scratch = (off_pf + sizeof(int32_t) * n * NS * 2 + 255) & ~(size_t)255;
+    // per-frame scratch: deblock cell codes, film grain templates / LUTs / offsets
     size_t scratch = 0;
-    std::vector<size_t> scratch_off(n, 0);
-    if (stage_mask & (1 << ST_GRAIN))
-        for (int i = 0; i < n; i++)
-            if (b.frames[i].do_stage[ST_GRAIN]) {
-                scratch_off[i] = off_scratch + scratch;
-                scratch += grain_scratch_bytes(b.frames[i]);
-            }
+    std::vector<size_t> lf_off(n, 0), grain_off(n, 0);
+    int max_cells = 0;
+    for (int i = 0; i < n; i++) {
+        const FrameDev& F = b.frames[i];
+        if ((stage_mask & (1 << ST_DEBLOCK)) && F.do_stage[ST_DEBLOCK]) {
+            int cells = cells_deblock(F);
+            max_cells = cells > max_cells ? cells : max_cells;
+            lf_off[i] = off_scratch + scratch;
+            scratch += ((size_t)cells * 2 + 255) & ~(size_t)255;
+        }
+        if ((stage_mask & (1 << ST_GRAIN)) && F.do_stage[ST_GRAIN]) {
+            grain_off[i] = off_scratch + scratch;
+            scratch += grain_scratch_bytes(F);
+        }
+    }
     size_t total_bytes = off_scratch + scratch;
     uint8_t* dev = nullptr;
     cudaError_t e = cudaMallocAsync((void**)&dev, total_bytes, s);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
-    for (int i = 0; i < n; i++)
-        if (scratch_off[i]) {
-            FrameDev& F = b.frames[i];
-            F.grain_tmpl = (int16_t*)(dev + scratch_off[i]);
-            F.grain_lut = (uint8_t*)(dev + scratch_off[i] + 3 * 73 * 82 * 2);
+    for (int i = 0; i < n; i++) {
+        FrameDev& F = b.frames[i];
+        if (lf_off[i]) {
+            uint16_t* c = (uint16_t*)(dev + lf_off[i]);
+            for (int p = 0; p < F.h.num_planes; p++) {
+                F.lf_codes[p] = c;
+                c += (F.recon[p].w >> 2) * (F.recon[p].h >> 2);
+            }
+        }
+        if (grain_off[i]) {
+            F.grain_tmpl = (int16_t*)(dev + grain_off[i]);
+            F.grain_lut = (uint8_t*)(dev + grain_off[i] + 3 * 73 * 82 * 2);
             F.grain_offs = F.grain_lut + 768;
         }
+    }
     std::vector<uint8_t> host(off_scratch, 0);
     memcpy(host.data(), b.frames.data(), sizeof(FrameDev) * n);
     int32_t* hs = (int32_t*)(host.data() + off_starts);
@@ -246,9 +272,9 @@ av1g_status run(const av1g_frame_job* jobs, int n, int stage_mask, int mode, voi
     const int32_t* dpf = (const int32_t*)(dev + off_pf);
     int nl = 0;
     auto launch_stage = [&](int st, const FrameDev* fr, const int32_t* starts, const int32_t* starts_tmpl, int nn,
-                            int total, int total_tmpl) {
+                            int total, int total_tmpl, int cells) {
         switch (st) {
-            case ST_DEBLOCK: if (total) { launch_deblock(fr, starts, nn, total, s); nl++; } break;
+            case ST_DEBLOCK: if (total) { launch_deblock(fr, starts, nn, total, cells, s); nl += 2; } break;
             case ST_CDEF: if (total) { launch_cdef(fr, starts, nn, total, s); nl++; } break;
             case ST_SUPERRES: if (total) { launch_superres(fr, starts, nn, total, s); nl++; } break;
             case ST_LR: if (total) { launch_lr(fr, starts, nn, total, s); nl++; } break;
@@ -261,11 +287,12 @@ av1g_status run(const av1g_frame_job* jobs, int n, int stage_mask, int mode, voi
     for (int st = 0; st < ST_COUNT; st++) {
         if (!(stage_mask & (1 << st))) continue;
         if (mode == AV1G_MODE_BATCHED) {
-            launch_stage(st, dframes, ds + st * (n + 1), ds + ST_COUNT * (n + 1), n, totals[st], totals[ST_COUNT]);
+            launch_stage(st, dframes, ds + st * (n + 1), ds + ST_COUNT * (n + 1), n, totals[st], totals[ST_COUNT],
+                         max_cells);
         } else {
             for (int i = 0; i < n; i++)
                 launch_stage(st, dframes + i, dpf + (i * NS + st) * 2, dpf + (i * NS + ST_COUNT) * 2, 1,
-                             hpf[(i * NS + st) * 2 + 1], hpf[(i * NS + ST_COUNT) * 2 + 1]);
+                             hpf[(i * NS + st) * 2 + 1], hpf[(i * NS + ST_COUNT) * 2 + 1], cells_deblock(b.frames[i]));
         }
     }
     e = cudaGetLastError();

@@ -42,6 +42,8 @@ struct FrameDev {
     PlaneDev lr[3];        // LR output (the reference payload, cropped view)
     PlaneDev out[3];       // film grain output
     int32_t do_stage[ST_COUNT];
+    // deblock scratch: per-4x4-cell edge codes of each plane
+    uint16_t* lf_codes[3];
     // film grain scratch: templates, scaling LUTs, per-stripe offsets
     int16_t* grain_tmpl;   // 3 x 73 x 82
     uint8_t* grain_lut;    // 3 x 256
@@ -80,7 +82,8 @@ __device__ __forceinline__ void st_px(const PlaneDev& P, int hbd, int y, int x, 
 // Stage launchers (one per .cu file).  Each takes the batch's device
 // FrameDev array, the stage's tile-start array (n+1 entries, device) and the
 // total tile count.
-void launch_deblock(const FrameDev* frames, const int32_t* starts, int n, int total, cudaStream_t s);
+void launch_deblock(const FrameDev* frames, const int32_t* starts, int n, int total, int max_cells,
+                    cudaStream_t s);
 void launch_cdef(const FrameDev* frames, const int32_t* starts, int n, int total, cudaStream_t s);
 void launch_superres(const FrameDev* frames, const int32_t* starts, int n, int total, cudaStream_t s);
 void launch_lr(const FrameDev* frames, const int32_t* starts, int n, int total, cudaStream_t s);
@@ -89,6 +92,7 @@ void launch_grain(const FrameDev* frames, const int32_t* starts_tmpl, const int3
 
 // Host-side tile counts (must match the kernels' tile decomposition).
 int tiles_deblock(const FrameDev& f);
+int cells_deblock(const FrameDev& f);  // 4x4 cells over all planes (deblock scratch: 2 bytes each)
 int tiles_cdef(const FrameDev& f);
 int tiles_superres(const FrameDev& f);
 int tiles_lr(const FrameDev& f);

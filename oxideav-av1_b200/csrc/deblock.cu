@@ -118,14 +118,66 @@ __device__ uint32_t edge_param(const FrameDev& F, int plane, int pass, int cy, i
     if (lvl == 0) return 0;
     int base = pass == 0 ? min((int)c_txw[tx], (int)c_txw[ptx]) : min((int)c_txh[tx], (int)c_txh[ptx]);
     int fsize = min(base, plane == 0 ? 16 : 8);
-    int sh = h.lf_sharpness > 4 ? 2 : (h.lf_sharpness > 0 ? 1 : 0);
-    int limit = h.lf_sharpness > 0 ? clip3(1, 9 - h.lf_sharpness, lvl >> sh) : max(lvl >> sh, 1);
+    // one byte: filter length class (1: 4, 2: 8 or chroma 6, 3: 16) << 6 | lvl (1..63)
+    return (uint32_t)((fsize == 4 ? 1 : (fsize == 8 ? 2 : 3)) << 6) | (uint32_t)lvl;
+}
+
+// Unpacks a cell code into filter length | limit << 8 | blimit << 16 |
+// thresh << 24 (adaptive_filter_strength, loop_filter.rs:500-525).
+__device__ __forceinline__ uint32_t decode_code(uint32_t code, int sharp) {
+    if (code == 0) return 0;
+    int lvl = code & 63, fsc = code >> 6;
+    int fsize = fsc == 1 ? 4 : (fsc == 2 ? 8 : 16);
+    int sh = sharp > 4 ? 2 : (sharp > 0 ? 1 : 0);
+    int limit = sharp > 0 ? clip3(1, 9 - sharp, lvl >> sh) : max(lvl >> sh, 1);
     int blimit = (2 * (lvl + 2) + limit) & 0xff;
-    int thresh = lvl >> 4;
-    return (uint32_t)fsize | ((uint32_t)limit << 8) | ((uint32_t)blimit << 16) | ((uint32_t)thresh << 24);
+    return (uint32_t)fsize | ((uint32_t)limit << 8) | ((uint32_t)blimit << 16) | ((uint32_t)(lvl >> 4) << 24);
+}
+
+// Per-cell edge codes of every deblocked plane of a frame: u16 per 4x4 cell,
+// vertical-edge code in the low byte, horizontal-edge code in the high byte.
+// blockIdx.y is the frame; cells are numbered plane by plane.
+__global__ void __launch_bounds__(256) lf_prep_kernel(const FrameDev* __restrict__ frames) {
+    const FrameDev& F = frames[blockIdx.y];
+    if (!F.do_stage[ST_DEBLOCK]) return;
+    int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int p = 0; p < F.h.num_planes; p++) {
+        int cw = F.recon[p].w >> 2, ch = F.recon[p].h >> 2;
+        if (cell < cw * ch) {
+            if (p > 0 && F.h.lf_level[1 + p] == 0) return;
+            int cy = cell / cw, cx = cell % cw;
+            uint32_t v = edge_param(F, p, 0, cy, cx), hh = edge_param(F, p, 1, cy, cx);
+            F.lf_codes[p][cell] = (uint16_t)(v | (hh << 8));
+            return;
+        }
+        cell -= cw * ch;
+    }
 }
 
 __device__ __forceinline__ int f4clamp(int v, int bd) { return clip3(-(1 << (bd - 1)), (1 << (bd - 1)) - 1, v); }
+
+// wide_filter (loop_filter.rs:789-822) for one (n, log2Size) case: outputs
+// i in [-n, n) from taps j in [-n, n] weighted 2 for |j| <= n2 else 1, source
+// positions clamped to [-(n + 1), n].  All indices are compile-time.
+template <int N, int LOG2, int N2>
+__device__ __forceinline__ void wide(int* b, int st) {
+    int v[2 * N + 2];
+#pragma unroll
+    for (int k = 0; k < 2 * N + 2; k++) v[k] = b[(k - N - 1) * st];
+    int o[2 * N];
+#pragma unroll
+    for (int i = -N; i < N; i++) {
+        int t = 0;
+#pragma unroll
+        for (int j = -N; j <= N; j++) {
+            int pp = i + j < -(N + 1) ? -(N + 1) : (i + j > N ? N : i + j);
+            t += v[pp + N + 1] * ((j <= N2 && j >= -N2) ? 2 : 1);
+        }
+        o[i + N] = (t + (1 << (LOG2 - 1))) >> LOG2;
+    }
+#pragma unroll
+    for (int i = -N; i < N; i++) b[i * st] = o[i + N];
+}
 
 // sample_filtering + filter_mask + narrow/wide filters (loop_filter.rs:582-822)
 // on a line of shared-memory samples; b points at q0, st is the step.
@@ -172,28 +224,12 @@ __device__ void filter_line(int* b, int st, uint32_t prm, int plane, int bd) {
         }
         return;
     }
-    int log2 = (fs == 8 || !flat2) ? 3 : 4;
-    int n = log2 == 4 ? 6 : (plane == 0 ? 3 : 2);
-    int n2 = (log2 == 3 && plane == 0) ? 0 : 1;
-    int v[14];
-#pragma unroll
-    for (int k = -7; k < 7; k++) v[k + 7] = (k >= -(n + 1) && k <= n) ? b[k * st] : 0;
-    int o[12];
-#pragma unroll
-    for (int i = -6; i < 6; i++) {
-        if (i < -n || i >= n) continue;
-        int t = 0;
-#pragma unroll
-        for (int j = -6; j <= 6; j++) {
-            if (j < -n || j > n) continue;
-            int pp = clip3(-(n + 1), n, i + j);
-            t += v[pp + 7] * (abs(j) <= n2 ? 2 : 1);
-        }
-        o[i + 6] = (t + (1 << (log2 - 1))) >> log2;
+    if (fs == 8 || !flat2) {
+        if (plane == 0) wide<3, 3, 0>(b, st);
+        else wide<2, 3, 1>(b, st);
+    } else {
+        wide<6, 4, 1>(b, st);
     }
-#pragma unroll
-    for (int i = -6; i < 6; i++)
-        if (i >= -n && i < n) b[i * st] = o[i + 6];
 }
 
 __global__ void __launch_bounds__(256) deblock_kernel(const FrameDev* __restrict__ frames,
@@ -217,16 +253,35 @@ __global__ void __launch_bounds__(256) deblock_kernel(const FrameDev* __restrict
         const int hbd = F.hbd, bd = F.h.bit_depth;
         const int gx0 = tx * TILE - HALO, gy0 = ty * TILE - HALO;
         __syncthreads();  // previous tile done with shared memory
-        for (int i = threadIdx.x; i < WIN * WIN; i += blockDim.x) {
-            int r = i / WIN, c = i % WIN;
-            int gy = clip3(0, S.h - 1, gy0 + r), gx = clip3(0, S.w - 1, gx0 + c);
-            win[r * PITCH + c] = ld_px(S, hbd, gy, gx);
+        // window: 4 consecutive samples per thread, one vector load when the
+        // group lies inside the plane (rows are 4-sample aligned: gx0 % 4 == 0)
+        for (int i = threadIdx.x; i < WIN * (WIN / 4); i += blockDim.x) {
+            int r = i / (WIN / 4), c = (i % (WIN / 4)) * 4;
+            int gy = clip3(0, S.h - 1, gy0 + r), gx = gx0 + c;
+            int* w = &win[r * PITCH + c];
+            const uint8_t* row = S.p + (size_t)gy * S.stride;
+            if (gx >= 0 && gx + 3 < S.w) {
+                if (hbd) {
+                    uint2 v = *reinterpret_cast<const uint2*>(row + 2 * gx);
+                    w[0] = v.x & 0xffff; w[1] = v.x >> 16; w[2] = v.y & 0xffff; w[3] = v.y >> 16;
+                } else {
+                    uint32_t v = *reinterpret_cast<const uint32_t*>(row + gx);
+                    w[0] = v & 0xff; w[1] = (v >> 8) & 0xff; w[2] = (v >> 16) & 0xff; w[3] = v >> 24;
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; k++) w[k] = ld_px(S, hbd, gy, clip3(0, S.w - 1, gx + k));
+            }
         }
         const int cy0 = gy0 / 4, cx0 = gx0 / 4;  // gx0,gy0 are multiples of 4 (may be negative)
+        const int cw = S.w >> 2, ch = S.h >> 2, sharp = F.h.lf_sharpness;
+        const uint16_t* codes = F.lf_codes[plane];
         for (int i = threadIdx.x; i < CELLS * CELLS; i += blockDim.x) {
             int cr = i / CELLS, cc = i % CELLS;
-            ev[i] = edge_param(F, plane, 0, cy0 + cr, cx0 + cc);
-            eh[i] = edge_param(F, plane, 1, cy0 + cr, cx0 + cc);
+            int cy = cy0 + cr, cx = cx0 + cc;
+            uint32_t code = (cy >= 0 && cx >= 0 && cy < ch && cx < cw) ? codes[cy * cw + cx] : 0;
+            ev[i] = decode_code(code & 0xff, sharp);
+            eh[i] = decode_code(code >> 8, sharp);
         }
         __syncthreads();
         // vertical pass: window rows x edge columns 8..88
@@ -264,8 +319,16 @@ int tiles_deblock(const FrameDev& f) {
     return n;
 }
 
-void launch_deblock(const FrameDev* frames, const int32_t* starts, int n, int total, cudaStream_t s) {
+int cells_deblock(const FrameDev& f) {
+    int n = 0;
+    for (int p = 0; p < f.h.num_planes; p++) n += (f.recon[p].w >> 2) * (f.recon[p].h >> 2);
+    return n;
+}
+
+void launch_deblock(const FrameDev* frames, const int32_t* starts, int n, int total, int max_cells,
+                    cudaStream_t s) {
     if (total <= 0) return;
+    lf_prep_kernel<<<dim3((max_cells + 255) / 256, n), 256, 0, s>>>(frames);
     int grid = total < kSMs * 6 ? total : kSMs * 6;
     deblock_kernel<<<grid, 256, 0, s>>>(frames, starts, n, total);
 }

@@ -114,7 +114,7 @@ def test_mixed_batch_equals_single(lib):
     for d in solo:
         postfilter.run_postfilter([d], mode=abi.MODE_BATCHED)
     torch.cuda.synchronize()
-    assert launches <= 6  # deblock, cdef, superres, lr, grain template + blend
+    assert launches <= 7  # deblock prep + filter, cdef, superres, lr, grain template + blend
     for b, s in zip(batch, solo):
         for stage in ("deblocked", "cdef", "lr", "out"):
             _assert_planes(stage, b.download(stage), s.download(stage))
