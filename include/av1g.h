@@ -255,6 +255,24 @@ av1g_status av1g_run_film_grain(const av1g_frame_job* jobs, int32_t n, void* str
 av1g_status av1g_run_postfilter(const av1g_frame_job* jobs, int32_t n, int32_t mode,
                                 void* stream, int32_t* launches);
 
+/* Film grain (as av1g_run_film_grain) without any device allocation.  No
+ * counterpart in the reference: it exists for callers that may not allocate
+ * device memory on the per-frame path, such as a host application that
+ * reserves the whole device-memory budget at start-up and forbids its
+ * plug-ins to allocate while frames flow (an allocation there can stall on
+ * the allocator or fail once the pool is full).
+ * The frame records and grain scratch live in one static device array of
+ * AV1G_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
+ * exit.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  At most AV1G_NOALLOC_MAX_FRAMES jobs per call,
+ * and the batch's scratch must fit the array; larger requests return
+ * AV1G_EINVAL with a message naming the limit.  All calls on a device share
+ * the array: calls that overlap on the GPU race on it. */
+#define AV1G_NOALLOC_MAX_FRAMES 16
+#define AV1G_NOALLOC_SCRATCH_BYTES (2 * 1024 * 1024)
+av1g_status av1g_run_film_grain_noalloc(const av1g_frame_job* jobs, int32_t n, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -103,7 +103,11 @@ _SIGS = {
     "av1g_run_film_grain": (C.c_int, [C.POINTER(FrameJob), C.c_int32, C.c_void_p]),
     "av1g_run_postfilter": (C.c_int, [C.POINTER(FrameJob), C.c_int32, C.c_int32, C.c_void_p,
                                       C.POINTER(C.c_int32)]),
+    "av1g_run_film_grain_noalloc": (C.c_int, [C.POINTER(FrameJob), C.c_int32, C.c_void_p]),
 }
+
+NOALLOC_MAX_FRAMES = 16
+NOALLOC_SCRATCH_BYTES = 2 * 1024 * 1024
 
 _lib = None
 

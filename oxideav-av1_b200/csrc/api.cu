@@ -14,6 +14,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -344,3 +345,114 @@ av1g_status av1g_run_postfilter(const av1g_frame_job* jobs, int32_t n, int32_t m
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Film grain without device allocation.
+//
+// For callers that may not allocate device memory on the per-frame path: a
+// host application that reserves the whole device-memory budget up front
+// (broadcast and other real-time pipelines) and forbids its plug-ins from
+// allocating while frames flow, because an allocation there can stall on the
+// allocator or fail once the pool is full.  av1g_run_film_grain takes its
+// frame records and grain scratch from the stream-ordered allocator; this
+// variant keeps them in one fixed array in device memory instead.
+//
+// The array is a file-scope static __device__ object of
+// AV1G_NOALLOC_SCRATCH_BYTES, so every GPU that loads this library holds it
+// until the process exits.  Host code may not use the symbol as a device
+// address: on first use on a device (with that device current) the entry
+// point asks the runtime for the array's address with cudaGetSymbolAddress,
+// checks the result, caches it per device, and passes that address to the
+// kernels.  Every call on a device shares the one array and the array keeps
+// the previous call's contents: the kernels write every template, table and
+// offset before reading it, so nothing needs clearing, and calls that overlap
+// on the GPU (two streams, or a second call before the first has finished on
+// another stream) race on the array.
+// ---------------------------------------------------------------------------
+
+static __device__ __align__(256) uint8_t g_noalloc_scratch[AV1G_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[256];  // per device ordinal; null until set up on that device
+
+// Device address of the static scratch on the current device (set up once per device).
+av1g_status noalloc_address(uint8_t** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if (dev < 0 || dev >= 256) return fail(AV1G_EDEVICE, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress");
+        g_noalloc_addr[dev] = p;
+    }
+    *out = (uint8_t*)g_noalloc_addr[dev];
+    return AV1G_OK;
+}
+
+// Host staging of the frame records and tile starts (no heap allocation).
+thread_local FrameDev t_noalloc_frames[AV1G_NOALLOC_MAX_FRAMES];
+thread_local int32_t t_noalloc_starts[2 * (AV1G_NOALLOC_MAX_FRAMES + 1)];
+
+}  // namespace
+
+extern "C" av1g_status av1g_run_film_grain_noalloc(const av1g_frame_job* jobs, int32_t n, void* stream) {
+    g_err.clear();
+    if (n < 0 || (n > 0 && !jobs)) return fail(AV1G_EINVAL, "bad job array");
+    if (n > AV1G_NOALLOC_MAX_FRAMES)
+        return fail(AV1G_EINVAL, "%d frames exceed the %d-frame limit of the allocation-free entry point", n,
+                    AV1G_NOALLOC_MAX_FRAMES);
+    if (n == 0) return AV1G_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    FrameDev* fr = t_noalloc_frames;
+    for (int i = 0; i < n; i++) {
+        av1g_status st = prepare_frame(jobs[i], fr[i]);
+        if (st != AV1G_OK) {
+            std::string m = g_err;
+            return fail(st, "job %d: %s", i, m.c_str());
+        }
+    }
+    // layout: frames | template starts (n+1) | blend starts (n+1) | per-frame grain scratch
+    size_t off_starts = (sizeof(FrameDev) * n + 255) & ~(size_t)255;
+    size_t off_scratch = (off_starts + sizeof(int32_t) * 2 * (n + 1) + 255) & ~(size_t)255;
+    size_t total = off_scratch;
+    for (int i = 0; i < n; i++)
+        if (fr[i].do_stage[ST_GRAIN]) total += grain_scratch_bytes(fr[i]);
+    if (total > AV1G_NOALLOC_SCRATCH_BYTES)
+        return fail(AV1G_EINVAL, "batch needs %zu bytes of scratch, above the %d-byte static array", total,
+                    AV1G_NOALLOC_SCRATCH_BYTES);
+    uint8_t* base = nullptr;
+    av1g_status st = noalloc_address(&base);
+    if (st != AV1G_OK) return st;
+    int32_t* hs = t_noalloc_starts;
+    size_t off = off_scratch;
+    int tmpl = 0, blend = 0;
+    for (int i = 0; i < n; i++) {
+        FrameDev& F = fr[i];
+        hs[i] = tmpl;
+        hs[n + 1 + i] = blend;
+        if (F.do_stage[ST_GRAIN]) {
+            F.grain_tmpl = (int16_t*)(base + off);
+            F.grain_lut = (uint8_t*)(base + off + 3 * 73 * 82 * 2);
+            F.grain_offs = F.grain_lut + 768;
+            off += grain_scratch_bytes(F);
+            tmpl += 1;
+            blend += tiles_grain_blend(F);
+        }
+    }
+    hs[n] = tmpl;
+    hs[2 * n + 1] = blend;
+    cudaError_t e = cudaMemcpyAsync(base, fr, sizeof(FrameDev) * n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(base + off_starts, hs, sizeof(int32_t) * 2 * (n + 1), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync");
+    const int32_t* ds = (const int32_t*)(base + off_starts);
+    launch_grain((const FrameDev*)base, ds, ds + n + 1, n, tmpl, blend, s);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+    return AV1G_OK;
+}
