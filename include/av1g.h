@@ -198,6 +198,67 @@ typedef struct av1g_frame_job {
     av1g_plane out[3];
 } av1g_frame_job;
 
+/* ---------------------------------------------------------------------
+ * Reconstruction (dequant, inverse transform, merge)
+ * ------------------------------------------------------------------- */
+
+/* Frame-level quantizer state (QuantizerParams, src/cdf.rs:13405) plus the
+ * per-segment LosslessArray.  seg_qm_level[plane][segment]; a level of 15
+ * means no quantizer matrix. */
+typedef struct av1g_quant_params {
+    uint8_t base_q_idx;
+    int8_t delta_q_y_dc;
+    int8_t delta_q_u_dc;
+    int8_t delta_q_u_ac;
+    int8_t delta_q_v_dc;
+    int8_t delta_q_v_ac;
+    uint8_t using_qmatrix;
+    uint8_t delta_q_present;
+    uint8_t segmentation_enabled;
+    uint8_t seg_alt_q_active[8];
+    uint8_t pad;
+    int16_t seg_alt_q_data[8];
+    uint8_t seg_qm_level[3][8];
+    uint8_t lossless[8];
+} av1g_quant_params;
+
+/* One transform unit with coefficients (the reference reconstructs a TU only
+ * when eob > 0, cdf.rs:32874; TUs without coefficients are not listed).
+ * x, y: plane sample position of the TU; tx_type is PlaneTxType;
+ * current_q_index is CurrentQIndex where the TU's block was decoded.
+ * Its quantized levels are min(32,w) x min(32,h) int32 at coeff_offset in the
+ * job's coefficient pool (row stride min(32,w), dequantize_step1's layout). */
+typedef struct av1g_tu {
+    uint16_t x;
+    uint16_t y;
+    uint8_t plane;
+    uint8_t tx_size;
+    uint8_t tx_type;
+    uint8_t segment_id;
+    uint8_t current_q_index;
+    uint8_t pad[3];
+    uint32_t coeff_offset;
+} av1g_tu;
+
+/* A frame's residual work: tus and coeffs are device arrays; planes hold the
+ * prediction on entry (CurrFrame at the padded mi extent) and the
+ * reconstruction on return. */
+typedef struct av1g_recon_job {
+    const av1g_frame_header* hdr;    /* host: bit depth, subsampling, mi dims */
+    const av1g_quant_params* quant;  /* host */
+    const av1g_tu* tus;              /* device */
+    int32_t num_tus;
+    const int32_t* coeffs;           /* device */
+    av1g_plane planes[3];            /* device, updated in place */
+} av1g_recon_job;
+
+/* §7.12.3 dequantization + §7.13.3 inverse transform + §7.12.3 step-3 merge
+ * for every listed TU of `n` frames.  Replaces the reconstruct tail of
+ * transform_block_emit (src/cdf.rs:32874-32910): dequantize_step1
+ * (cdf.rs:13655), inverse_transform_2d (src/transform.rs:707),
+ * curr_frame_step3_merge (cdf.rs:17398). */
+av1g_status av1g_run_recon(const av1g_recon_job* jobs, int32_t n, void* stream);
+
 /* Launch modes for av1g_run_postfilter. */
 #define AV1G_MODE_BATCHED 0     /* one launch per stage across all jobs    */
 #define AV1G_MODE_PER_FRAME 1   /* one launch per stage per frame          */

@@ -184,3 +184,34 @@ def random_draws(seed, bits, count):
     lib = load()
     st = C.c_uint16(seed)
     return [lib.ora_random_next(C.byref(st), bits) for _ in range(count)]
+
+
+def recon(frame):
+    """Dequant + inverse transform + merge of every TU onto the prediction planes (int32 copies)."""
+    lib = load()
+    planes = [np.ascontiguousarray(p, dtype=np.int32) for p in frame.planes]
+    tus = np.ascontiguousarray(frame.tus)
+    coeffs = np.ascontiguousarray(frame.coeffs, dtype=np.int32)
+    lib.ora_recon_frame(C.byref(frame.hdr), C.byref(frame.quant), tus.ctypes.data_as(C.c_void_p), len(tus),
+                        _ptr(coeffs), _planes(planes))
+    return planes
+
+
+def dequantize(quant, bit_depth, levels, tx, plane, segment_id, current_q_index, tx_type):
+    lib = load()
+    w = [4, 8, 16, 32, 64, 4, 8, 8, 16, 16, 32, 32, 64, 4, 16, 8, 32, 16, 64][tx]
+    h = [4, 8, 16, 32, 64, 8, 4, 16, 8, 32, 16, 64, 32, 16, 4, 32, 8, 64, 16][tx]
+    lv = np.ascontiguousarray(levels, dtype=np.int32)
+    out = np.zeros(w * h, np.int64)
+    lib.ora_dequantize(C.byref(quant), bit_depth, _ptr(lv), tx, plane, segment_id, current_q_index, tx_type,
+                       out.ctypes.data_as(C.c_void_p))
+    return out.reshape(h, w)
+
+
+def inverse_transform(dequant, tx, tx_type, bit_depth, lossless=False):
+    lib = load()
+    d = np.ascontiguousarray(dequant, dtype=np.int64)
+    res = np.zeros_like(d)
+    lib.ora_inverse_transform_2d(d.ctypes.data_as(C.c_void_p), tx, tx_type, bit_depth, int(lossless),
+                                 res.ctypes.data_as(C.c_void_p))
+    return res

@@ -74,6 +74,18 @@ int ora_postfilter_frame(const av1g_frame_header* hdr, const av1g_mi_grid* grid,
                          const int32_t* const recon[3], int32_t* ref_out[3],
                          int32_t* out[3]);
 
+/* §7.12.3 step 1 — dequantize_step1 (src/cdf.rs:13655): compact levels ->
+ * dense w*h int64. */
+void ora_dequantize(const av1g_quant_params* q, int bit_depth, const int32_t* levels, int tx, int plane,
+                    int segment_id, int current_q_index, int plane_tx_type, int64_t* out);
+
+/* §7.13.3 — inverse_transform_2d (src/transform.rs:707): w*h int64 -> w*h int64. */
+void ora_inverse_transform_2d(const int64_t* dq, int tx, int tx_type, int bit_depth, int lossless, int64_t* res);
+
+/* dequant + inverse transform + step-3 merge of every TU (in place on planes). */
+void ora_recon_frame(const av1g_frame_header* hdr, const av1g_quant_params* q, const av1g_tu* tus, int n,
+                     const int32_t* coeffs, ora_plane planes[3]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -87,8 +87,30 @@ class FrameJob(C.Structure):
     ]
 
 
+class QuantParams(C.Structure):
+    _fields_ = [
+        ("base_q_idx", C.c_uint8), ("delta_q_y_dc", C.c_int8), ("delta_q_u_dc", C.c_int8),
+        ("delta_q_u_ac", C.c_int8), ("delta_q_v_dc", C.c_int8), ("delta_q_v_ac", C.c_int8),
+        ("using_qmatrix", C.c_uint8), ("delta_q_present", C.c_uint8), ("segmentation_enabled", C.c_uint8),
+        ("seg_alt_q_active", C.c_uint8 * 8), ("pad", C.c_uint8), ("seg_alt_q_data", C.c_int16 * 8),
+        ("seg_qm_level", (C.c_uint8 * 8) * 3), ("lossless", C.c_uint8 * 8),
+    ]
+
+
+class Tu(C.Structure):
+    _fields_ = [("x", C.c_uint16), ("y", C.c_uint16), ("plane", C.c_uint8), ("tx_size", C.c_uint8),
+                ("tx_type", C.c_uint8), ("segment_id", C.c_uint8), ("current_q_index", C.c_uint8),
+                ("pad", C.c_uint8 * 3), ("coeff_offset", C.c_uint32)]
+
+
+class ReconJob(C.Structure):
+    _fields_ = [("hdr", C.POINTER(FrameHeader)), ("quant", C.POINTER(QuantParams)), ("tus", C.c_void_p),
+                ("num_tus", C.c_int32), ("coeffs", C.c_void_p), ("planes", Plane * 3)]
+
+
 _STRUCTS = {"av1g_film_grain": FilmGrain, "av1g_frame_header": FrameHeader, "av1g_lr_unit": LrUnit,
-            "av1g_mi_grid": MiGrid, "av1g_plane": Plane, "av1g_frame_job": FrameJob}
+            "av1g_mi_grid": MiGrid, "av1g_plane": Plane, "av1g_frame_job": FrameJob,
+            "av1g_quant_params": QuantParams, "av1g_tu": Tu, "av1g_recon_job": ReconJob}
 
 # exported entry points and their ctypes signatures
 _SIGS = {
@@ -104,6 +126,7 @@ _SIGS = {
     "av1g_run_postfilter": (C.c_int, [C.POINTER(FrameJob), C.c_int32, C.c_int32, C.c_void_p,
                                       C.POINTER(C.c_int32)]),
     "av1g_run_film_grain_noalloc": (C.c_int, [C.POINTER(FrameJob), C.c_int32, C.c_void_p]),
+    "av1g_run_recon": (C.c_int, [C.POINTER(ReconJob), C.c_int32, C.c_void_p]),
 }
 
 NOALLOC_MAX_FRAMES = 16

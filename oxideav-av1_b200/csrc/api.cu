@@ -22,6 +22,7 @@
 
 namespace av1g {
 size_t lr_smem_bytes();
+av1g_status recon_run(const av1g_recon_job* jobs, int n, cudaStream_t s, std::string& err);
 }
 
 using namespace av1g;
@@ -317,6 +318,9 @@ int32_t av1g_struct_size(const char* name) {
     if (!strcmp(name, "av1g_mi_grid")) return (int32_t)sizeof(av1g_mi_grid);
     if (!strcmp(name, "av1g_plane")) return (int32_t)sizeof(av1g_plane);
     if (!strcmp(name, "av1g_frame_job")) return (int32_t)sizeof(av1g_frame_job);
+    if (!strcmp(name, "av1g_quant_params")) return (int32_t)sizeof(av1g_quant_params);
+    if (!strcmp(name, "av1g_tu")) return (int32_t)sizeof(av1g_tu);
+    if (!strcmp(name, "av1g_recon_job")) return (int32_t)sizeof(av1g_recon_job);
     return -1;
 }
 
@@ -338,6 +342,15 @@ av1g_status av1g_run_lr(const av1g_frame_job* jobs, int32_t n, void* stream) {
 }
 av1g_status av1g_run_film_grain(const av1g_frame_job* jobs, int32_t n, void* stream) {
     return run(jobs, n, 1 << ST_GRAIN, AV1G_MODE_BATCHED, stream, nullptr);
+}
+av1g_status av1g_run_recon(const av1g_recon_job* jobs, int32_t n, void* stream) {
+    g_err.clear();
+    if (n < 0 || (n > 0 && !jobs)) return fail(AV1G_EINVAL, "bad job array");
+    if (n == 0) return AV1G_OK;
+    std::string err;
+    av1g_status st = recon_run(jobs, n, (cudaStream_t)stream, err);
+    if (st != AV1G_OK) g_err = err;
+    return st;
 }
 av1g_status av1g_run_postfilter(const av1g_frame_job* jobs, int32_t n, int32_t mode, void* stream,
                                 int32_t* launches) {

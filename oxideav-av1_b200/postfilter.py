@@ -164,3 +164,38 @@ def run_postfilter(frames, mode=abi.MODE_BATCHED, stream=None, jobs=None):
     n = C.c_int32(0)
     abi.check(lib.av1g_run_postfilter(jobs, len(frames), mode, _stream_ptr(stream), C.byref(n)))
     return n.value
+
+
+class DeviceRecon:
+    """A reconstruction frame on the GPU: prediction planes (updated in place) + coefficient pool."""
+
+    def __init__(self, rframe, device="cuda"):
+        self.frame = rframe
+        hbd = rframe.hbd
+        self.planes = [DevPlane(*rframe.plane_dims(p), hbd, device, fill=rframe.planes[p])
+                       for p in range(rframe.hdr.num_planes)]
+        self.coeffs = torch.from_numpy(np.ascontiguousarray(rframe.coeffs)).to(device)
+        self.tus = np.ascontiguousarray(rframe.tus)   # host array: the library buckets and uploads it
+
+    def job(self):
+        j = abi.ReconJob()
+        j.hdr = C.pointer(self.frame.hdr)
+        j.quant = C.pointer(self.frame.quant)
+        j.tus = self.tus.ctypes.data
+        j.num_tus = len(self.tus)
+        j.coeffs = self.coeffs.data_ptr()
+        for p, pl in enumerate(self.planes):
+            j.planes[p] = pl.cplane()
+        return j
+
+    def download(self):
+        return [pl.download() for pl in self.planes]
+
+
+def run_recon(frames, stream=None):
+    lib = abi.load()
+    arr = (abi.ReconJob * len(frames))()
+    for i, f in enumerate(frames):
+        arr[i] = f.job()
+    abi.check(lib.av1g_run_recon(arr, len(frames), _stream_ptr(stream)))
+    return arr

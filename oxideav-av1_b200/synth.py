@@ -306,3 +306,111 @@ def _film_grain(rng, fg, bd, mono):
     fg.cb_offset, fg.cr_offset = int(rng.integers(0, 512)), int(rng.integers(0, 512))
     fg.overlap_flag = int(rng.random() < 0.7)
     fg.clip_to_restricted_range = int(rng.random() < 0.5)
+
+
+# ---------------------------------------------------------------------------
+# Reconstruction workloads: predictions + TU lists with coefficients
+# ---------------------------------------------------------------------------
+
+TU_DTYPE = np.dtype([("x", np.uint16), ("y", np.uint16), ("plane", np.uint8), ("tx_size", np.uint8),
+                     ("tx_type", np.uint8), ("segment_id", np.uint8), ("current_q_index", np.uint8),
+                     ("pad", np.uint8, (3,)), ("coeff_offset", np.uint32)])
+assert TU_DTYPE.itemsize == C.sizeof(abi.Tu)
+TX_W = [4, 8, 16, 32, 64, 4, 8, 8, 16, 16, 32, 32, 64, 4, 16, 8, 32, 16, 64]
+TX_H = [4, 8, 16, 32, 64, 8, 4, 16, 8, 32, 16, 64, 32, 16, 4, 32, 8, 64, 16]
+TX_OF = {(w, h): i for i, (w, h) in enumerate(zip(TX_W, TX_H))}
+
+
+class ReconFrame:
+    """Prediction planes + the TUs (with levels) the reference would reconstruct."""
+
+    def __init__(self):
+        self.hdr = abi.FrameHeader()
+        self.quant = abi.QuantParams()
+        self.tus = None
+        self.coeffs = None
+        self.planes = []
+
+    @property
+    def hbd(self):
+        return self.hdr.bit_depth > 8
+
+    def plane_dims(self, p):
+        h = self.hdr
+        return (h.mi_rows * 4) >> (h.subsampling_y if p else 0), (h.mi_cols * 4) >> (h.subsampling_x if p else 0)
+
+
+def _tx_type_for(rng, w, h):
+    m = max(w, h)
+    if m == 64:
+        return 0                                   # TX_SET_DCTONLY
+    if m == 32:
+        return int(rng.choice([0, 9]))             # DCT_DCT or IDTX
+    return int(rng.integers(0, 16))
+
+
+def _levels(rng, tw, th, big):
+    n = tw * th
+    lv = np.zeros(n, np.int32)
+    k = int(min(n, 1 + rng.geometric(0.15)))       # roughly an end-of-block position
+    mags = rng.geometric(0.35, size=k).astype(np.int64)
+    sign = np.where(rng.random(k) < 0.5, -1, 1)
+    lv[:k] = (mags * sign).astype(np.int32)
+    if big and rng.random() < 0.2:
+        lv[int(rng.integers(0, k))] = int(rng.choice([-1, 1]) * rng.integers(2000, 200000))
+    return lv
+
+
+def make_recon_frame(seed, width=352, height=288, bit_depth=8, ssx=1, ssy=1, mono=False, qmatrix=True,
+                     lossless_segments=True, big_levels=True):
+    rng = np.random.default_rng(seed)
+    f = ReconFrame()
+    h = f.hdr
+    h.frame_width = h.upscaled_width = width
+    h.frame_height = height
+    h.mi_cols, h.mi_rows = 2 * ((width + 7) >> 3), 2 * ((height + 7) >> 3)
+    h.bit_depth = bit_depth
+    h.num_planes = 1 if mono else 3
+    h.subsampling_x, h.subsampling_y = (1, 1) if mono else (ssx, ssy)
+    q = f.quant
+    q.base_q_idx = int(rng.integers(0, 256))
+    for name in ("delta_q_y_dc", "delta_q_u_dc", "delta_q_u_ac", "delta_q_v_dc", "delta_q_v_ac"):
+        setattr(q, name, int(rng.integers(-15, 16)))
+    q.using_qmatrix = int(qmatrix and rng.random() < 0.7)
+    q.delta_q_present = int(rng.random() < 0.5)
+    q.segmentation_enabled = 1
+    for s in range(8):
+        q.seg_alt_q_active[s] = int(rng.random() < 0.4)
+        q.seg_alt_q_data[s] = int(rng.integers(-60, 61))
+        for p in range(3):
+            q.seg_qm_level[p][s] = int(rng.integers(0, 16))
+        q.lossless[s] = int(lossless_segments and s == 7)
+    maxv = (1 << bit_depth) - 1
+    for p in range(h.num_planes):
+        ph, pw = f.plane_dims(p)
+        f.planes.append(rng.integers(0, maxv + 1, size=(ph, pw)).astype(np.uint8 if bit_depth == 8 else np.uint16))
+    tus, coeffs, off = [], [], 0
+    for p in range(h.num_planes):
+        ph, pw = f.plane_dims(p)
+        # tile the plane with 64x64 areas, each split into TUs of one random legal size
+        for y0 in range(0, ph, 64):
+            for x0 in range(0, pw, 64):
+                seg = int(rng.integers(0, 8))
+                if q.lossless[seg]:
+                    w = hh = 4
+                else:
+                    w, hh = [(TX_W[i], TX_H[i]) for i in range(19)][int(rng.integers(0, 19))]
+                tx = TX_OF[(w, hh)]
+                cq = int(rng.integers(1, 256))
+                for y in range(y0, min(y0 + 64, ph), hh):
+                    for x in range(x0, min(x0 + 64, pw), w):
+                        if rng.random() < 0.3:
+                            continue                      # no coefficients (eob == 0): not listed
+                        tw, th = min(32, w), min(32, hh)
+                        tt = 0 if q.lossless[seg] else _tx_type_for(rng, w, hh)
+                        tus.append((x, y, p, tx, tt, seg, cq, (0, 0, 0), off))
+                        coeffs.append(_levels(rng, tw, th, big_levels))
+                        off += tw * th
+    f.tus = np.array(tus, dtype=TU_DTYPE)
+    f.coeffs = np.concatenate(coeffs).astype(np.int32) if coeffs else np.zeros(1, np.int32)
+    return f
