@@ -259,6 +259,68 @@ typedef struct av1g_recon_job {
  * curr_frame_step3_merge (cdf.rs:17398). */
 av1g_status av1g_run_recon(const av1g_recon_job* jobs, int32_t n, void* stream);
 
+/* ---------------------------------------------------------------------
+ * Intra prediction + reconstruction
+ * ------------------------------------------------------------------- */
+
+/* flags of av1g_intra_tu */
+#define AV1G_INTRA_HAVE_ABOVE        0x01
+#define AV1G_INTRA_HAVE_LEFT         0x02
+#define AV1G_INTRA_HAVE_ABOVE_RIGHT  0x04
+#define AV1G_INTRA_HAVE_BELOW_LEFT   0x08
+#define AV1G_INTRA_EDGE_FILTER       0x10  /* enable_intra_edge_filter        */
+#define AV1G_INTRA_FILTER_TYPE       0x20  /* get_filter_type() == 1 (smooth)  */
+#define AV1G_INTRA_RESIDUAL          0x40  /* the TU has coefficients (eob>0)  */
+#define AV1G_INTRA_CFL               0x80  /* chroma-from-luma on top of DC    */
+
+/* One intra transform unit, in decode order, with the prediction inputs the
+ * tile walker derives at transform_block_emit (src/cdf.rs:32540-32700):
+ * mode is YMode for luma and UVMode for chroma with UV_CFL_PRED mapped to
+ * DC_PRED; haveAbove / haveLeft are `avail || x/y > 0`; filter_intra_mode is
+ * 0..4 or 255 for none (luma only).  For CfL TUs, cfl_alpha is CflAlphaU/V and
+ * max_luma_w/h are MaxLumaW/H (luma samples) of the block.  `res` is the
+ * residual (used when AV1G_INTRA_RESIDUAL is set); res.x/y/plane/tx_size must
+ * equal the TU's. */
+typedef struct av1g_intra_tu {
+    uint16_t x;
+    uint16_t y;
+    uint8_t plane;
+    uint8_t tx_size;
+    uint8_t mode;
+    uint8_t flags;
+    int8_t angle_delta;
+    int8_t cfl_alpha;
+    uint8_t filter_intra_mode;
+    uint8_t pad;
+    uint16_t max_luma_w;
+    uint16_t max_luma_h;
+    av1g_tu res;
+} av1g_intra_tu;
+
+/* A frame's intra work, reconstructed in place on top of whatever the
+ * planes already hold (inter predictions + residuals of inter blocks).
+ * tus: host array in decode order; coeffs: device pool; planes: device. */
+typedef struct av1g_intra_job {
+    const av1g_frame_header* hdr;    /* host */
+    const av1g_quant_params* quant;  /* host */
+    const av1g_intra_tu* tus;        /* host, decode order */
+    int32_t num_tus;
+    int32_t sb_size;                 /* 64 or 128 (luma samples) */
+    const int32_t* coeffs;           /* device */
+    av1g_plane planes[3];            /* device, updated in place */
+} av1g_intra_job;
+
+/* §7.11.2 intra prediction (DC, V, H, directional with edge filter and
+ * upsampling, SMOOTH*, PAETH, recursive filter intra), §7.11.5 chroma from
+ * luma, then dequant + inverse transform + merge, for every intra TU of `n`
+ * frames.  Replaces predict_intra_into_curr_frame (src/cdf.rs:16789),
+ * intra_predict_block_samples (cdf.rs:16990-17250), the kernels at
+ * cdf.rs:1348-3120 and predict_chroma_from_luma_into_curr_frame
+ * (cdf.rs:17256) as called from transform_block_emit (cdf.rs:32482).
+ * Superblocks run as a wavefront (level = column + 2 * row): one launch per
+ * level across all frames, each superblock's TUs in decode order. */
+av1g_status av1g_run_intra(const av1g_intra_job* jobs, int32_t n, void* stream);
+
 /* Launch modes for av1g_run_postfilter. */
 #define AV1G_MODE_BATCHED 0     /* one launch per stage across all jobs    */
 #define AV1G_MODE_PER_FRAME 1   /* one launch per stage per frame          */

@@ -215,3 +215,14 @@ def inverse_transform(dequant, tx, tx_type, bit_depth, lossless=False):
     lib.ora_inverse_transform_2d(d.ctypes.data_as(C.c_void_p), tx, tx_type, bit_depth, int(lossless),
                                  res.ctypes.data_as(C.c_void_p))
     return res
+
+
+def intra(frame):
+    """Every intra TU in decode order (prediction, CfL, residual) on int32 copies of the planes."""
+    lib = load()
+    planes = [np.ascontiguousarray(p, dtype=np.int32) for p in frame.planes]
+    tus = np.ascontiguousarray(frame.tus)
+    coeffs = np.ascontiguousarray(frame.coeffs, dtype=np.int32)
+    lib.ora_intra_frame(C.byref(frame.hdr), C.byref(frame.quant), tus.ctypes.data_as(C.c_void_p), len(tus),
+                        _ptr(coeffs), _planes(planes))
+    return planes

@@ -86,6 +86,16 @@ void ora_inverse_transform_2d(const int64_t* dq, int tx, int tx_type, int bit_de
 void ora_recon_frame(const av1g_frame_header* hdr, const av1g_quant_params* q, const av1g_tu* tus, int n,
                      const int32_t* coeffs, ora_plane planes[3]);
 
+/* intra_predict_block_samples (src/cdf.rs:16990-17250) reading plane p;
+ * filter_intra_mode 0..4 or 255; pred receives w*h samples. */
+void ora_intra_predict(const ora_plane* p, int sx, int sy, int tx, int mode, int angle_delta, int bd, int flags,
+                       int filter_intra_mode, uint16_t* pred);
+
+/* Every intra TU of a frame in decode order: prediction, chroma from luma,
+ * residual (transform_block_emit order, src/cdf.rs:32540-32910). */
+void ora_intra_frame(const av1g_frame_header* hdr, const av1g_quant_params* q, const av1g_intra_tu* tus, int n,
+                     const int32_t* coeffs, ora_plane planes[3]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -108,9 +108,25 @@ class ReconJob(C.Structure):
                 ("num_tus", C.c_int32), ("coeffs", C.c_void_p), ("planes", Plane * 3)]
 
 
+class IntraTu(C.Structure):
+    _fields_ = [("x", C.c_uint16), ("y", C.c_uint16), ("plane", C.c_uint8), ("tx_size", C.c_uint8),
+                ("mode", C.c_uint8), ("flags", C.c_uint8), ("angle_delta", C.c_int8), ("cfl_alpha", C.c_int8),
+                ("filter_intra_mode", C.c_uint8), ("pad", C.c_uint8), ("max_luma_w", C.c_uint16),
+                ("max_luma_h", C.c_uint16), ("res", Tu)]
+
+
+class IntraJob(C.Structure):
+    _fields_ = [("hdr", C.POINTER(FrameHeader)), ("quant", C.POINTER(QuantParams)), ("tus", C.c_void_p),
+                ("num_tus", C.c_int32), ("sb_size", C.c_int32), ("coeffs", C.c_void_p), ("planes", Plane * 3)]
+
+
+INTRA_HAVE_ABOVE, INTRA_HAVE_LEFT, INTRA_HAVE_ABOVE_RIGHT, INTRA_HAVE_BELOW_LEFT = 1, 2, 4, 8
+INTRA_EDGE_FILTER, INTRA_FILTER_TYPE, INTRA_RESIDUAL, INTRA_CFL = 16, 32, 64, 128
+
 _STRUCTS = {"av1g_film_grain": FilmGrain, "av1g_frame_header": FrameHeader, "av1g_lr_unit": LrUnit,
             "av1g_mi_grid": MiGrid, "av1g_plane": Plane, "av1g_frame_job": FrameJob,
-            "av1g_quant_params": QuantParams, "av1g_tu": Tu, "av1g_recon_job": ReconJob}
+            "av1g_quant_params": QuantParams, "av1g_tu": Tu, "av1g_recon_job": ReconJob,
+            "av1g_intra_tu": IntraTu, "av1g_intra_job": IntraJob}
 
 # exported entry points and their ctypes signatures
 _SIGS = {
@@ -127,6 +143,7 @@ _SIGS = {
                                       C.POINTER(C.c_int32)]),
     "av1g_run_film_grain_noalloc": (C.c_int, [C.POINTER(FrameJob), C.c_int32, C.c_void_p]),
     "av1g_run_recon": (C.c_int, [C.POINTER(ReconJob), C.c_int32, C.c_void_p]),
+    "av1g_run_intra": (C.c_int, [C.POINTER(IntraJob), C.c_int32, C.c_void_p]),
 }
 
 NOALLOC_MAX_FRAMES = 16

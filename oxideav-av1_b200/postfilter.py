@@ -199,3 +199,28 @@ def run_recon(frames, stream=None):
         arr[i] = f.job()
     abi.check(lib.av1g_run_recon(arr, len(frames), _stream_ptr(stream)))
     return arr
+
+
+class DeviceIntra(DeviceRecon):
+    """An intra frame on the GPU: planes (reconstructed in place) + coefficient pool + TU list."""
+
+    def job(self):
+        j = abi.IntraJob()
+        j.hdr = C.pointer(self.frame.hdr)
+        j.quant = C.pointer(self.frame.quant)
+        j.tus = self.tus.ctypes.data
+        j.num_tus = len(self.tus)
+        j.sb_size = self.frame.sb_size
+        j.coeffs = self.coeffs.data_ptr()
+        for p, pl in enumerate(self.planes):
+            j.planes[p] = pl.cplane()
+        return j
+
+
+def run_intra(frames, stream=None):
+    lib = abi.load()
+    arr = (abi.IntraJob * len(frames))()
+    for i, f in enumerate(frames):
+        arr[i] = f.job()
+    abi.check(lib.av1g_run_intra(arr, len(frames), _stream_ptr(stream)))
+    return arr

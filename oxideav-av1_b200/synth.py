@@ -414,3 +414,122 @@ def make_recon_frame(seed, width=352, height=288, bit_depth=8, ssx=1, ssy=1, mon
     f.tus = np.array(tus, dtype=TU_DTYPE)
     f.coeffs = np.concatenate(coeffs).astype(np.int32) if coeffs else np.zeros(1, np.int32)
     return f
+
+
+# ---------------------------------------------------------------------------
+# Intra workloads: TU lists in decode order with prediction parameters
+# ---------------------------------------------------------------------------
+
+INTRA_TU_DTYPE = np.dtype([("x", np.uint16), ("y", np.uint16), ("plane", np.uint8), ("tx_size", np.uint8),
+                           ("mode", np.uint8), ("flags", np.uint8), ("angle_delta", np.int8), ("cfl_alpha", np.int8),
+                           ("filter_intra_mode", np.uint8), ("pad", np.uint8), ("max_luma_w", np.uint16),
+                           ("max_luma_h", np.uint16), ("res", TU_DTYPE)])
+assert INTRA_TU_DTYPE.itemsize == C.sizeof(abi.IntraTu)
+
+
+class IntraFrame(ReconFrame):
+    """Planes (left as garbage: intra TUs overwrite every sample) + intra TUs in decode order."""
+
+    def __init__(self):
+        super().__init__()
+        self.sb_size = 64
+
+
+def _blocks(rng, x0, y0, n, pw, ph, out):
+    """Recursive square/rect partition of an n x n area (samples) into blocks, in decode order."""
+    if x0 >= pw or y0 >= ph:
+        return
+    if n > 4 and (rng.random() < 0.55 or x0 + n > pw or y0 + n > ph):
+        h = n // 2
+        for dy in (0, h):
+            for dx in (0, h):
+                _blocks(rng, x0 + dx, y0 + dy, h, pw, ph, out)
+        return
+    r = rng.random()
+    if n >= 8 and r < 0.2:
+        out.append((x0, y0, n, n // 2))
+        out.append((x0, y0 + n // 2, n, n // 2))
+    elif n >= 8 and r < 0.4:
+        out.append((x0, y0, n // 2, n))
+        out.append((x0 + n // 2, y0, n // 2, n))
+    else:
+        out.append((x0, y0, n, n))
+
+
+def make_intra_frame(seed, width=176, height=144, bit_depth=8, ssx=1, ssy=1, mono=False, sb_size=64,
+                     edge_filter=True):
+    rng = np.random.default_rng(seed)
+    base = make_recon_frame(seed + 1000, width, height, bit_depth, ssx, ssy, mono)
+    f = IntraFrame()
+    f.hdr, f.quant, f.sb_size = base.hdr, base.quant, sb_size
+    h = f.hdr
+    maxv = (1 << bit_depth) - 1
+    f.planes = [rng.integers(0, maxv + 1, size=f.plane_dims(p)).astype(np.uint8 if bit_depth == 8 else np.uint16)
+                for p in range(h.num_planes)]
+    tus, coeffs, off = [], [], 0
+    decoded = [np.zeros(((f.plane_dims(p)[0] + 3) // 4, (f.plane_dims(p)[1] + 3) // 4), bool)
+               for p in range(h.num_planes)]
+    lossless_seg = [s for s in range(8) if f.quant.lossless[s]]
+    for sby in range(0, h.mi_rows * 4, sb_size):
+        for sbx in range(0, h.mi_cols * 4, sb_size):
+            for p in range(h.num_planes):
+                sx_, sy_ = (h.subsampling_x, h.subsampling_y) if p else (0, 0)
+                ph, pw = f.plane_dims(p)
+                blocks = []
+                _blocks(rng, sbx >> sx_, sby >> sy_, sb_size >> max(sx_, sy_), pw, ph, blocks)
+                for (bx, by, bw, bh) in blocks:
+                    # a legal TU size for the block (Max_Tx_Size_Rect, optionally split once)
+                    bw_, bh_ = min(bw, 64), min(bh, 64)
+                    tw, th = bw_, bh_
+                    if rng.random() < 0.3 and tw >= 8 and th >= 8:
+                        tw, th = tw // 2, th // 2
+                    if (tw, th) not in TX_OF:
+                        tw, th = min(tw, th), min(tw, th)
+                    tx = TX_OF[(tw, th)]
+                    mode = int(rng.integers(0, 13))
+                    ad = int(rng.integers(-3, 4)) if 1 <= mode <= 8 else 0
+                    fim = 255
+                    cfl = False
+                    if p == 0 and tw <= 32 and th <= 32 and rng.random() < 0.15:
+                        mode, ad, fim = 0, 0, int(rng.integers(0, 5))
+                    if p > 0 and rng.random() < 0.25:
+                        mode, ad, cfl = 0, 0, True
+                    seg = int(rng.integers(0, 8))
+                    if seg in lossless_seg and tx != 0:
+                        seg = 0 if 0 not in lossless_seg else 1
+                    for ty in range(by, by + bh, th):
+                        for tx_ in range(bx, bx + bw, tw):
+                            if ty >= ph or tx_ >= pw:
+                                continue
+                            flags = 0
+                            if ty > 0:
+                                flags |= abi.INTRA_HAVE_ABOVE
+                            if tx_ > 0:
+                                flags |= abi.INTRA_HAVE_LEFT
+                            cy, cx = ty // 4, tx_ // 4
+                            if cy > 0 and (tx_ + tw) // 4 < decoded[p].shape[1] and decoded[p][cy - 1, (tx_ + tw) // 4]:
+                                flags |= abi.INTRA_HAVE_ABOVE_RIGHT
+                            if cx > 0 and (ty + th) // 4 < decoded[p].shape[0] and decoded[p][(ty + th) // 4, cx - 1]:
+                                flags |= abi.INTRA_HAVE_BELOW_LEFT
+                            if edge_filter:
+                                flags |= abi.INTRA_EDGE_FILTER
+                            if rng.random() < 0.3:
+                                flags |= abi.INTRA_FILTER_TYPE
+                            if cfl:
+                                flags |= abi.INTRA_CFL
+                            res = (tx_, ty, p, tx, 0, seg, int(rng.integers(1, 256)), (0, 0, 0), 0)
+                            if rng.random() < 0.7 and (seg not in lossless_seg or tx == 0):
+                                flags |= abi.INTRA_RESIDUAL
+                                tt = 0 if seg in lossless_seg else _tx_type_for(rng, tw, th)
+                                res = (tx_, ty, p, tx, tt, seg, res[6], (0, 0, 0), off)
+                                lv = _levels(rng, min(32, tw), min(32, th), True)
+                                coeffs.append(lv)
+                                off += len(lv)
+                            mlw = min((bx + bw) << sx_, 65535)
+                            mlh = min((by + bh) << sy_, 65535)
+                            tus.append((tx_, ty, p, tx, mode, flags, ad, int(rng.integers(-16, 17)) if cfl else 0,
+                                        fim, 0, mlw, mlh, res))
+                            decoded[p][cy:cy + (th + 3) // 4, cx:cx + (tw + 3) // 4] = True
+    f.tus = np.array(tus, dtype=INTRA_TU_DTYPE)
+    f.coeffs = np.concatenate(coeffs).astype(np.int32) if coeffs else np.zeros(1, np.int32)
+    return f
