@@ -57,10 +57,10 @@ def test_intra_rejects_split_superblock():
     abi.load()
     f = synth.make_intra_frame(seed=88, width=128, height=64)
     tus = f.tus.copy()
-    # move the first TU of the second superblock to the end: the superblock is no longer contiguous
-    sb = (tus["x"].astype(int) << 0) // 64
-    k = int(np.argmax((tus["plane"] == 0) & (sb == 1)))
-    f.tus = np.concatenate([tus[:k], tus[k + 1:], tus[k:k + 1]])
+    # move the first luma TU of the second superblock to the front: that superblock's
+    # TUs are no longer contiguous in decode order
+    k = int(np.argmax((tus["plane"] == 0) & (tus["x"] >= 64)))
+    f.tus = np.concatenate([tus[k:k + 1], tus[:k], tus[k + 1:]])
     d = postfilter.DeviceIntra(f)
     with pytest.raises(abi.Av1gError):
         postfilter.run_intra([d])
