@@ -321,6 +321,129 @@ typedef struct av1g_intra_job {
  * level across all frames, each superblock's TUs in decode order. */
 av1g_status av1g_run_intra(const av1g_intra_job* jobs, int32_t n, void* stream);
 
+/* ---------------------------------------------------------------------
+ * Inter prediction
+ * ------------------------------------------------------------------- */
+
+/* One reference-store entry as the inter predictor reads it: the stored
+ * (cropped, upscaled, pre-grain) planes and the stored frame's LUMA extents,
+ * which serve both as RefUpscaledWidth / RefFrameHeight of the §7.11.3.3
+ * scale and as the clamp extents of §7.11.3.4 / §7.11.3.5
+ * (RefFrameStoreEntry as built at src/decoder/frame_driver.rs:566-583).
+ * Each plane must hold at least ((upscaled_width + ss) >> ss) x
+ * ((frame_height + ss) >> ss) samples.  planes: device. */
+typedef struct av1g_ref_frame {
+    av1g_plane planes[3];
+    int32_t upscaled_width;
+    int32_t frame_height;
+} av1g_ref_frame;
+
+/* WarpDriverParams (src/inter_pred.rs:1420-1429): the useWarp inputs of one
+ * prediction, per reference list. */
+typedef struct av1g_warp_ctx {
+    int32_t gm_params[2][6];
+    int32_t local_warp_params[6];
+    uint8_t y_mode[2];
+    uint8_t gm_type[2];
+    uint8_t local_valid;
+    uint8_t ref_is_scaled[2];
+    uint8_t force_integer_mv;
+} av1g_warp_ctx;
+
+/* ObmcNeighbour (src/inter_pred.rs:1430-1437): one above or left neighbour
+ * of an OBMC block.  ref: 0..6 = LAST_FRAME..ALTREF_FRAME; axis_pos4: the
+ * neighbour's mi column (above pass) or mi row (left pass). */
+typedef struct av1g_obmc_neighbour {
+    int16_t mv[2];
+    uint16_t axis_pos4;
+    uint8_t ref;
+    uint8_t step4;
+    uint8_t filter_x;
+    uint8_t filter_y;
+    uint8_t pad[2];
+} av1g_obmc_neighbour;
+
+/* kind of av1g_inter_pred */
+#define AV1G_INTER_SINGLE     0
+#define AV1G_INTER_COMPOUND   1
+#define AV1G_INTER_INTRA      2   /* IsInterIntra: blends with CurrFrame */
+
+/* One predict_inter call (src/inter_pred.rs:2100-2510) together with the
+ * CurrFrame write of its caller (reconstruct_inter_block*,
+ * inter_pred.rs:4881-6010: the w x h prediction clipped to the plane).
+ * x, y, w, h are in the plane's samples; the subsampling of plane > 0 is the
+ * header's.  filter_x = InterpFilter[1], filter_y = InterpFilter[0], 0..5.
+ * mv[list] = {row, col} in 1/8 luma samples.  compound_type: 0 WEDGE,
+ * 1 DIFFWTD, 2 AVERAGE, 4 DISTANCE (with fwd/bck_weight).  Wedge masks use
+ * mi_size (the luma block size), wedge_index and wedge_sign; an inter-intra
+ * wedge uses wedge_sign 0.  A DIFFWTD chroma call reads the mask its block's
+ * plane-0 call computed (the mask of the luma samples at (x << ss, y << ss)),
+ * so list the plane-0 call of each DIFFWTD block too.  AV1G_INTER_INTRA
+ * blends with the intra prediction the CurrFrame region holds on entry.
+ * warp: index into the job's warps (-1: no warp context).  motion_mode 1
+ * (OBMC) uses obmc_above + obmc_left neighbours from obmc_first (above ones
+ * first) with the ObmcParams fields below (inter_pred.rs:1438-1450).
+ * Calls of one job must cover disjoint CurrFrame regions. */
+typedef struct av1g_inter_pred {
+    uint16_t x;
+    uint16_t y;
+    uint16_t w;
+    uint16_t h;
+    uint8_t plane;
+    uint8_t kind;
+    uint8_t motion_mode;        /* 0 SIMPLE, 1 OBMC, 2 WARPED_CAUSAL */
+    uint8_t filter_x;
+    uint8_t filter_y;
+    uint8_t ref[2];
+    uint8_t compound_type;
+    int16_t mv[2][2];
+    uint8_t mi_size;
+    uint8_t wedge_index;
+    uint8_t wedge_sign;
+    uint8_t mask_type;
+    uint8_t interintra_mode;    /* II_DC_PRED..II_SMOOTH_PRED */
+    uint8_t wedge_interintra;
+    uint8_t fwd_weight;
+    uint8_t bck_weight;
+    int32_t warp;
+    uint32_t obmc_first;
+    uint8_t obmc_above;
+    uint8_t obmc_left;
+    uint8_t avail_u;
+    uint8_t avail_l;
+    uint8_t plane_residual_ge_8x8;
+    uint8_t mi_width_log2;
+    uint8_t mi_height_log2;
+    uint8_t pad;
+    uint16_t mi_row;
+    uint16_t mi_col;
+} av1g_inter_pred;
+
+/* A frame's inter predictions.  hdr gives bit depth, subsampling, FrameWidth
+ * / FrameHeight (frame_width, frame_height: the §7.11.3.3 scale divisors)
+ * and mi dims; refs: 7 entries, LAST_FRAME..ALTREF_FRAME. */
+typedef struct av1g_inter_job {
+    const av1g_frame_header* hdr;           /* host */
+    const av1g_ref_frame* refs;             /* host array of 7 */
+    const av1g_inter_pred* preds;           /* host */
+    int32_t num_preds;
+    const av1g_obmc_neighbour* neighbours;  /* host */
+    int32_t num_neighbours;
+    const av1g_warp_ctx* warps;             /* host */
+    int32_t num_warps;
+    av1g_plane planes[3];                   /* CurrFrame, device, written */
+} av1g_inter_job;
+
+/* §7.11.3 inter prediction for every listed call of `n` frames: motion
+ * vector scaling (§7.11.3.3), 8-tap sub-sample interpolation with scaled
+ * references (§7.11.3.4), local / global warp (§7.11.3.5-6), OBMC
+ * (§7.11.3.9-10), wedge / difference-weight / inter-intra masks and blends
+ * (§7.11.3.11-14), distance weights (§7.11.3.15).  Replaces predict_inter
+ * (src/inter_pred.rs:2100) as called by reconstruct_inter_block,
+ * _warp, _obmc, _compound and _interintra (inter_pred.rs:4881-6010).
+ * One launch for all frames, plus one for DIFFWTD chroma calls. */
+av1g_status av1g_run_inter(const av1g_inter_job* jobs, int32_t n, void* stream);
+
 /* Launch modes for av1g_run_postfilter. */
 #define AV1G_MODE_BATCHED 0     /* one launch per stage across all jobs    */
 #define AV1G_MODE_PER_FRAME 1   /* one launch per stage per frame          */

@@ -226,3 +226,57 @@ def intra(frame):
     lib.ora_intra_frame(C.byref(frame.hdr), C.byref(frame.quant), tus.ctypes.data_as(C.c_void_p), len(tus),
                         _ptr(coeffs), _planes(planes))
     return planes
+
+
+def _struct_ptr(a):
+    return a.ctypes.data_as(C.c_void_p) if len(a) else None
+
+
+def inter(frame):
+    """Every inter prediction call in list order on int32 copies of the planes.
+
+    Returns (planes, rc): rc is 0, or 1 + the index of the first call the
+    reference rejects."""
+    lib = load()
+    abi = _abi_module()
+    planes = [np.ascontiguousarray(p, dtype=np.int32) for p in frame.planes]
+    refs = (abi.RefFrame * 7)()
+    ref_planes = (OraPlane * 21)()
+    keep = []
+    for r in range(7):
+        refs[r].upscaled_width = frame.refs[r]["upscaled_width"]
+        refs[r].frame_height = frame.refs[r]["frame_height"]
+        for p in range(3):
+            a = np.ascontiguousarray(frame.refs[r]["planes"][p], dtype=np.int32)
+            keep.append(a)
+            ref_planes[r * 3 + p] = OraPlane(_ptr(a), a.shape[0], a.shape[1])
+    preds = np.ascontiguousarray(frame.preds)
+    nb = np.ascontiguousarray(frame.neighbours)
+    warps = np.ascontiguousarray(frame.warps)
+    rc = lib.ora_inter_frame(C.byref(frame.hdr), refs, ref_planes, _struct_ptr(preds), len(preds),
+                             _struct_ptr(nb), len(nb), _struct_ptr(warps), len(warps), _planes(planes))
+    return planes, rc
+
+
+def mv_scaling(plane, ssx, ssy, fw, fh, ruw, rh, x, y, mv_row, mv_col):
+    lib = load()
+    out = (C.c_int32 * 4)()
+    rc = lib.ora_mv_scaling(plane, ssx, ssy, fw, fh, ruw, rh, x, y, mv_row, mv_col, out)
+    return None if rc else tuple(out)
+
+
+def setup_shear(params):
+    lib = load()
+    p = (C.c_int32 * 6)(*params)
+    out = (C.c_int32 * 5)()
+    rc = lib.ora_setup_shear(p, out)
+    return None if rc else tuple(out)
+
+
+def wedge_mask(mi_size, wedge_index, wedge_sign):
+    lib = load()
+    w = [4, 4, 8, 8, 8, 16, 16, 16, 32, 32, 32, 64, 64, 64, 128, 128, 4, 16, 8, 32, 16, 64][mi_size]
+    h = [4, 8, 4, 8, 16, 8, 16, 32, 16, 32, 64, 32, 64, 128, 64, 128, 16, 4, 32, 8, 64, 16][mi_size]
+    m = np.zeros((h, w), np.uint8)
+    rc = lib.ora_wedge_mask(mi_size, wedge_index, wedge_sign, m.ctypes.data_as(C.c_void_p))
+    return None if rc else m

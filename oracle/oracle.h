@@ -96,6 +96,23 @@ void ora_intra_predict(const ora_plane* p, int sx, int sy, int tx, int mode, int
 void ora_intra_frame(const av1g_frame_header* hdr, const av1g_quant_params* q, const av1g_intra_tu* tus, int n,
                      const int32_t* coeffs, ora_plane planes[3]);
 
+/* Every inter prediction call of a frame in list order (predict_inter,
+ * src/inter_pred.rs:2100, with the CurrFrame copy of its
+ * reconstruct_inter_block* caller).  refs: dims of the 7 references;
+ * ref_planes: their int32 planes, [ref * 3 + plane].  Returns 0, or
+ * 1 + the index of the first call the reference rejects. */
+int ora_inter_frame(const av1g_frame_header* hdr, const av1g_ref_frame* refs, const ora_plane* ref_planes,
+                    const av1g_inter_pred* preds, int n, const av1g_obmc_neighbour* nb, int n_nb,
+                    const av1g_warp_ctx* warps, int n_warps, ora_plane planes[3]);
+
+/* motion_vector_scaling (inter_pred.rs:318): out = startX, startY, stepX, stepY. */
+int ora_mv_scaling(int plane, int ssx, int ssy, int fw, int fh, int ruw, int rh, int x, int y, int mv_row,
+                   int mv_col, int32_t out[4]);
+/* setup_shear (inter_pred.rs:3982): out = alpha, beta, gamma, delta, warpValid; -1 for None. */
+int ora_setup_shear(const int32_t p[6], int32_t out[5]);
+/* wedge_mask (inter_pred.rs:2844) into a block_width x block_height mask. */
+int ora_wedge_mask(int mi_size, int idx, int sign, uint8_t* mask);
+
 #ifdef __cplusplus
 }
 #endif

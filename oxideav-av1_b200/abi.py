@@ -120,13 +120,51 @@ class IntraJob(C.Structure):
                 ("num_tus", C.c_int32), ("sb_size", C.c_int32), ("coeffs", C.c_void_p), ("planes", Plane * 3)]
 
 
+class RefFrame(C.Structure):
+    _fields_ = [("planes", Plane * 3), ("upscaled_width", C.c_int32), ("frame_height", C.c_int32)]
+
+
+class WarpCtx(C.Structure):
+    _fields_ = [("gm_params", (C.c_int32 * 6) * 2), ("local_warp_params", C.c_int32 * 6),
+                ("y_mode", C.c_uint8 * 2), ("gm_type", C.c_uint8 * 2), ("local_valid", C.c_uint8),
+                ("ref_is_scaled", C.c_uint8 * 2), ("force_integer_mv", C.c_uint8)]
+
+
+class ObmcNeighbour(C.Structure):
+    _fields_ = [("mv", C.c_int16 * 2), ("axis_pos4", C.c_uint16), ("ref", C.c_uint8), ("step4", C.c_uint8),
+                ("filter_x", C.c_uint8), ("filter_y", C.c_uint8), ("pad", C.c_uint8 * 2)]
+
+
+class InterPred(C.Structure):
+    _fields_ = [("x", C.c_uint16), ("y", C.c_uint16), ("w", C.c_uint16), ("h", C.c_uint16),
+                ("plane", C.c_uint8), ("kind", C.c_uint8), ("motion_mode", C.c_uint8), ("filter_x", C.c_uint8),
+                ("filter_y", C.c_uint8), ("ref", C.c_uint8 * 2), ("compound_type", C.c_uint8),
+                ("mv", (C.c_int16 * 2) * 2), ("mi_size", C.c_uint8), ("wedge_index", C.c_uint8),
+                ("wedge_sign", C.c_uint8), ("mask_type", C.c_uint8), ("interintra_mode", C.c_uint8),
+                ("wedge_interintra", C.c_uint8), ("fwd_weight", C.c_uint8), ("bck_weight", C.c_uint8),
+                ("warp", C.c_int32), ("obmc_first", C.c_uint32), ("obmc_above", C.c_uint8),
+                ("obmc_left", C.c_uint8), ("avail_u", C.c_uint8), ("avail_l", C.c_uint8),
+                ("plane_residual_ge_8x8", C.c_uint8), ("mi_width_log2", C.c_uint8),
+                ("mi_height_log2", C.c_uint8), ("pad", C.c_uint8), ("mi_row", C.c_uint16), ("mi_col", C.c_uint16)]
+
+
+class InterJob(C.Structure):
+    _fields_ = [("hdr", C.POINTER(FrameHeader)), ("refs", C.POINTER(RefFrame)), ("preds", C.c_void_p),
+                ("num_preds", C.c_int32), ("neighbours", C.c_void_p), ("num_neighbours", C.c_int32),
+                ("warps", C.c_void_p), ("num_warps", C.c_int32), ("planes", Plane * 3)]
+
+
+INTER_SINGLE, INTER_COMPOUND, INTER_INTRA = 0, 1, 2
+
 INTRA_HAVE_ABOVE, INTRA_HAVE_LEFT, INTRA_HAVE_ABOVE_RIGHT, INTRA_HAVE_BELOW_LEFT = 1, 2, 4, 8
 INTRA_EDGE_FILTER, INTRA_FILTER_TYPE, INTRA_RESIDUAL, INTRA_CFL = 16, 32, 64, 128
 
 _STRUCTS = {"av1g_film_grain": FilmGrain, "av1g_frame_header": FrameHeader, "av1g_lr_unit": LrUnit,
             "av1g_mi_grid": MiGrid, "av1g_plane": Plane, "av1g_frame_job": FrameJob,
             "av1g_quant_params": QuantParams, "av1g_tu": Tu, "av1g_recon_job": ReconJob,
-            "av1g_intra_tu": IntraTu, "av1g_intra_job": IntraJob}
+            "av1g_intra_tu": IntraTu, "av1g_intra_job": IntraJob, "av1g_ref_frame": RefFrame,
+            "av1g_warp_ctx": WarpCtx, "av1g_obmc_neighbour": ObmcNeighbour, "av1g_inter_pred": InterPred,
+            "av1g_inter_job": InterJob}
 
 # exported entry points and their ctypes signatures
 _SIGS = {
@@ -144,6 +182,7 @@ _SIGS = {
     "av1g_run_film_grain_noalloc": (C.c_int, [C.POINTER(FrameJob), C.c_int32, C.c_void_p]),
     "av1g_run_recon": (C.c_int, [C.POINTER(ReconJob), C.c_int32, C.c_void_p]),
     "av1g_run_intra": (C.c_int, [C.POINTER(IntraJob), C.c_int32, C.c_void_p]),
+    "av1g_run_inter": (C.c_int, [C.POINTER(InterJob), C.c_int32, C.c_void_p]),
 }
 
 NOALLOC_MAX_FRAMES = 16

@@ -24,6 +24,7 @@ namespace av1g {
 size_t lr_smem_bytes();
 av1g_status recon_run(const av1g_recon_job* jobs, int n, cudaStream_t s, std::string& err);
 av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t s, std::string& err);
+av1g_status inter_run(const av1g_inter_job* jobs, int n, cudaStream_t s, std::string& err);
 }
 
 using namespace av1g;
@@ -324,6 +325,11 @@ int32_t av1g_struct_size(const char* name) {
     if (!strcmp(name, "av1g_recon_job")) return (int32_t)sizeof(av1g_recon_job);
     if (!strcmp(name, "av1g_intra_tu")) return (int32_t)sizeof(av1g_intra_tu);
     if (!strcmp(name, "av1g_intra_job")) return (int32_t)sizeof(av1g_intra_job);
+    if (!strcmp(name, "av1g_ref_frame")) return (int32_t)sizeof(av1g_ref_frame);
+    if (!strcmp(name, "av1g_warp_ctx")) return (int32_t)sizeof(av1g_warp_ctx);
+    if (!strcmp(name, "av1g_obmc_neighbour")) return (int32_t)sizeof(av1g_obmc_neighbour);
+    if (!strcmp(name, "av1g_inter_pred")) return (int32_t)sizeof(av1g_inter_pred);
+    if (!strcmp(name, "av1g_inter_job")) return (int32_t)sizeof(av1g_inter_job);
     return -1;
 }
 
@@ -361,6 +367,15 @@ av1g_status av1g_run_intra(const av1g_intra_job* jobs, int32_t n, void* stream) 
     if (n == 0) return AV1G_OK;
     std::string err;
     av1g_status st = intra_run(jobs, n, (cudaStream_t)stream, err);
+    if (st != AV1G_OK) g_err = err;
+    return st;
+}
+av1g_status av1g_run_inter(const av1g_inter_job* jobs, int32_t n, void* stream) {
+    g_err.clear();
+    if (n < 0 || (n > 0 && !jobs)) return fail(AV1G_EINVAL, "bad job array");
+    if (n == 0) return AV1G_OK;
+    std::string err;
+    av1g_status st = inter_run(jobs, n, (cudaStream_t)stream, err);
     if (st != AV1G_OK) g_err = err;
     return st;
 }

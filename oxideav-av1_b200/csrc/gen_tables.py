@@ -39,6 +39,17 @@ TABLES = [
     ("src/inter_pred.rs", "DIV_LUT", "int16_t"),
     ("src/inter_pred.rs", "WEDGE_CODEBOOK", "uint8_t"),
     ("src/inter_pred.rs", "QUANT_DIST_LOOKUP", "int8_t"),
+    ("src/inter_pred.rs", "QUANT_DIST_WEIGHT", "int8_t"),
+    ("src/inter_pred.rs", "WEDGE_MASTER_OBLIQUE_ODD", "uint8_t"),
+    ("src/inter_pred.rs", "WEDGE_MASTER_OBLIQUE_EVEN", "uint8_t"),
+    ("src/inter_pred.rs", "WEDGE_MASTER_VERTICAL", "uint8_t"),
+    ("src/inter_pred.rs", "WEDGE_BITS", "uint8_t"),
+    ("src/inter_pred.rs", "II_WEIGHTS_1D", "uint8_t"),
+    ("src/inter_pred.rs", "OBMC_MASK_2", "uint8_t"),
+    ("src/inter_pred.rs", "OBMC_MASK_4", "uint8_t"),
+    ("src/inter_pred.rs", "OBMC_MASK_8", "uint8_t"),
+    ("src/inter_pred.rs", "OBMC_MASK_16", "uint8_t"),
+    ("src/inter_pred.rs", "OBMC_MASK_32", "uint8_t"),
     ("src/cdf.rs", "INTRA_FILTER_TAPS", "int16_t"),
     ("src/cdf.rs", "SM_WEIGHTS_TX_4X4", "uint8_t"),
     ("src/cdf.rs", "SM_WEIGHTS_TX_8X8", "uint8_t"),

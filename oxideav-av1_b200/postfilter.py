@@ -224,3 +224,53 @@ def run_intra(frames, stream=None):
         arr[i] = f.job()
     abi.check(lib.av1g_run_intra(arr, len(frames), _stream_ptr(stream)))
     return arr
+
+
+class DeviceInter:
+    """An inter frame on the GPU: CurrFrame planes (written in place), the 7
+    reference planes, and the host call / neighbour / warp lists."""
+
+    def __init__(self, frame, device="cuda"):
+        self.frame = frame
+        h = frame.hdr
+        hbd = h.bit_depth > 8
+        self.planes = [DevPlane(*frame.plane_dims(p), hbd, device, frame.planes[p]) for p in range(h.num_planes)]
+        self.refs = (abi.RefFrame * 7)()
+        self.ref_planes = []
+        for r, ref in enumerate(frame.refs):
+            self.refs[r].upscaled_width = ref["upscaled_width"]
+            self.refs[r].frame_height = ref["frame_height"]
+            for p in range(h.num_planes):
+                a = ref["planes"][p]
+                dp = DevPlane(a.shape[0], a.shape[1], hbd, device, a)
+                self.ref_planes.append(dp)
+                self.refs[r].planes[p] = dp.cplane()
+        self.preds = np.ascontiguousarray(frame.preds)
+        self.neighbours = np.ascontiguousarray(frame.neighbours)
+        self.warps = np.ascontiguousarray(frame.warps)
+
+    def job(self):
+        j = abi.InterJob()
+        j.hdr = C.pointer(self.frame.hdr)
+        j.refs = C.cast(self.refs, C.POINTER(abi.RefFrame))
+        j.preds = self.preds.ctypes.data if len(self.preds) else None
+        j.num_preds = len(self.preds)
+        j.neighbours = self.neighbours.ctypes.data if len(self.neighbours) else None
+        j.num_neighbours = len(self.neighbours)
+        j.warps = self.warps.ctypes.data if len(self.warps) else None
+        j.num_warps = len(self.warps)
+        for p, pl in enumerate(self.planes):
+            j.planes[p] = pl.cplane()
+        return j
+
+    def download(self):
+        return [pl.download() for pl in self.planes]
+
+
+def run_inter(frames, stream=None):
+    lib = abi.load()
+    arr = (abi.InterJob * len(frames))()
+    for i, f in enumerate(frames):
+        arr[i] = f.job()
+    abi.check(lib.av1g_run_inter(arr, len(frames), _stream_ptr(stream)))
+    return arr

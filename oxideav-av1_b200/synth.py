@@ -533,3 +533,246 @@ def make_intra_frame(seed, width=176, height=144, bit_depth=8, ssx=1, ssy=1, mon
     f.tus = np.array(tus, dtype=INTRA_TU_DTYPE)
     f.coeffs = np.concatenate(coeffs).astype(np.int32) if coeffs else np.zeros(1, np.int32)
     return f
+
+
+# ---------------------------------------------------------------------------
+# Inter prediction calls
+# ---------------------------------------------------------------------------
+
+INTER_DTYPE = np.dtype([("x", np.uint16), ("y", np.uint16), ("w", np.uint16), ("h", np.uint16),
+                        ("plane", np.uint8), ("kind", np.uint8), ("motion_mode", np.uint8),
+                        ("filter_x", np.uint8), ("filter_y", np.uint8), ("ref", np.uint8, (2,)),
+                        ("compound_type", np.uint8), ("mv", np.int16, (2, 2)), ("mi_size", np.uint8),
+                        ("wedge_index", np.uint8), ("wedge_sign", np.uint8), ("mask_type", np.uint8),
+                        ("interintra_mode", np.uint8), ("wedge_interintra", np.uint8), ("fwd_weight", np.uint8),
+                        ("bck_weight", np.uint8), ("warp", np.int32), ("obmc_first", np.uint32),
+                        ("obmc_above", np.uint8), ("obmc_left", np.uint8), ("avail_u", np.uint8),
+                        ("avail_l", np.uint8), ("plane_residual_ge_8x8", np.uint8), ("mi_width_log2", np.uint8),
+                        ("mi_height_log2", np.uint8), ("pad", np.uint8), ("mi_row", np.uint16),
+                        ("mi_col", np.uint16)], align=True)
+assert INTER_DTYPE.itemsize == C.sizeof(abi.InterPred)
+NB_DTYPE = np.dtype([("mv", np.int16, (2,)), ("axis_pos4", np.uint16), ("ref", np.uint8), ("step4", np.uint8),
+                     ("filter_x", np.uint8), ("filter_y", np.uint8), ("pad", np.uint8, (2,))], align=True)
+assert NB_DTYPE.itemsize == C.sizeof(abi.ObmcNeighbour)
+WARP_DTYPE = np.dtype([("gm_params", np.int32, (2, 6)), ("local_warp_params", np.int32, (6,)),
+                       ("y_mode", np.uint8, (2,)), ("gm_type", np.uint8, (2,)), ("local_valid", np.uint8),
+                       ("ref_is_scaled", np.uint8, (2,)), ("force_integer_mv", np.uint8)], align=True)
+assert WARP_DTYPE.itemsize == C.sizeof(abi.WarpCtx)
+
+BLOCK_W = [4, 4, 8, 8, 8, 16, 16, 16, 32, 32, 32, 64, 64, 64, 128, 128, 4, 16, 8, 32, 16, 64]
+BLOCK_H = [4, 8, 4, 8, 16, 8, 16, 32, 16, 32, 64, 32, 64, 128, 64, 128, 16, 4, 32, 8, 64, 16]
+WEDGE_OK = {3, 4, 5, 6, 7, 8, 9, 18, 19}        # blocks with WEDGE_BITS > 0
+DIST_WEIGHTS = [(9, 7), (11, 5), (12, 4), (13, 3), (7, 9), (5, 11), (4, 12), (3, 13)]
+SUBSAMPLED = None
+
+
+class InterFrame(ReconFrame):
+    """CurrFrame planes on entry, the 7 references and the predict_inter calls."""
+
+    def __init__(self):
+        super().__init__()
+        self.refs = []
+        self.preds = None
+        self.neighbours = None
+        self.warps = None
+
+
+def _warp_params(rng, valid=True, tx=0, ty=0):
+    spread = 1500 if valid else 30000
+    a, b, c, d = (int(v) for v in rng.integers(-spread, spread + 1, size=4))
+    return [int(tx * 65536 + rng.integers(-20000, 20000)), int(ty * 65536 + rng.integers(-20000, 20000)),
+            65536 + a, b, c, 65536 + d]
+
+
+def _subsampled(mi_size, ssx, ssy):
+    global SUBSAMPLED
+    if SUBSAMPLED is None:
+        from . import tables
+        SUBSAMPLED = tables.SUBSAMPLED_SIZE
+    return int(SUBSAMPLED[mi_size][ssx][ssy])
+
+
+def make_inter_frame(seed, width=176, height=144, bit_depth=8, ssx=1, ssy=1, mono=False, scaled=True,
+                     sb_size=64, overhang=True, p_intra=0.12, ref_dims=None):
+    """A frame of inter blocks over a random partition: single, compound
+    (average / distance / wedge / difference weight), inter-intra (smooth and
+    wedge), OBMC with neighbour lists walked like obmc_dispatch_leaf
+    (src/inter_pred.rs:6519), local and global warp; references of other sizes
+    (2x, 1/2, 1.5x and a 3x one past the spec's 2x limit) when `scaled`."""
+    rng = np.random.default_rng(seed)
+    f = InterFrame()
+    h = f.hdr
+    h.frame_width = h.upscaled_width = width
+    h.frame_height = height
+    h.mi_cols, h.mi_rows = 2 * ((width + 7) >> 3), 2 * ((height + 7) >> 3)
+    h.bit_depth = bit_depth
+    h.num_planes = 1 if mono else 3
+    h.subsampling_x, h.subsampling_y = (1, 1) if mono else (ssx, ssy)
+    maxv = (1 << bit_depth) - 1
+    dt = np.uint8 if bit_depth == 8 else np.uint16
+    if ref_dims is None:
+        ref_dims = [(width, height)] * 7
+        if scaled:
+            ref_dims[3] = (2 * width, 2 * height)
+            ref_dims[4] = ((width + 1) // 2, (height + 1) // 2)
+            ref_dims[5] = (width * 3 // 2 + 3, height * 3 // 2 - 1)
+            ref_dims[6] = (3 * width, 3 * height)
+    for r in range(7):
+        uw, rh = ref_dims[r]
+        planes = []
+        for p in range(3):
+            sx_, sy_ = (h.subsampling_x, h.subsampling_y) if p else (0, 0)
+            if p < h.num_planes:
+                planes.append(_plane(rng, (rh + sy_) >> sy_, (uw + sx_) >> sx_, bit_depth))
+            else:
+                planes.append(np.zeros((1, 1), dt))
+        f.refs.append({"planes": planes, "upscaled_width": uw, "frame_height": rh})
+    f.planes = [rng.integers(0, maxv + 1, size=f.plane_dims(p)).astype(dt) for p in range(h.num_planes)]
+    scaled_ref = [ref_dims[r] != (width, height) for r in range(7)]
+
+    pw, ph = h.mi_cols * 4, h.mi_rows * 4
+    blocks = []
+    ext = 16 if overhang else 0   # edge blocks may run past the plane (the write is clipped)
+    for sby in range(0, ph, sb_size):
+        for sbx in range(0, pw, sb_size):
+            if overhang and sb_size == 128 and rng.random() < 0.3 and sbx + 128 <= pw + 64:
+                blocks.append((sbx, sby, 128, 128))
+                continue
+            _blocks(rng, sbx, sby, sb_size, pw + ext, ph + ext, blocks)
+    blocks = [b for b in blocks if b[0] < pw and b[1] < ph]
+    mi_map = -np.ones((h.mi_rows, h.mi_cols), np.int64)
+    info = []
+    for bi, (x0, y0, bw, bh) in enumerate(blocks):
+        mi_size = BLOCK_OF[(bw // 4, bh // 4)]
+        intra = rng.random() < p_intra
+        mvs = rng.integers(-160, 161, size=(2, 2))
+        if rng.random() < 0.1:
+            mvs = rng.integers(-2400, 2401, size=(2, 2))   # far outside the reference
+        info.append({"mi_size": mi_size, "intra": intra, "ref": [int(rng.integers(0, 7)), int(rng.integers(0, 7))],
+                     "mv": mvs, "fx": int(rng.integers(0, 4)), "fy": int(rng.integers(0, 4))})
+        if rng.random() < 0.03:
+            info[-1]["fx"] = int(rng.integers(4, 6))
+        r0, c0 = y0 // 4, x0 // 4
+        mi_map[r0:r0 + bh // 4, c0:c0 + bw // 4] = bi
+
+    preds, nbs, warps = [], [], []
+    for bi, (x0, y0, bw, bh) in enumerate(blocks):
+        b = info[bi]
+        if b["intra"]:
+            continue
+        mi_size, mi_row, mi_col = b["mi_size"], y0 // 4, x0 // 4
+        big = min(bw, bh) >= 8
+        r = rng.random()
+        kind, ctype, mmode, ii_mode, wii = abi.INTER_SINGLE, 2, 0, 0, 0
+        warp = -1
+        if big and r < 0.35:
+            kind = abi.INTER_COMPOUND
+            choices = [2, 4, 1] + ([0] if mi_size in WEDGE_OK else [])
+            ctype = int(rng.choice(choices))
+        elif big and r < 0.45 and bw <= 32 and bh <= 32:
+            kind = abi.INTER_INTRA
+            ii_mode = int(rng.integers(0, 4))
+            wii = int(mi_size in WEDGE_OK and rng.random() < 0.5)
+        elif big and r < 0.65:
+            mmode = 1
+        elif big and r < 0.78:
+            mmode = 2
+        w = {}
+        if mmode == 2 or (big and rng.random() < 0.25):
+            wc = np.zeros((), WARP_DTYPE)
+            glob = rng.random() < 0.6
+            wc["y_mode"][:] = (24 if kind == abi.INTER_COMPOUND else 16) if glob else 13
+            wc["gm_type"][:] = rng.integers(1, 4, size=2)
+            for l in range(2):
+                wc["gm_params"][l] = _warp_params(rng, rng.random() < 0.9, b["mv"][l][1] / 8, b["mv"][l][0] / 8)
+            wc["local_warp_params"] = _warp_params(rng, rng.random() < 0.85, b["mv"][0][1] / 8, b["mv"][0][0] / 8)
+            wc["local_valid"] = int(rng.random() < 0.9)
+            wc["ref_is_scaled"] = [scaled_ref[b["ref"][0]], scaled_ref[b["ref"][1]]]
+            wc["force_integer_mv"] = int(rng.random() < 0.05)
+            warp = len(warps)
+            warps.append(wc)
+        obmc_first, n_above, n_left = len(nbs), 0, 0
+        avail_u, avail_l = int(mi_row > 0), int(mi_col > 0)
+        if mmode == 1:
+            w4, h4 = bw // 4, bh // 4
+            wl2, hl2 = w4.bit_length() - 1, h4.bit_length() - 1
+            if avail_u:
+                x4, n = mi_col, 0
+                while n < min(4, wl2) and x4 < min(h.mi_cols, mi_col + w4):
+                    cc = min(x4 | 1, h.mi_cols - 1)
+                    cand = mi_map[mi_row - 1, cc]
+                    ci = info[cand]
+                    step4 = min(max(BLOCK_W[ci["mi_size"]] // 4, 2), 16)
+                    if not ci["intra"]:
+                        n += 1
+                        nbs.append((ci["mv"][0], x4, ci["ref"][0], step4, ci["fx"], ci["fy"]))
+                        n_above += 1
+                    x4 += step4
+            if avail_l:
+                y4, n = mi_row, 0
+                while n < min(4, hl2) and y4 < min(h.mi_rows, mi_row + h4):
+                    cr = min(y4 | 1, h.mi_rows - 1)
+                    cand = mi_map[cr, mi_col - 1]
+                    ci = info[cand]
+                    step4 = min(max(BLOCK_H[ci["mi_size"]] // 4, 2), 16)
+                    if not ci["intra"]:
+                        n += 1
+                        nbs.append((ci["mv"][0], y4, ci["ref"][0], step4, ci["fx"], ci["fy"]))
+                        n_left += 1
+                    y4 += step4
+        wedge_index, wedge_sign = int(rng.integers(0, 16)), int(rng.integers(0, 2))
+        mask_type = int(rng.integers(0, 2))
+        fwd, bck = DIST_WEIGHTS[int(rng.integers(0, len(DIST_WEIGHTS)))]
+        for p in range(h.num_planes):
+            sx_, sy_ = (h.subsampling_x, h.subsampling_y) if p else (0, 0)
+            cw, chh = bw >> sx_, bh >> sy_
+            if cw < 2 or chh < 2:
+                continue
+            ge8 = _subsampled(mi_size, sx_, sy_) >= 3
+            preds.append(((x0 >> sx_), (y0 >> sy_), cw, chh, p, kind, mmode, b["fx"], b["fy"], b["ref"], ctype,
+                          b["mv"], mi_size, wedge_index, wedge_sign, mask_type, ii_mode, wii, fwd, bck, warp,
+                          obmc_first, n_above, n_left, avail_u, avail_l, int(ge8), (bw // 4).bit_length() - 1,
+                          (bh // 4).bit_length() - 1, 0, mi_row, mi_col))
+    f.preds = np.zeros(len(preds), INTER_DTYPE)
+    for i, t in enumerate(preds):
+        f.preds[i] = t
+    f.neighbours = np.zeros(len(nbs), NB_DTYPE)
+    for i, (mv, pos, ref, step4, fx, fy) in enumerate(nbs):
+        f.neighbours[i] = (mv, pos, ref, step4, fx, fy, (0, 0))
+    f.warps = np.array(warps, WARP_DTYPE) if warps else np.zeros(0, WARP_DTYPE)
+    return f
+
+
+def custom_inter_frame(width, height, refs, calls, neighbours=(), warps=(), bit_depth=8, ssx=1, ssy=1,
+                       mono=True, fill=0):
+    """A hand-built inter frame: refs = list of (upscaled_width, frame_height,
+    [plane arrays]) (padded to 7 with copies of the first), calls = dicts of
+    av1g_inter_pred fields (missing ones zero, warp -1)."""
+    f = InterFrame()
+    h = f.hdr
+    h.frame_width = h.upscaled_width = width
+    h.frame_height = height
+    h.mi_cols, h.mi_rows = 2 * ((width + 7) >> 3), 2 * ((height + 7) >> 3)
+    h.bit_depth = bit_depth
+    h.num_planes = 1 if mono else 3
+    h.subsampling_x, h.subsampling_y = (1, 1) if mono else (ssx, ssy)
+    dt = np.uint8 if bit_depth == 8 else np.uint16
+    refs = list(refs) + [refs[0]] * (7 - len(refs))
+    for uw, rh, planes in refs:
+        ps = [np.asarray(p, dt) for p in planes] + [np.zeros((1, 1), dt)] * (3 - len(planes))
+        f.refs.append({"planes": ps, "upscaled_width": uw, "frame_height": rh})
+    f.planes = [np.full(f.plane_dims(p), fill, dt) for p in range(h.num_planes)]
+    f.preds = np.zeros(len(calls), INTER_DTYPE)
+    for i, c in enumerate(calls):
+        f.preds[i]["warp"] = -1
+        for k, v in c.items():
+            f.preds[i][k] = v
+    f.neighbours = np.zeros(len(neighbours), NB_DTYPE)
+    for i, c in enumerate(neighbours):
+        for k, v in c.items():
+            f.neighbours[i][k] = v
+    f.warps = np.zeros(len(warps), WARP_DTYPE)
+    for i, c in enumerate(warps):
+        for k, v in c.items():
+            f.warps[i][k] = v
+    return f
