@@ -273,6 +273,11 @@ av1g_status av1g_run_recon(const av1g_recon_job* jobs, int32_t n, void* stream);
 #define AV1G_INTRA_RESIDUAL          0x40  /* the TU has coefficients (eob>0)  */
 #define AV1G_INTRA_CFL               0x80  /* chroma-from-luma on top of DC    */
 
+/* mode values of av1g_intra_tu beyond the intra modes 0..12 */
+#define AV1G_INTRA_MODE_PALETTE  64   /* §7.11.4 palette prediction              */
+#define AV1G_INTRA_MODE_INTRABC  65   /* intra block copy from CurrFrame          */
+#define AV1G_INTRA_MODE_NONE     255  /* no prediction (residual / CfL only)     */
+
 /* One intra transform unit, in decode order, with the prediction inputs the
  * tile walker derives at transform_block_emit (src/cdf.rs:32540-32700):
  * mode is YMode for luma and UVMode for chroma with UV_CFL_PRED mapped to
@@ -280,7 +285,15 @@ av1g_status av1g_run_recon(const av1g_recon_job* jobs, int32_t n, void* stream);
  * 0..4 or 255 for none (luma only).  For CfL TUs, cfl_alpha is CflAlphaU/V and
  * max_luma_w/h are MaxLumaW/H (luma samples) of the block.  `res` is the
  * residual (used when AV1G_INTRA_RESIDUAL is set); res.x/y/plane/tx_size must
- * equal the TU's. */
+ * equal the TU's.
+ * AV1G_INTRA_MODE_PALETTE (predict_palette_tu_into_curr_frame,
+ * cdf.rs:18603): the TU's colour indices start at palette_map in the job's
+ * map pool with row stride palette_stride; palette_colors[0..palette_size).
+ * AV1G_INTRA_MODE_INTRABC (predict_intrabc_leaf_into_curr_frame,
+ * cdf.rs:19235): the TU-sized piece at (x, y) of a block predicted from the
+ * pre-filter CurrFrame with the block's mv = {row, col} (1/8 luma samples);
+ * list one piece per transform-sized part of the block, before its residual
+ * TUs. */
 typedef struct av1g_intra_tu {
     uint16_t x;
     uint16_t y;
@@ -295,6 +308,12 @@ typedef struct av1g_intra_tu {
     uint16_t max_luma_w;
     uint16_t max_luma_h;
     av1g_tu res;
+    int16_t mv[2];
+    uint32_t palette_map;
+    uint16_t palette_stride;
+    uint8_t palette_size;
+    uint8_t pad2;
+    uint16_t palette_colors[8];
 } av1g_intra_tu;
 
 /* A frame's intra work, reconstructed in place on top of whatever the
@@ -308,6 +327,8 @@ typedef struct av1g_intra_job {
     int32_t sb_size;                 /* 64 or 128 (luma samples) */
     const int32_t* coeffs;           /* device */
     av1g_plane planes[3];            /* device, updated in place */
+    const uint8_t* palette_maps;     /* host: colour-index pool of palette TUs */
+    int64_t palette_map_bytes;
 } av1g_intra_job;
 
 /* §7.11.2 intra prediction (DC, V, H, directional with edge filter and

@@ -217,15 +217,35 @@ def inverse_transform(dequant, tx, tx_type, bit_depth, lossless=False):
     return res
 
 
-def intra(frame):
-    """Every intra TU in decode order (prediction, CfL, residual) on int32 copies of the planes."""
+def intra_rc(frame):
+    """Every intra TU in decode order (prediction, CfL, residual) on int32 copies
+    of the planes; returns (planes, rc) with rc = 0 or 1 + the first rejected TU."""
     lib = load()
     planes = [np.ascontiguousarray(p, dtype=np.int32) for p in frame.planes]
     tus = np.ascontiguousarray(frame.tus)
     coeffs = np.ascontiguousarray(frame.coeffs, dtype=np.int32)
-    lib.ora_intra_frame(C.byref(frame.hdr), C.byref(frame.quant), tus.ctypes.data_as(C.c_void_p), len(tus),
-                        _ptr(coeffs), _planes(planes))
+    maps = np.ascontiguousarray(getattr(frame, "palette_maps", np.zeros(1, np.uint8)), dtype=np.uint8)
+    rc = lib.ora_intra_frame(C.byref(frame.hdr), C.byref(frame.quant), tus.ctypes.data_as(C.c_void_p), len(tus),
+                             _ptr(coeffs), _planes(planes), maps.ctypes.data_as(C.c_void_p),
+                             C.c_int64(len(getattr(frame, "palette_maps", []))))
+    return planes, rc
+
+
+def intra(frame):
+    planes, rc = intra_rc(frame)
+    if rc:
+        raise RuntimeError(f"oracle rejected intra TU {rc - 1}")
     return planes
+
+
+def intrabc_predict(plane_arr, plane, ssx, ssy, mi_cols, mi_rows, x, y, w, h, mv_row, mv_col, bd):
+    lib = load()
+    a = np.ascontiguousarray(plane_arr, dtype=np.int32)
+    p = OraPlane(_ptr(a), a.shape[0], a.shape[1])
+    out = np.zeros((h, w), np.uint16)
+    rc = lib.ora_intrabc_predict(C.byref(p), plane, ssx, ssy, mi_cols, mi_rows, x, y, w, h, mv_row, mv_col, bd,
+                                 out.ctypes.data_as(C.c_void_p))
+    return None if rc else out
 
 
 def _struct_ptr(a):

@@ -602,3 +602,39 @@ int ora_setup_shear(const int32_t p[6], int32_t out[5]) {
     return 0;
 }
 int ora_wedge_mask(int mi_size, int idx, int sign, uint8_t* mask) { return wedge_mask(mi_size, idx, sign, mask); }
+
+/* predict_intrabc_leaf_into_curr_frame (src/cdf.rs:19235-19370) for one
+ * w x h region of plane p at (x, y): BILINEAR prediction from the window of
+ * the pre-filter CurrFrame the filter can reach, clamped to the mi-padded
+ * plane.  Returns 0 or ERR. */
+int ora_intrabc_predict(const ora_plane* p, int plane, int ssx, int ssy, int mi_cols, int mi_rows, int x, int y,
+                        int w, int h, int mv_row, int mv_col, int bd, uint16_t* pred) {
+    if (abs(mv_row) >= (1 << 14) || abs(mv_col) >= (1 << 14)) return ERR;
+    int sub_x = plane ? ssx : 0, sub_y = plane ? ssy : 0;
+    int plane_rows = (mi_rows * 4) >> sub_y, plane_cols = (mi_cols * 4) >> sub_x;
+    if (plane_rows == 0 || plane_cols == 0) return ERR;
+    int32_t s[4];
+    int16_t mv[2] = {(int16_t)mv_row, (int16_t)mv_col};
+    if (mv_scaling(plane, ssx, ssy, mi_cols * 4, mi_rows * 4, mi_cols * 4, mi_rows * 4, x, y, mv, s)) return ERR;
+    int last_x = plane_cols - 1, last_y = plane_rows - 1;
+    int ih = (int)((((int64_t)h - 1) * s[3] + 1023) >> 10) + 8;
+    int y_raw0 = (s[1] >> 10) - 3, x_raw0 = (s[0] >> 10) - 3;
+    int x_raw1 = (int)(((int64_t)s[0] + (int64_t)s[2] * (w - 1)) >> 10) + 4;
+    int y0 = clip3(0, last_y, y_raw0), y1 = clip3(0, last_y, y_raw0 + ih - 1);
+    int x0 = clip3(0, last_x, x_raw0), x1 = clip3(0, last_x, x_raw1);
+    int ww = x1 - x0 + 1, wh = y1 - y0 + 1;
+    ora_plane win = {(int32_t*)malloc(sizeof(int32_t) * (size_t)ww * wh), wh, ww};
+    for (int yy = y0; yy <= y1; yy++)
+        for (int xx = x0; xx <= x1; xx++) win.s[(size_t)(yy - y0) * ww + xx - x0] = p->s[(size_t)yy * p->cols + xx];
+    int r0, r1, post;
+    rounding(bd, 0, &r0, &r1, &post);
+    int32_t* pr = (int32_t*)malloc(sizeof(int32_t) * (size_t)w * h);
+    ref_view rv = {&win, ww << sub_x, wh << sub_y};
+    int rc = block_inter(plane, ssx, ssy, rv, s[0] - (x0 << 10), s[1] - (y0 << 10), s[2], s[3], w, h, 3, 3, r0, r1, pr);
+    int maxv = (1 << bd) - 1;
+    if (!rc)
+        for (int i = 0; i < w * h; i++) pred[i] = (uint16_t)clip3(0, maxv, pr[i]);
+    free(pr);
+    free(win.s);
+    return rc;
+}

@@ -360,17 +360,46 @@ void ora_recon_frame(const av1g_frame_header* hdr, const av1g_quant_params* q, c
 
 /* Every intra TU of a frame in decode order: predict (writing the TU area
  * inside the plane), CfL, residual. */
-void ora_intra_frame(const av1g_frame_header* hdr, const av1g_quant_params* q, const av1g_intra_tu* tus, int n,
-                     const int32_t* coeffs, ora_plane planes[3]) {
+int ora_intra_frame(const av1g_frame_header* hdr, const av1g_quant_params* q, const av1g_intra_tu* tus, int n,
+                    const int32_t* coeffs, ora_plane planes[3], const uint8_t* maps, int64_t map_bytes) {
     uint16_t* pred = (uint16_t*)malloc(sizeof(uint16_t) * 64 * 64);
+    int rc = 0;
     for (int k = 0; k < n; k++) {
         const av1g_intra_tu* t = &tus[k];
         ora_plane* p = &planes[t->plane];
         int w = TW_[t->tx_size], h = TH_[t->tx_size];
-        if (t->mode < INTRA_MODES) {
+        int have_pred = t->mode < INTRA_MODES;
+        if (t->mode == AV1G_INTRA_MODE_PALETTE) {
+            /* predict_palette (cdf.rs:11907) */
+            int64_t last = (int64_t)t->palette_map + (int64_t)(h - 1) * t->palette_stride + (w - 1);
+            if (t->palette_size == 0 || t->palette_size > 8 || t->palette_stride < w || last >= map_bytes) {
+                rc = k + 1;
+                break;
+            }
+            for (int i = 0; i < h && !rc; i++)
+                for (int j = 0; j < w; j++) {
+                    int idx = maps[t->palette_map + (int64_t)i * t->palette_stride + j];
+                    if (idx >= t->palette_size) {
+                        rc = k + 1;
+                        break;
+                    }
+                    pred[i * w + j] = t->palette_colors[idx];
+                }
+            if (rc) break;
+            have_pred = 1;
+        } else if (t->mode == AV1G_INTRA_MODE_INTRABC) {
+            if (ora_intrabc_predict(p, t->plane, hdr->subsampling_x, hdr->subsampling_y, hdr->mi_cols, hdr->mi_rows,
+                                    t->x, t->y, w, h, t->mv[0], t->mv[1], hdr->bit_depth, pred)) {
+                rc = k + 1;
+                break;
+            }
+            have_pred = 1;
+        } else if (t->mode < INTRA_MODES) {
             int fim = (t->plane == 0 && t->filter_intra_mode < 5) ? t->filter_intra_mode : 255;
             ora_intra_predict(p, t->x, t->y, t->tx_size, t->mode, t->angle_delta, hdr->bit_depth, t->flags, fim,
                               pred);
+        }
+        if (have_pred) {
             for (int i = 0; i < h; i++)
                 for (int j = 0; j < w; j++) {
                     int yy = t->y + i, xx = t->x + j;
@@ -383,4 +412,5 @@ void ora_intra_frame(const av1g_frame_header* hdr, const av1g_quant_params* q, c
         if (t->flags & AV1G_INTRA_RESIDUAL) ora_recon_frame(hdr, q, &t->res, 1, coeffs, planes);
     }
     free(pred);
+    return rc;
 }

@@ -91,10 +91,16 @@ void ora_recon_frame(const av1g_frame_header* hdr, const av1g_quant_params* q, c
 void ora_intra_predict(const ora_plane* p, int sx, int sy, int tx, int mode, int angle_delta, int bd, int flags,
                        int filter_intra_mode, uint16_t* pred);
 
-/* Every intra TU of a frame in decode order: prediction, chroma from luma,
- * residual (transform_block_emit order, src/cdf.rs:32540-32910). */
-void ora_intra_frame(const av1g_frame_header* hdr, const av1g_quant_params* q, const av1g_intra_tu* tus, int n,
-                     const int32_t* coeffs, ora_plane planes[3]);
+/* Every intra TU of a frame in decode order: prediction (intra modes,
+ * palette from `maps`, intra block copy), chroma from luma, residual
+ * (transform_block_emit order, src/cdf.rs:32540-32910).  Returns 0, or
+ * 1 + the index of the first TU the reference rejects. */
+int ora_intra_frame(const av1g_frame_header* hdr, const av1g_quant_params* q, const av1g_intra_tu* tus, int n,
+                    const int32_t* coeffs, ora_plane planes[3], const uint8_t* maps, int64_t map_bytes);
+
+/* predict_intrabc_leaf_into_curr_frame (cdf.rs:19235) for one w x h region. */
+int ora_intrabc_predict(const ora_plane* p, int plane, int ssx, int ssy, int mi_cols, int mi_rows, int x, int y,
+                        int w, int h, int mv_row, int mv_col, int bd, uint16_t* pred);
 
 /* Every inter prediction call of a frame in list order (predict_inter,
  * src/inter_pred.rs:2100, with the CurrFrame copy of its

@@ -112,12 +112,15 @@ class IntraTu(C.Structure):
     _fields_ = [("x", C.c_uint16), ("y", C.c_uint16), ("plane", C.c_uint8), ("tx_size", C.c_uint8),
                 ("mode", C.c_uint8), ("flags", C.c_uint8), ("angle_delta", C.c_int8), ("cfl_alpha", C.c_int8),
                 ("filter_intra_mode", C.c_uint8), ("pad", C.c_uint8), ("max_luma_w", C.c_uint16),
-                ("max_luma_h", C.c_uint16), ("res", Tu)]
+                ("max_luma_h", C.c_uint16), ("res", Tu), ("mv", C.c_int16 * 2), ("palette_map", C.c_uint32),
+                ("palette_stride", C.c_uint16), ("palette_size", C.c_uint8), ("pad2", C.c_uint8),
+                ("palette_colors", C.c_uint16 * 8)]
 
 
 class IntraJob(C.Structure):
     _fields_ = [("hdr", C.POINTER(FrameHeader)), ("quant", C.POINTER(QuantParams)), ("tus", C.c_void_p),
-                ("num_tus", C.c_int32), ("sb_size", C.c_int32), ("coeffs", C.c_void_p), ("planes", Plane * 3)]
+                ("num_tus", C.c_int32), ("sb_size", C.c_int32), ("coeffs", C.c_void_p), ("planes", Plane * 3),
+                ("palette_maps", C.c_void_p), ("palette_map_bytes", C.c_int64)]
 
 
 class RefFrame(C.Structure):
@@ -158,6 +161,7 @@ INTER_SINGLE, INTER_COMPOUND, INTER_INTRA = 0, 1, 2
 
 INTRA_HAVE_ABOVE, INTRA_HAVE_LEFT, INTRA_HAVE_ABOVE_RIGHT, INTRA_HAVE_BELOW_LEFT = 1, 2, 4, 8
 INTRA_EDGE_FILTER, INTRA_FILTER_TYPE, INTRA_RESIDUAL, INTRA_CFL = 16, 32, 64, 128
+INTRA_MODE_PALETTE, INTRA_MODE_INTRABC, INTRA_MODE_NONE = 64, 65, 255
 
 _STRUCTS = {"av1g_film_grain": FilmGrain, "av1g_frame_header": FrameHeader, "av1g_lr_unit": LrUnit,
             "av1g_mi_grid": MiGrid, "av1g_plane": Plane, "av1g_frame_job": FrameJob,

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cstring>
 #include <string>
+#include <unordered_map>
 #include <unordered_set>
 #include <vector>
 
@@ -43,10 +44,12 @@ __constant__ AV1T_SM_WEIGHTS_TX_8X8_TYPE c_sm8 AV1T_SM_WEIGHTS_TX_8X8_DIMS = AV1
 __constant__ AV1T_SM_WEIGHTS_TX_16X16_TYPE c_sm16 AV1T_SM_WEIGHTS_TX_16X16_DIMS = AV1T_SM_WEIGHTS_TX_16X16_INIT;
 __constant__ AV1T_SM_WEIGHTS_TX_32X32_TYPE c_sm32 AV1T_SM_WEIGHTS_TX_32X32_DIMS = AV1T_SM_WEIGHTS_TX_32X32_INIT;
 __constant__ AV1T_SM_WEIGHTS_TX_64X64_TYPE c_sm64 AV1T_SM_WEIGHTS_TX_64X64_DIMS = AV1T_SM_WEIGHTS_TX_64X64_INIT;
+__constant__ AV1T_SUBPEL_FILTERS_TYPE c_subpel AV1T_SUBPEL_FILTERS_DIMS = AV1T_SUBPEL_FILTERS_INIT;
 
 struct IntraFrame {
     ReconFrame rf;
     int32_t ssx, ssy;
+    const uint8_t* maps;  // palette colour-index pool
 };
 
 struct IntraItem {
@@ -296,6 +299,50 @@ __device__ void intra_tu(Smem& s, const IntraFrame& F, const av1g_intra_tu& t) {
         }
         __syncthreads();
     }
+    if (t.mode == AV1G_INTRA_MODE_PALETTE || t.mode == AV1G_INTRA_MODE_INTRABC) {
+        const int maxv = (1 << bd) - 1;
+        if (t.mode == AV1G_INTRA_MODE_PALETTE) {
+            // predict_palette (cdf.rs:11907); indices checked on the host
+            const uint8_t* m = F.maps + t.palette_map;
+            for (int k = tid; k < W * H; k += kT) {
+                int i = k >> LW, j = k & (W - 1);
+                s.pred[k] = s.tu.palette_colors[m[i * t.palette_stride + j]];
+            }
+        } else {
+            // predict_intrabc_leaf_into_curr_frame (cdf.rs:19235): BILINEAR
+            // block_inter_prediction from the pre-filter plane at unit scale,
+            // start = (x << 10) + (((2 * mv) >> ss) << 6) + 32, clamped to the
+            // mi-padded plane (the reference's window clamp is the same set).
+            const int pss_x = t.plane ? F.ssx : 0, pss_y = t.plane ? F.ssy : 0;
+            const int stx = (sx << 10) + ((2 * t.mv[1]) >> pss_x) * 64 + 32;
+            const int sty = (sy << 10) + ((2 * t.mv[0]) >> pss_y) * 64 + 32;
+            const int r0 = bd == 12 ? 5 : 3, r1 = bd == 12 ? 9 : 11;
+            const int hph = (stx >> 6) & 15, vph = (sty >> 6) & 15;
+            for (int k = tid; k < W * H; k += kT) {
+                int i = k >> LW, j = k & (W - 1);
+                int xi = ((stx >> 10) + j) - 3, yi = ((sty >> 10) + i) - 3;
+                int acc = 0;
+                for (int tt = 0; tt < 8; tt++) {
+                    int vc = c_subpel[3][vph][tt];
+                    if (!vc) continue;
+                    int yy = min(max(yi + tt, 0), P.h - 1);
+                    int hsum = 0;
+                    for (int u = 0; u < 8; u++) {
+                        int hc = c_subpel[3][hph][u];
+                        if (hc) hsum += hc * ld_px(P, hbd, yy, min(max(xi + u, 0), P.w - 1));
+                    }
+                    acc += vc * ((hsum + ((1 << r0) >> 1)) >> r0);
+                }
+                s.pred[k] = (uint16_t)min(max((acc + (1 << (r1 - 1))) >> r1, 0), maxv);
+            }
+        }
+        __syncthreads();
+        for (int k = tid; k < W * H; k += kT) {
+            int i = k >> LW, j = k & (W - 1);
+            if (sy + i < P.h && sx + j < P.w) st_px(P, hbd, sy + i, sx + j, s.pred[k]);
+        }
+        __syncthreads();
+    }
     if ((t.flags & AV1G_INTRA_CFL) && t.plane > 0) {
         // predict_chroma_from_luma_into_curr_frame (cdf.rs:17256-17340); luma
         // outside the luma plane reads as 0
@@ -381,10 +428,13 @@ av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t st, std::s
     std::vector<IntraFrame> frames(n);
     std::vector<av1g_intra_tu> all;
     std::vector<IntraItem> items;
+    std::vector<uint8_t> maps;            // palette colour indices of all jobs
+    std::vector<size_t> map_base(n, 0);
     for (int i = 0; i < n; i++) {
         const av1g_intra_job& j = jobs[i];
-        if (!j.hdr || !j.quant || j.num_tus < 0 || (j.num_tus > 0 && !j.tus) || (j.sb_size != 64 && j.sb_size != 128)) {
-            err = "intra job " + std::to_string(i) + ": missing header/quantizer/TUs or superblock size not 64/128";
+        if (!j.hdr || !j.quant || j.num_tus < 0 || (j.num_tus > 0 && !j.tus) || (j.sb_size != 64 && j.sb_size != 128) ||
+            j.palette_map_bytes < 0 || (j.palette_map_bytes > 0 && !j.palette_maps)) {
+            err = "intra job " + std::to_string(i) + ": missing header/quantizer/TUs/maps or superblock size not 64/128";
             return AV1G_EINVAL;
         }
         const av1g_frame_header& h = *j.hdr;
@@ -410,8 +460,20 @@ av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t st, std::s
             }
             F.rf.planes[p] = PlaneDev{(uint8_t*)pl.data, pl.stride, pw, ph};
         }
-        std::unordered_set<long long> seen;
+        map_base[i] = maps.size();
+        if (j.palette_map_bytes > 0) maps.insert(maps.end(), j.palette_maps, j.palette_maps + j.palette_map_bytes);
+        // superblocks in decode order, and the intra block copy windows
+        struct Sb {
+            int sbx, sby, seq;
+        };
+        std::vector<Sb> sbs;
+        std::unordered_map<long long, int> sb_index;
+        struct Bc {
+            int sb, x0, y0, x1, y1;  // luma-sample window, inclusive
+        };
+        std::vector<Bc> bcs;
         int base = (int)all.size();
+        int first_item = (int)items.size();
         long long prev = -1;
         for (int k = 0; k < j.num_tus; k++) {
             const av1g_intra_tu& t = j.tus[k];
@@ -425,36 +487,104 @@ av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t st, std::s
                 err = "intra job " + std::to_string(i) + ": TU " + std::to_string(k) + " is malformed";
                 return AV1G_EINVAL;
             }
-            int lx = t.x << (t.plane ? h.subsampling_x : 0), ly = t.y << (t.plane ? h.subsampling_y : 0);
+            const int tw = kTxW[t.tx_size], th = kTxH[t.tx_size];
+            const int pss_x = t.plane ? h.subsampling_x : 0, pss_y = t.plane ? h.subsampling_y : 0;
+            if (t.mode == AV1G_INTRA_MODE_PALETTE) {
+                // predict_palette's checks (cdf.rs:11907-11960)
+                long long last = (long long)t.palette_map + (long long)(th - 1) * t.palette_stride + (tw - 1);
+                bool ok = t.palette_size >= 1 && t.palette_size <= 8 && t.palette_stride >= tw &&
+                          last < j.palette_map_bytes;
+                for (int r = 0; ok && r < th; r++)
+                    for (int c = 0; ok && c < tw; c++)
+                        ok = j.palette_maps[t.palette_map + (long long)r * t.palette_stride + c] < t.palette_size;
+                if (!ok) {
+                    err = "intra job " + std::to_string(i) + ": palette TU " + std::to_string(k) + " is malformed";
+                    return AV1G_EINVAL;
+                }
+            }
+            int lx = t.x << pss_x, ly = t.y << pss_y;
             long long sb = ((long long)(ly / j.sb_size) << 32) | (unsigned)(lx / j.sb_size);
             if (sb != prev) {
-                if (!seen.insert(sb).second) {
+                if (sb_index.count(sb)) {
                     err = "intra job " + std::to_string(i) + ": TUs of a superblock are not contiguous in decode order";
                     return AV1G_EINVAL;
                 }
                 int sbx = lx / j.sb_size, sby = ly / j.sb_size;
-                items.push_back(IntraItem{i, base + k, 0, sbx + 2 * sby});
+                sb_index[sb] = (int)sbs.size();
+                sbs.push_back(Sb{sbx, sby, (int)sbs.size()});
+                items.push_back(IntraItem{i, base + k, 0, 0});
                 prev = sb;
+            }
+            if (t.mode == AV1G_INTRA_MODE_INTRABC) {
+                if (std::abs((int)t.mv[0]) >= (1 << 14) || std::abs((int)t.mv[1]) >= (1 << 14)) {
+                    err = "intra job " + std::to_string(i) + ": intra block copy TU " + std::to_string(k) +
+                          " has a motion vector out of range";
+                    return AV1G_EINVAL;
+                }
+                // the window the BILINEAR filter reads, in luma samples
+                int pw = (h.mi_cols * 4) >> pss_x, ph = (h.mi_rows * 4) >> pss_y;
+                int stx = (t.x << 10) + ((2 * t.mv[1]) >> pss_x) * 64 + 32;
+                int sty = (t.y << 10) + ((2 * t.mv[0]) >> pss_y) * 64 + 32;
+                int x0 = std::min(std::max((stx >> 10) - 3, 0), pw - 1);
+                int x1 = std::min(std::max((stx >> 10) + tw - 1 + 4, 0), pw - 1);
+                int y0 = std::min(std::max((sty >> 10) - 3, 0), ph - 1);
+                int y1 = std::min(std::max((sty >> 10) + th - 1 + 4, 0), ph - 1);
+                bcs.push_back(Bc{sb_index[sb], x0 << pss_x, y0 << pss_y, ((x1 + 1) << pss_x) - 1,
+                                 ((y1 + 1) << pss_y) - 1});
             }
             items.back().count++;
             all.push_back(t);
+        }
+        // Superblock (c, r) gets level c + k r.  k = 2 covers the intra edge
+        // reads (above-right is one superblock up and right).  An intra block
+        // copy may read any earlier superblock, so every superblock its window
+        // touches must sit on the same side of it in level order as in decode
+        // order; steeper slopes follow the spec's intra-block-copy wavefront
+        // delay, and decode order itself (one superblock per level) always
+        // reproduces sequential decoding.
+        auto level_ok = [&](auto level) {
+            for (const Bc& b : bcs) {
+                const Sb& cur = sbs[b.sb];
+                for (int by = b.y0 / j.sb_size; by <= b.y1 / j.sb_size; by++)
+                    for (int bx = b.x0 / j.sb_size; bx <= b.x1 / j.sb_size; bx++) {
+                        auto it = sb_index.find(((long long)by << 32) | (unsigned)bx);
+                        if (it == sb_index.end() || it->second == b.sb) continue;
+                        const Sb& o = sbs[it->second];
+                        int lo = level(o), lc = level(cur);
+                        if (lo == lc || (o.seq < cur.seq) != (lo < lc)) return false;
+                    }
+            }
+            return true;
+        };
+        int slope = 0;
+        for (int k : {2, 3, 4, 5, 6, 8})
+            if (level_ok([k](const Sb& b) { return b.sbx + k * b.sby; })) {
+                slope = k;
+                break;
+            }
+        for (int q = first_item; q < (int)items.size(); q++) {
+            const Sb& b = sbs[q - first_item];
+            items[q].level = slope ? b.sbx + slope * b.sby : b.seq;
         }
     }
     if (items.empty()) return AV1G_OK;
     std::stable_sort(items.begin(), items.end(), [](const IntraItem& a, const IntraItem& b) { return a.level < b.level; });
     size_t off_tus = (sizeof(IntraFrame) * n + 255) & ~(size_t)255;
     size_t off_items = (off_tus + sizeof(av1g_intra_tu) * all.size() + 255) & ~(size_t)255;
-    size_t bytes = off_items + sizeof(IntraItem) * items.size();
-    std::vector<uint8_t> host(bytes);
-    memcpy(host.data(), frames.data(), sizeof(IntraFrame) * n);
-    memcpy(host.data() + off_tus, all.data(), sizeof(av1g_intra_tu) * all.size());
-    memcpy(host.data() + off_items, items.data(), sizeof(IntraItem) * items.size());
+    size_t off_maps = (off_items + sizeof(IntraItem) * items.size() + 255) & ~(size_t)255;
+    size_t bytes = off_maps + maps.size();
     uint8_t* dev = nullptr;
     cudaError_t e = cudaMallocAsync((void**)&dev, bytes, st);
     if (e != cudaSuccess) {
         err = std::string("cudaMallocAsync: ") + cudaGetErrorString(e);
         return AV1G_EDEVICE;
     }
+    for (int i = 0; i < n; i++) frames[i].maps = dev + off_maps + map_base[i];
+    std::vector<uint8_t> host(bytes);
+    memcpy(host.data(), frames.data(), sizeof(IntraFrame) * n);
+    memcpy(host.data() + off_tus, all.data(), sizeof(av1g_intra_tu) * all.size());
+    memcpy(host.data() + off_items, items.data(), sizeof(IntraItem) * items.size());
+    if (!maps.empty()) memcpy(host.data() + off_maps, maps.data(), maps.size());
     e = cudaMemcpyAsync(dev, host.data(), bytes, cudaMemcpyHostToDevice, st);
     const IntraFrame* df = (const IntraFrame*)dev;
     const av1g_intra_tu* dt = (const av1g_intra_tu*)(dev + off_tus);

@@ -214,6 +214,9 @@ class DeviceIntra(DeviceRecon):
         j.coeffs = self.coeffs.data_ptr()
         for p, pl in enumerate(self.planes):
             j.planes[p] = pl.cplane()
+        self._maps = np.ascontiguousarray(getattr(self.frame, "palette_maps", np.zeros(0, np.uint8)), np.uint8)
+        j.palette_maps = self._maps.ctypes.data if len(self._maps) else None
+        j.palette_map_bytes = len(self._maps)
         return j
 
 

@@ -423,7 +423,9 @@ def make_recon_frame(seed, width=352, height=288, bit_depth=8, ssx=1, ssy=1, mon
 INTRA_TU_DTYPE = np.dtype([("x", np.uint16), ("y", np.uint16), ("plane", np.uint8), ("tx_size", np.uint8),
                            ("mode", np.uint8), ("flags", np.uint8), ("angle_delta", np.int8), ("cfl_alpha", np.int8),
                            ("filter_intra_mode", np.uint8), ("pad", np.uint8), ("max_luma_w", np.uint16),
-                           ("max_luma_h", np.uint16), ("res", TU_DTYPE)])
+                           ("max_luma_h", np.uint16), ("res", TU_DTYPE), ("mv", np.int16, (2,)),
+                           ("palette_map", np.uint32), ("palette_stride", np.uint16), ("palette_size", np.uint8),
+                           ("pad2", np.uint8), ("palette_colors", np.uint16, (8,))])
 assert INTRA_TU_DTYPE.itemsize == C.sizeof(abi.IntraTu)
 
 
@@ -457,7 +459,13 @@ def _blocks(rng, x0, y0, n, pw, ph, out):
 
 
 def make_intra_frame(seed, width=176, height=144, bit_depth=8, ssx=1, ssy=1, mono=False, sb_size=64,
-                     edge_filter=True):
+                     edge_filter=True, palette=0.0, intrabc=0.0, intrabc_order="wavefront"):
+    """Intra TUs in decode order.  palette / intrabc: probability that a block
+    is a palette block / an intra-block-copy block.  intrabc_order picks where
+    copies read from: "wavefront" (the superblock row above, within reach of
+    the level-2 wavefront), "steep" (further right in the row above, which
+    needs a steeper wavefront) or "raster" (the row below, not yet decoded,
+    which only decode order reproduces)."""
     rng = np.random.default_rng(seed)
     base = make_recon_frame(seed + 1000, width, height, bit_depth, ssx, ssy, mono)
     f = IntraFrame()
@@ -467,6 +475,7 @@ def make_intra_frame(seed, width=176, height=144, bit_depth=8, ssx=1, ssy=1, mon
     f.planes = [rng.integers(0, maxv + 1, size=f.plane_dims(p)).astype(np.uint8 if bit_depth == 8 else np.uint16)
                 for p in range(h.num_planes)]
     tus, coeffs, off = [], [], 0
+    maps, map_off = [], 0
     decoded = [np.zeros(((f.plane_dims(p)[0] + 3) // 4, (f.plane_dims(p)[1] + 3) // 4), bool)
                for p in range(h.num_planes)]
     lossless_seg = [s for s in range(8) if f.quant.lossless[s]]
@@ -494,6 +503,34 @@ def make_intra_frame(seed, width=176, height=144, bit_depth=8, ssx=1, ssy=1, mon
                         mode, ad, fim = 0, 0, int(rng.integers(0, 5))
                     if p > 0 and rng.random() < 0.25:
                         mode, ad, cfl = 0, 0, True
+                    kind = rng.random()
+                    pal, bc_mv = None, None
+                    if kind < palette:
+                        n_col = int(rng.integers(1, 9))
+                        colors = [int(v) for v in rng.integers(0, maxv + 1, size=n_col)] + [0] * (8 - n_col)
+                        idx = rng.integers(0, n_col, size=(bh, bw)).astype(np.uint8)
+                        pal = (map_off, bw, n_col, colors)
+                        maps.append(idx.ravel())
+                        map_off += idx.size
+                        mode, ad, fim, cfl = abi.INTRA_MODE_PALETTE, 0, 255, False
+                    elif kind < palette + intrabc:
+                        sbp_x, sbp_y = sb_size >> sx_, sb_size >> sy_
+                        spx, spy = sbx >> sx_, sby >> sy_
+                        src = None
+                        if intrabc_order in ("wavefront", "steep") and spy >= sbp_y and spy - bh - 5 >= 0:
+                            reach = 2 if intrabc_order == "wavefront" else 5
+                            xs_max = min(spx + reach * sbp_x - bw - 6, pw - bw)
+                            xs_min = spx + 2 * sbp_x if intrabc_order == "steep" else 0
+                            if xs_max >= max(xs_min, 0):
+                                src = (int(rng.integers(max(xs_min, 0), xs_max + 1)),
+                                       int(rng.integers(0, spy - bh - 5 + 1)))
+                        elif intrabc_order == "raster" and spy + sbp_y + bh + 5 <= ph and spx >= 3 * sbp_x:
+                            src = (int(rng.integers(0, spx - 2 * sbp_x)),
+                                   int(rng.integers(spy + sbp_y, ph - bh - 5 + 1)))
+                        if src is not None:
+                            odd = int(rng.integers(0, 2))
+                            bc_mv = (((src[1] - by) << sy_) * 8, (((src[0] - bx) << sx_) + odd) * 8)
+                            mode, ad, fim, cfl = abi.INTRA_MODE_INTRABC, 0, 255, False
                     seg = int(rng.integers(0, 8))
                     if seg in lossless_seg and tx != 0:
                         seg = 0 if 0 not in lossless_seg else 1
@@ -527,11 +564,15 @@ def make_intra_frame(seed, width=176, height=144, bit_depth=8, ssx=1, ssy=1, mon
                                 off += len(lv)
                             mlw = min((bx + bw) << sx_, 65535)
                             mlh = min((by + bh) << sy_, 65535)
+                            pm, ps, pn, pc = (0, 0, 0, [0] * 8) if pal is None else pal
+                            if pal is not None:
+                                pm += (ty - by) * bw + (tx_ - bx)
                             tus.append((tx_, ty, p, tx, mode, flags, ad, int(rng.integers(-16, 17)) if cfl else 0,
-                                        fim, 0, mlw, mlh, res))
+                                        fim, 0, mlw, mlh, res, bc_mv if bc_mv else (0, 0), pm, ps, pn, 0, pc))
                             decoded[p][cy:cy + (th + 3) // 4, cx:cx + (tw + 3) // 4] = True
     f.tus = np.array(tus, dtype=INTRA_TU_DTYPE)
     f.coeffs = np.concatenate(coeffs).astype(np.int32) if coeffs else np.zeros(1, np.int32)
+    f.palette_maps = np.concatenate(maps).astype(np.uint8) if maps else np.zeros(0, np.uint8)
     return f
 
 

@@ -1,9 +1,12 @@
 """Intra prediction + reconstruction on the GPU (superblock wavefront) against the oracle.
 
 Every mode (DC, V, H, the six directional modes with angle deltas, edge filter
-and upsampling, SMOOTH/_V/_H, PAETH), recursive filter intra, chroma from luma
-and residuals, with availability flags derived from decode order, at 8/10/12
-bits, 4:2:0, 4:4:4 and monochrome, 64x64 and 128x128 superblocks.
+and upsampling, SMOOTH/_V/_H, PAETH), recursive filter intra, chroma from luma,
+palette prediction, intra block copy (reading within the level-2 wavefront,
+further right so that a steeper wavefront is needed, and from not yet decoded
+superblocks so that only decode order reproduces the reference) and residuals,
+with availability flags derived from decode order, at 8/10/12 bits, 4:2:0,
+4:4:4 and monochrome, 64x64 and 128x128 superblocks.
 """
 import numpy as np
 import pytest
@@ -23,6 +26,11 @@ CASES = [
     dict(seed=85, width=96, height=96, mono=True),
     dict(seed=86, width=352, height=288, sb_size=128),
     dict(seed=87, width=640, height=360),
+    dict(seed=90, width=176, height=144, palette=0.3),
+    dict(seed=91, width=352, height=288, intrabc=0.4),
+    dict(seed=92, width=640, height=360, intrabc=0.4, intrabc_order="steep"),
+    dict(seed=93, width=1280, height=128, intrabc=0.5, intrabc_order="raster"),
+    dict(seed=94, width=352, height=288, bit_depth=10, palette=0.2, intrabc=0.2, ssx=0, ssy=0),
 ]
 
 
@@ -61,6 +69,19 @@ def test_intra_rejects_split_superblock():
     # TUs are no longer contiguous in decode order
     k = int(np.argmax((tus["plane"] == 0) & (tus["x"] >= 64)))
     f.tus = np.concatenate([tus[k:k + 1], tus[:k], tus[k + 1:]])
+    d = postfilter.DeviceIntra(f)
+    with pytest.raises(abi.Av1gError):
+        postfilter.run_intra([d])
+
+
+def test_intra_rejects_palette_index_out_of_range():
+    abi.load()
+    f = synth.make_intra_frame(seed=95, width=128, height=64, palette=1.0)
+    k = int(np.argmax(f.tus["mode"] == abi.INTRA_MODE_PALETTE))
+    t = f.tus[k]
+    f.palette_maps = f.palette_maps.copy()
+    f.palette_maps[int(t["palette_map"])] = int(t["palette_size"])
+    assert oracle.intra_rc(f)[1] == k + 1
     d = postfilter.DeviceIntra(f)
     with pytest.raises(abi.Av1gError):
         postfilter.run_intra([d])

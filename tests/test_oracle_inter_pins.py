@@ -182,3 +182,35 @@ def test_caller_bugs_are_rejected():
     for c in bad:
         f = synth.custom_inter_frame(16, 16, ref, [c])
         assert oracle.inter(f)[1] == 1, c
+
+
+def test_intrabc_pieces_equal_the_whole_block():
+    # predict_intrabc_leaf_into_curr_frame predicts the whole block at unit
+    # scale; transform-sized pieces at their own origins give the same samples
+    rng = np.random.default_rng(0)
+    pl = rng.integers(0, 1024, size=(64, 128))
+    for mv in [(-56, -72), (-64, 8), (-120, -4)]:
+        a = oracle.intrabc_predict(pl, 1, 1, 1, 64, 32, 40, 20, 16, 16, *mv, 10)
+        b = np.block([[oracle.intrabc_predict(pl, 1, 1, 1, 64, 32, 40 + dx, 20 + dy, 8, 8, *mv, 10)
+                       for dx in (0, 8)] for dy in (0, 8)])
+        assert np.array_equal(a, b)
+
+
+def test_intrabc_integer_mv_copies_and_rejects_out_of_range():
+    rng = np.random.default_rng(1)
+    pl = rng.integers(0, 256, size=(64, 64))
+    got = oracle.intrabc_predict(pl, 0, 1, 1, 16, 16, 32, 32, 8, 8, -8 * 16, -8 * 24, 8)
+    assert np.array_equal(got, pl[16:24, 8:16])
+    assert oracle.intrabc_predict(pl, 0, 1, 1, 16, 16, 32, 32, 8, 8, 1 << 14, 0, 8) is None
+
+
+def test_palette_prediction_and_index_check():
+    # predict_palette: CurrFrame = palette[map]; an index >= PaletteSize is rejected
+    f = synth.make_intra_frame(seed=5, width=64, height=64, palette=1.0, mono=True)
+    planes, rc = oracle.intra_rc(f)
+    assert rc == 0
+    t = f.tus[0]
+    assert t["mode"] == abi.INTRA_MODE_PALETTE
+    f.palette_maps = f.palette_maps.copy()
+    f.palette_maps[int(t["palette_map"])] = 9
+    assert oracle.intra_rc(f)[1] == 1
