@@ -455,6 +455,20 @@ typedef struct av1g_inter_job {
     av1g_plane planes[3];                   /* CurrFrame, device, written */
 } av1g_inter_job;
 
+/* WarpSampleCand (src/inter_pred.rs:4030): one §7.10.4 warp sample. */
+typedef struct av1g_warp_sample {
+    int32_t sy, sx, dy, dx;
+} av1g_warp_sample;
+
+/* The §7.11.3.8 least-squares local warp fit of a WARPED_CAUSAL block
+ * (warp_estimation, src/inter_pred.rs:4083, called by the tile walker at
+ * cdf.rs:30929): at most 8 samples are used.  Writes LocalWarpParams and
+ * LocalValid.  A host function (eight samples per block); its output feeds
+ * av1g_warp_ctx.local_warp_params / local_valid. */
+av1g_status av1g_warp_estimation(const av1g_warp_sample* cands, int32_t n, int32_t mi_row, int32_t mi_col,
+                                 int32_t block_w4, int32_t block_h4, int16_t mv_row, int16_t mv_col,
+                                 int32_t params[6], uint8_t* valid);
+
 /* §7.11.3 inter prediction for every listed call of `n` frames: motion
  * vector scaling (§7.11.3.3), 8-tap sub-sample interpolation with scaled
  * references (§7.11.3.4), local / global warp (§7.11.3.5-6), OBMC

@@ -300,3 +300,13 @@ def wedge_mask(mi_size, wedge_index, wedge_sign):
     m = np.zeros((h, w), np.uint8)
     rc = lib.ora_wedge_mask(mi_size, wedge_index, wedge_sign, m.ctypes.data_as(C.c_void_p))
     return None if rc else m
+
+
+def warp_estimation(cands, mi_row, mi_col, bw4, bh4, mv_row, mv_col):
+    """cands: sequence of (sy, sx, dy, dx).  Returns (valid, params)."""
+    lib = load()
+    arr = np.ascontiguousarray(np.array(cands, np.int32).reshape(-1, 4))
+    params = (C.c_int32 * 6)()
+    v = lib.ora_warp_estimation(arr.ctypes.data_as(C.c_void_p), len(arr), mi_row, mi_col, bw4, bh4, mv_row, mv_col,
+                                params)
+    return bool(v), list(params)

@@ -638,3 +638,66 @@ int ora_intrabc_predict(const ora_plane* p, int plane, int ssx, int ssy, int mi_
     free(win.s);
     return rc;
 }
+
+/* warp_estimation, inter_pred.rs:4083-4226, with the reference's release-
+ * build integer semantics (wrapping +, -, *; saturating where it says so). */
+static int64_t ls_product(int32_t a, int32_t b) { return (((int64_t)a * b) >> 2) + a + b; }
+static int64_t wadd64(int64_t a, int64_t b) { return (int64_t)((uint64_t)a + (uint64_t)b); }
+static int64_t wsub64(int64_t a, int64_t b) { return (int64_t)((uint64_t)a - (uint64_t)b); }
+static int64_t wmul64(int64_t a, int64_t b) { return (int64_t)((uint64_t)a * (uint64_t)b); }
+static int32_t wsub32(int32_t a, int32_t b) { return (int32_t)((uint32_t)a - (uint32_t)b); }
+static int32_t wabs32(int32_t v) { return v == INT32_MIN ? v : (v < 0 ? -v : v); }
+
+int ora_warp_estimation(const av1g_warp_sample* cand, int n, int mi_row, int mi_col, int bw4, int bh4, int mv_row,
+                        int mv_col, int32_t params[6]) {
+    if (n > 8) n = 8;
+    int32_t mid_y = (int32_t)((uint32_t)mi_row * 4u + (uint32_t)bh4 * 2u - 1u);
+    int32_t mid_x = (int32_t)((uint32_t)mi_col * 4u + (uint32_t)bw4 * 2u - 1u);
+    int32_t suy = (int32_t)((uint32_t)mid_y * 8u), sux = (int32_t)((uint32_t)mid_x * 8u);
+    int32_t duy = (int32_t)((uint32_t)suy + (uint32_t)(int32_t)(int16_t)mv_row);
+    int32_t dux = (int32_t)((uint32_t)sux + (uint32_t)(int32_t)(int16_t)mv_col);
+    int64_t A00 = 0, A01 = 0, A11 = 0, Bx0 = 0, Bx1 = 0, By0 = 0, By1 = 0;
+    for (int i = 0; i < n; i++) {
+        int32_t sy = wsub32(cand[i].sy, suy), sx = wsub32(cand[i].sx, sux);
+        int32_t dy = wsub32(cand[i].dy, duy), dx = wsub32(cand[i].dx, dux);
+        if (wabs32(wsub32(sx, dx)) < 256 && wabs32(wsub32(sy, dy)) < 256) {
+            A00 = wadd64(A00, ls_product(sx, sx) + 8);
+            A01 = wadd64(A01, ls_product(sx, sy) + 4);
+            A11 = wadd64(A11, ls_product(sy, sy) + 8);
+            Bx0 = wadd64(Bx0, ls_product(sx, dx) + 8);
+            Bx1 = wadd64(Bx1, ls_product(sy, dx) + 4);
+            By0 = wadd64(By0, ls_product(sx, dy) + 4);
+            By1 = wadd64(By1, ls_product(sy, dy) + 8);
+        }
+    }
+    int64_t det = wsub64(sat_mul(A00, A11), sat_mul(A01, A01));
+    memset(params, 0, 6 * sizeof(int32_t));
+    if (det == 0) return 0;
+    uint64_t ad = det < 0 ? 0ull - (uint64_t)det : (uint64_t)det;
+    int nb = 63 - __builtin_clzll(ad);
+    int64_t e = (int64_t)(ad - (1ull << nb));
+    int64_t f = nb > 8 ? (e + ((int64_t)1 << (nb - 8 - 1))) >> (nb - 8) : e << (8 - nb);
+    if (f > 256) f = 256;
+    int64_t fac = DIV_LUT[f];
+    if (det < 0) fac = -fac;
+    int shift = nb + 14 - 16;
+    if (shift < 0) {
+        fac = wmul64(fac, (int64_t)1 << -shift);
+        shift = 0;
+    }
+    int32_t one = 1 << 16, ndc = 1 << 13;
+#define DIAG(v) clip3(one - ndc + 1, one + ndc - 1, (int32_t)rnd2s(sat_mul((v), fac), shift))
+#define NONDIAG(v) clip3(-ndc + 1, ndc - 1, (int32_t)rnd2s(sat_mul((v), fac), shift))
+    params[2] = DIAG(wsub64(wmul64(A11, Bx0), wmul64(A01, Bx1)));
+    params[3] = NONDIAG(wadd64(wmul64(wsub64(0, A01), Bx0), wmul64(A00, Bx1)));
+    params[4] = NONDIAG(wsub64(wmul64(A11, By0), wmul64(A01, By1)));
+    params[5] = DIAG(wadd64(wmul64(wsub64(0, A01), By0), wmul64(A00, By1)));
+#undef DIAG
+#undef NONDIAG
+    int64_t vx = (int64_t)(int16_t)mv_col * (1 << 13) - ((int64_t)mid_x * (params[2] - one) + (int64_t)mid_y * params[3]);
+    int64_t vy = (int64_t)(int16_t)mv_row * (1 << 13) - ((int64_t)mid_x * params[4] + (int64_t)mid_y * (params[5] - one));
+    int64_t tc = 1 << 23;
+    params[0] = (int32_t)(vx < -tc ? -tc : (vx > tc - 1 ? tc - 1 : vx));
+    params[1] = (int32_t)(vy < -tc ? -tc : (vy > tc - 1 ? tc - 1 : vy));
+    return 1;
+}

@@ -116,6 +116,9 @@ int ora_mv_scaling(int plane, int ssx, int ssy, int fw, int fh, int ruw, int rh,
                    int mv_col, int32_t out[4]);
 /* setup_shear (inter_pred.rs:3982): out = alpha, beta, gamma, delta, warpValid; -1 for None. */
 int ora_setup_shear(const int32_t p[6], int32_t out[5]);
+/* warp_estimation (inter_pred.rs:4083): returns LocalValid, fills params. */
+int ora_warp_estimation(const av1g_warp_sample* cand, int n, int mi_row, int mi_col, int bw4, int bh4, int mv_row,
+                        int mv_col, int32_t params[6]);
 /* wedge_mask (inter_pred.rs:2844) into a block_width x block_height mask. */
 int ora_wedge_mask(int mi_size, int idx, int sign, uint8_t* mask);
 

@@ -151,6 +151,10 @@ class InterPred(C.Structure):
                 ("mi_height_log2", C.c_uint8), ("pad", C.c_uint8), ("mi_row", C.c_uint16), ("mi_col", C.c_uint16)]
 
 
+class WarpSample(C.Structure):
+    _fields_ = [("sy", C.c_int32), ("sx", C.c_int32), ("dy", C.c_int32), ("dx", C.c_int32)]
+
+
 class InterJob(C.Structure):
     _fields_ = [("hdr", C.POINTER(FrameHeader)), ("refs", C.POINTER(RefFrame)), ("preds", C.c_void_p),
                 ("num_preds", C.c_int32), ("neighbours", C.c_void_p), ("num_neighbours", C.c_int32),
@@ -168,7 +172,7 @@ _STRUCTS = {"av1g_film_grain": FilmGrain, "av1g_frame_header": FrameHeader, "av1
             "av1g_quant_params": QuantParams, "av1g_tu": Tu, "av1g_recon_job": ReconJob,
             "av1g_intra_tu": IntraTu, "av1g_intra_job": IntraJob, "av1g_ref_frame": RefFrame,
             "av1g_warp_ctx": WarpCtx, "av1g_obmc_neighbour": ObmcNeighbour, "av1g_inter_pred": InterPred,
-            "av1g_inter_job": InterJob}
+            "av1g_inter_job": InterJob, "av1g_warp_sample": WarpSample}
 
 # exported entry points and their ctypes signatures
 _SIGS = {
@@ -187,6 +191,8 @@ _SIGS = {
     "av1g_run_recon": (C.c_int, [C.POINTER(ReconJob), C.c_int32, C.c_void_p]),
     "av1g_run_intra": (C.c_int, [C.POINTER(IntraJob), C.c_int32, C.c_void_p]),
     "av1g_run_inter": (C.c_int, [C.POINTER(InterJob), C.c_int32, C.c_void_p]),
+    "av1g_warp_estimation": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                       C.c_int16, C.c_int16, C.POINTER(C.c_int32), C.POINTER(C.c_uint8)]),
 }
 
 NOALLOC_MAX_FRAMES = 16
@@ -231,3 +237,14 @@ def check(status):
 
 def exported_symbols():
     return list(_SIGS)
+
+
+def warp_estimation(cands, mi_row, mi_col, bw4, bh4, mv_row, mv_col):
+    """av1g_warp_estimation: cands = sequence of (sy, sx, dy, dx); returns (valid, params)."""
+    lib = load()
+    arr = (WarpSample * max(len(cands), 1))(*[WarpSample(*c) for c in cands])
+    params = (C.c_int32 * 6)()
+    valid = C.c_uint8()
+    check(lib.av1g_warp_estimation(C.cast(arr, C.c_void_p), len(cands), mi_row, mi_col, bw4, bh4, mv_row, mv_col,
+                                   params, C.byref(valid)))
+    return bool(valid.value), list(params)

@@ -330,6 +330,7 @@ int32_t av1g_struct_size(const char* name) {
     if (!strcmp(name, "av1g_obmc_neighbour")) return (int32_t)sizeof(av1g_obmc_neighbour);
     if (!strcmp(name, "av1g_inter_pred")) return (int32_t)sizeof(av1g_inter_pred);
     if (!strcmp(name, "av1g_inter_job")) return (int32_t)sizeof(av1g_inter_job);
+    if (!strcmp(name, "av1g_warp_sample")) return (int32_t)sizeof(av1g_warp_sample);
     return -1;
 }
 
