@@ -240,13 +240,14 @@ typedef struct av1g_tu {
     uint32_t coeff_offset;
 } av1g_tu;
 
-/* A frame's residual work: tus and coeffs are device arrays; planes hold the
+/* A frame's residual work: tus is a host array (the library buckets the TUs
+ * by size and type and uploads them), coeffs a device array; planes hold the
  * prediction on entry (CurrFrame at the padded mi extent) and the
  * reconstruction on return. */
 typedef struct av1g_recon_job {
     const av1g_frame_header* hdr;    /* host: bit depth, subsampling, mi dims */
     const av1g_quant_params* quant;  /* host */
-    const av1g_tu* tus;              /* device */
+    const av1g_tu* tus;              /* host */
     int32_t num_tus;
     const int32_t* coeffs;           /* device */
     av1g_plane planes[3];            /* device, updated in place */
@@ -478,6 +479,121 @@ av1g_status av1g_warp_estimation(const av1g_warp_sample* cands, int32_t n, int32
  * _warp, _obmc, _compound and _interintra (inter_pred.rs:4881-6010).
  * One launch for all frames, plus one for DIFFWTD chroma calls. */
 av1g_status av1g_run_inter(const av1g_inter_job* jobs, int32_t n, void* stream);
+
+/* ---------------------------------------------------------------------
+ * Serving engine: streams, device-resident reference slots, tickets
+ * ------------------------------------------------------------------- */
+
+typedef struct av1g_engine av1g_engine;
+typedef struct av1g_stream av1g_stream;
+
+typedef struct av1g_config {
+    int32_t device;              /* CUDA device ordinal                           */
+    int32_t max_batch;           /* frames (one per stream) per step; 0 = 64      */
+    int64_t hbm_budget_bytes;    /* admission budget; 0 = 80% of free memory      */
+    int32_t max_inflight_steps;  /* steps enqueued ahead of completion; 0 = 3     */
+    int32_t pad;
+} av1g_config;
+
+/* What a stream's sequence header fixes: the largest upscaled frame and the
+ * sample format.  The engine reserves eight reference slots of that size in
+ * its budget when the stream opens. */
+typedef struct av1g_seq_info {
+    int32_t max_width;
+    int32_t max_height;
+    uint8_t bit_depth;
+    uint8_t subsampling_x;
+    uint8_t subsampling_y;
+    uint8_t num_planes;
+    int32_t sb_size;             /* 64 or 128 */
+} av1g_seq_info;
+
+/* One frame as the tile walker hands it over (all pointers HOST memory; the
+ * engine copies what it needs before av1g_submit_frame returns).  Decoding
+ * runs: inter predictions (references: the stream's slots named by
+ * ref_frame_idx), inter residuals, the intra wavefront, then the §7.4
+ * post-filter chain (decode_frame_spec_tiles, frame_driver.rs:790-1116),
+ * the §7.20 slot refresh with the pre-grain frame (reference_frame_update,
+ * frame_driver.rs:1409) and, if shown, the output.  show_existing_frame
+ * outputs slot frame_to_show_map_idx with its stored grain parameters
+ * (output_existing_frame, frame_driver.rs:1495) and refreshes the slots in
+ * refresh_frame_flags with it. */
+typedef struct av1g_frame_desc {
+    const av1g_frame_header* hdr;
+    const av1g_quant_params* quant;
+    av1g_mi_grid grid;
+    const int8_t* cdef_idx;
+    const av1g_lr_unit* lr_units[3];
+    const av1g_inter_pred* inter_preds;
+    int32_t num_inter_preds;
+    const av1g_obmc_neighbour* neighbours;
+    int32_t num_neighbours;
+    const av1g_warp_ctx* warps;
+    int32_t num_warps;
+    const av1g_tu* inter_tus;           /* residuals of inter blocks            */
+    int32_t num_inter_tus;
+    const av1g_intra_tu* intra_tus;     /* decode order                          */
+    int32_t num_intra_tus;
+    const uint8_t* palette_maps;
+    int64_t palette_map_bytes;
+    const int32_t* coeffs;              /* pool indexed by coeff_offset          */
+    int64_t num_coeffs;
+    uint8_t ref_frame_idx[7];           /* slot of LAST_FRAME..ALTREF_FRAME      */
+    uint8_t refresh_frame_flags;
+    uint8_t show_frame;
+    uint8_t show_existing_frame;
+    uint8_t frame_to_show_map_idx;
+    uint8_t pad;
+} av1g_frame_desc;
+
+/* A finished frame: cropped planes with tight strides (width x 1 or 2 bytes,
+ * SpecFrame layout, frame_driver.rs:64-77) in engine-owned pinned host memory,
+ * valid until av1g_release_output.  latency_ms: submit to completion. */
+typedef struct av1g_frame_out {
+    av1g_plane planes[3];
+    int32_t num_planes;
+    int32_t bit_depth;
+    int32_t shown;
+    int32_t pad;
+    double latency_ms;
+} av1g_frame_out;
+
+typedef struct av1g_engine_stats {
+    int64_t frames_done;
+    int64_t steps_done;
+    int64_t bytes_reserved;     /* reference slots of open streams             */
+    int64_t bytes_in_flight;    /* work buffers of enqueued steps              */
+    int64_t budget;
+    int32_t streams_open;
+    int32_t pad;
+} av1g_engine_stats;
+
+av1g_status av1g_engine_create(const av1g_config* cfg, av1g_engine** out);
+/* Waits (bounded) for enqueued work, then frees everything. */
+void av1g_engine_destroy(av1g_engine* e);
+av1g_status av1g_engine_get_stats(av1g_engine* e, av1g_engine_stats* out);
+
+/* AV1G_ENOMEM_BUDGET when the stream's reference slots do not fit the
+ * remaining budget (retry after another stream closes). */
+av1g_status av1g_stream_open(av1g_engine* e, const av1g_seq_info* seq, av1g_stream** out);
+/* Waits for the stream's frames, then releases its slots and outputs. */
+av1g_status av1g_stream_close(av1g_stream* s);
+/* reset_references (frame_driver.rs:1401), ordered after frames already
+ * submitted on the stream. */
+av1g_status av1g_stream_reset_refs(av1g_stream* s);
+
+/* Queues a frame; *ticket identifies it.  Frames of one stream run in
+ * submission order; frames of different streams are batched into shared
+ * launches (one per stage per step). */
+av1g_status av1g_submit_frame(av1g_stream* s, const av1g_frame_desc* d, uint64_t* ticket);
+/* Waits up to timeout_ns (0: no wait) for the ticket.  Returns AV1G_OK with
+ * *result = the frame's status once finished, AV1G_TIMEOUT (timeout > 0) or
+ * AV1G_ENOTREADY (timeout 0) otherwise. */
+av1g_status av1g_poll(av1g_engine* e, uint64_t ticket, int64_t timeout_ns, av1g_status* result);
+/* The finished frame of a ticket (its status is returned). */
+av1g_status av1g_fetch_output(av1g_stream* s, uint64_t ticket, av1g_frame_out* out);
+/* Frees a finished ticket and its output buffer. */
+av1g_status av1g_release_output(av1g_stream* s, uint64_t ticket);
 
 /* Launch modes for av1g_run_postfilter. */
 #define AV1G_MODE_BATCHED 0     /* one launch per stage across all jobs    */

@@ -310,3 +310,65 @@ def warp_estimation(cands, mi_row, mi_col, bw4, bh4, mv_row, mv_col):
     v = lib.ora_warp_estimation(arr.ctypes.data_as(C.c_void_p), len(arr), mi_row, mi_col, bw4, bh4, mv_row, mv_col,
                                 params)
     return bool(v), list(params)
+
+
+
+class _Obj:
+    pass
+
+
+def decode_stream(frames):
+    """Sequential CPU decode of synth.StreamFrame objects: inter calls, inter
+    residuals, intra TUs, the §7.4 chain, slot refresh with the pre-grain
+    frame, output (show_existing_frame: the slot with its grain).  Returns the
+    shown frames' int32 planes in order (None for frames not shown)."""
+    import copy
+    from oxideav_av1_b200 import synth
+    slots = [None] * 8
+    outs = []
+    for fr in frames:
+        if fr.show_existing:
+            sl = slots[fr.show_idx]
+            planes = [p.copy() for p in sl["planes"]]
+            if sl["hdr"].film_grain.apply_grain:
+                o = _Obj()
+                o.hdr = sl["hdr"]
+                film_grain(o, planes)
+            for i in range(8):
+                if (fr.refresh >> i) & 1:
+                    slots[i] = sl
+            outs.append(planes)
+            continue
+        h = fr.hdr
+        ph = lambda p: ((h.mi_rows * 4) >> (h.subsampling_y if p else 0), (h.mi_cols * 4) >> (h.subsampling_x if p else 0))
+        planes = [np.zeros(ph(p), np.int32) for p in range(h.num_planes)]
+        if fr.preds is not None and len(fr.preds):
+            o = _Obj()
+            o.hdr, o.preds, o.neighbours, o.warps, o.planes = h, fr.preds, fr.neighbours, fr.warps, planes
+            o.refs = []
+            for r in range(7):
+                sl = slots[fr.ref_frame_idx[r]]
+                pls = list(sl["planes"]) + [np.zeros((1, 1), np.int32)] * (3 - len(sl["planes"]))
+                o.refs.append({"planes": pls, "upscaled_width": sl["uw"], "frame_height": sl["fh"]})
+            planes, rc = inter(o)
+            if rc:
+                raise RuntimeError(f"oracle rejected inter call {rc - 1}")
+        if fr.inter_tus is not None and len(fr.inter_tus):
+            o = _Obj()
+            o.hdr, o.quant, o.tus, o.coeffs, o.planes = h, fr.quant, fr.inter_tus, fr.coeffs, planes
+            planes = recon(o)
+        if fr.intra_tus is not None and len(fr.intra_tus):
+            o = _Obj()
+            o.hdr, o.quant, o.tus, o.coeffs, o.planes = h, fr.quant, fr.intra_tus, fr.coeffs, planes
+            o.palette_maps = fr.palette_maps if fr.palette_maps is not None else np.zeros(0, np.uint8)
+            planes = intra(o)
+        sf = synth.SyntheticFrame()
+        sf.hdr, sf.grid, sf.cdef_idx, sf.lr_units, sf.recon = h, fr.grid, fr.cdef_idx, fr.lr_units, planes
+        ref, out = postfilter_frame(sf)
+        if fr.refresh:
+            sl = {"planes": ref, "uw": h.upscaled_width, "fh": h.frame_height, "hdr": copy.copy(h)}
+            for i in range(8):
+                if (fr.refresh >> i) & 1:
+                    slots[i] = sl
+        outs.append(out if fr.show else None)
+    return outs

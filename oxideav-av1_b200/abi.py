@@ -163,6 +163,40 @@ class InterJob(C.Structure):
 
 INTER_SINGLE, INTER_COMPOUND, INTER_INTRA = 0, 1, 2
 
+
+class Config(C.Structure):
+    _fields_ = [("device", C.c_int32), ("max_batch", C.c_int32), ("hbm_budget_bytes", C.c_int64),
+                ("max_inflight_steps", C.c_int32), ("pad", C.c_int32)]
+
+
+class SeqInfo(C.Structure):
+    _fields_ = [("max_width", C.c_int32), ("max_height", C.c_int32), ("bit_depth", C.c_uint8),
+                ("subsampling_x", C.c_uint8), ("subsampling_y", C.c_uint8), ("num_planes", C.c_uint8),
+                ("sb_size", C.c_int32)]
+
+
+class FrameDesc(C.Structure):
+    _fields_ = [("hdr", C.POINTER(FrameHeader)), ("quant", C.POINTER(QuantParams)), ("grid", MiGrid),
+                ("cdef_idx", C.c_void_p), ("lr_units", C.c_void_p * 3), ("inter_preds", C.c_void_p),
+                ("num_inter_preds", C.c_int32), ("neighbours", C.c_void_p), ("num_neighbours", C.c_int32),
+                ("warps", C.c_void_p), ("num_warps", C.c_int32), ("inter_tus", C.c_void_p),
+                ("num_inter_tus", C.c_int32), ("intra_tus", C.c_void_p), ("num_intra_tus", C.c_int32),
+                ("palette_maps", C.c_void_p), ("palette_map_bytes", C.c_int64), ("coeffs", C.c_void_p),
+                ("num_coeffs", C.c_int64), ("ref_frame_idx", C.c_uint8 * 7), ("refresh_frame_flags", C.c_uint8),
+                ("show_frame", C.c_uint8), ("show_existing_frame", C.c_uint8), ("frame_to_show_map_idx", C.c_uint8),
+                ("pad", C.c_uint8)]
+
+
+class FrameOut(C.Structure):
+    _fields_ = [("planes", Plane * 3), ("num_planes", C.c_int32), ("bit_depth", C.c_int32), ("shown", C.c_int32),
+                ("pad", C.c_int32), ("latency_ms", C.c_double)]
+
+
+class EngineStats(C.Structure):
+    _fields_ = [("frames_done", C.c_int64), ("steps_done", C.c_int64), ("bytes_reserved", C.c_int64),
+                ("bytes_in_flight", C.c_int64), ("budget", C.c_int64), ("streams_open", C.c_int32),
+                ("pad", C.c_int32)]
+
 INTRA_HAVE_ABOVE, INTRA_HAVE_LEFT, INTRA_HAVE_ABOVE_RIGHT, INTRA_HAVE_BELOW_LEFT = 1, 2, 4, 8
 INTRA_EDGE_FILTER, INTRA_FILTER_TYPE, INTRA_RESIDUAL, INTRA_CFL = 16, 32, 64, 128
 INTRA_MODE_PALETTE, INTRA_MODE_INTRABC, INTRA_MODE_NONE = 64, 65, 255
@@ -172,7 +206,9 @@ _STRUCTS = {"av1g_film_grain": FilmGrain, "av1g_frame_header": FrameHeader, "av1
             "av1g_quant_params": QuantParams, "av1g_tu": Tu, "av1g_recon_job": ReconJob,
             "av1g_intra_tu": IntraTu, "av1g_intra_job": IntraJob, "av1g_ref_frame": RefFrame,
             "av1g_warp_ctx": WarpCtx, "av1g_obmc_neighbour": ObmcNeighbour, "av1g_inter_pred": InterPred,
-            "av1g_inter_job": InterJob, "av1g_warp_sample": WarpSample}
+            "av1g_inter_job": InterJob, "av1g_warp_sample": WarpSample, "av1g_config": Config,
+            "av1g_seq_info": SeqInfo, "av1g_frame_desc": FrameDesc, "av1g_frame_out": FrameOut,
+            "av1g_engine_stats": EngineStats}
 
 # exported entry points and their ctypes signatures
 _SIGS = {
@@ -191,6 +227,16 @@ _SIGS = {
     "av1g_run_recon": (C.c_int, [C.POINTER(ReconJob), C.c_int32, C.c_void_p]),
     "av1g_run_intra": (C.c_int, [C.POINTER(IntraJob), C.c_int32, C.c_void_p]),
     "av1g_run_inter": (C.c_int, [C.POINTER(InterJob), C.c_int32, C.c_void_p]),
+    "av1g_engine_create": (C.c_int, [C.POINTER(Config), C.POINTER(C.c_void_p)]),
+    "av1g_engine_destroy": (None, [C.c_void_p]),
+    "av1g_engine_get_stats": (C.c_int, [C.c_void_p, C.POINTER(EngineStats)]),
+    "av1g_stream_open": (C.c_int, [C.c_void_p, C.POINTER(SeqInfo), C.POINTER(C.c_void_p)]),
+    "av1g_stream_close": (C.c_int, [C.c_void_p]),
+    "av1g_stream_reset_refs": (C.c_int, [C.c_void_p]),
+    "av1g_submit_frame": (C.c_int, [C.c_void_p, C.POINTER(FrameDesc), C.POINTER(C.c_uint64)]),
+    "av1g_poll": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int64, C.POINTER(C.c_int)]),
+    "av1g_fetch_output": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(FrameOut)]),
+    "av1g_release_output": (C.c_int, [C.c_void_p, C.c_uint64]),
     "av1g_warp_estimation": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                        C.c_int16, C.c_int16, C.POINTER(C.c_int32), C.POINTER(C.c_uint8)]),
 }

@@ -266,7 +266,7 @@ av1g_status run(const av1g_frame_job* jobs, int n, int stage_mask, int mode, voi
         hs[st * (n + 1) + n] = acc;
         totals[st] = acc;
     }
-    e = cudaMemcpyAsync(dev, host.data(), off_scratch, cudaMemcpyHostToDevice, s);
+    e = upload(dev, host.data(), off_scratch, s);
     if (e != cudaSuccess) {
         cudaFreeAsync(dev, s);
         return cuda_fail(e, "cudaMemcpyAsync");
@@ -308,6 +308,33 @@ av1g_status run(const av1g_frame_job* jobs, int n, int stage_mask, int mode, voi
 
 }  // namespace
 
+namespace av1g {
+
+// The whole chain for a batch (the serving engine's post-filter step).
+av1g_status postfilter_run(const av1g_frame_job* jobs, int n, cudaStream_t s, std::string& err) {
+    av1g_status st = run(jobs, n, (1 << ST_COUNT) - 1, AV1G_MODE_BATCHED, s, nullptr);
+    if (st != AV1G_OK) err = g_err;
+    return st;
+}
+
+// The planes holding a job's cropped pre-grain result (the reference-slot
+// payload) and its output, after the stage gating.
+av1g_status postfilter_result_planes(const av1g_frame_job& j, PlaneDev pre[3], PlaneDev out[3], std::string& err) {
+    FrameDev F;
+    av1g_status st = prepare_frame(j, F);
+    if (st != AV1G_OK) {
+        err = g_err;
+        return st;
+    }
+    for (int p = 0; p < 3; p++) {
+        pre[p] = F.lr[p];
+        out[p] = F.out[p];
+    }
+    return AV1G_OK;
+}
+
+}  // namespace av1g
+
 extern "C" {
 
 int32_t av1g_abi_version(void) { return AV1G_ABI_VERSION; }
@@ -331,6 +358,11 @@ int32_t av1g_struct_size(const char* name) {
     if (!strcmp(name, "av1g_inter_pred")) return (int32_t)sizeof(av1g_inter_pred);
     if (!strcmp(name, "av1g_inter_job")) return (int32_t)sizeof(av1g_inter_job);
     if (!strcmp(name, "av1g_warp_sample")) return (int32_t)sizeof(av1g_warp_sample);
+    if (!strcmp(name, "av1g_config")) return (int32_t)sizeof(av1g_config);
+    if (!strcmp(name, "av1g_seq_info")) return (int32_t)sizeof(av1g_seq_info);
+    if (!strcmp(name, "av1g_frame_desc")) return (int32_t)sizeof(av1g_frame_desc);
+    if (!strcmp(name, "av1g_frame_out")) return (int32_t)sizeof(av1g_frame_out);
+    if (!strcmp(name, "av1g_engine_stats")) return (int32_t)sizeof(av1g_engine_stats);
     return -1;
 }
 

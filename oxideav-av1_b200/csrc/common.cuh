@@ -69,6 +69,10 @@ __device__ __forceinline__ long long round2ll(long long x, int n) {
 }
 __device__ __forceinline__ int floor_log2u(unsigned x) { return x ? 31 - __clz(x) : 0; }
 
+// Enqueues a host-to-device copy of n bytes through a pinned staging block
+// (returns once enqueued; the host bytes may be reused immediately).
+cudaError_t upload(void* dev, const void* host, size_t n, cudaStream_t s);
+
 __device__ __forceinline__ int ld_px(const PlaneDev& P, int hbd, int y, int x) {
     const uint8_t* row = P.p + (size_t)y * P.stride;
     return hbd ? (int)reinterpret_cast<const uint16_t*>(row)[x] : (int)row[x];

@@ -760,7 +760,7 @@ av1g_status inter_run(const av1g_inter_job* jobs, int n, cudaStream_t st, std::s
     memcpy(host.data() + o_sb, sb.data(), sizeof(uint32_t) * sb.size());
     if (!warps.empty()) memcpy(host.data() + o_w, warps.data(), sizeof(WarpRec) * warps.size());
     if (!segs.empty()) memcpy(host.data() + o_s, segs.data(), sizeof(Seg) * segs.size());
-    e = cudaMemcpyAsync(dev, host.data(), host_bytes, cudaMemcpyHostToDevice, st);
+    e = upload(dev, host.data(), host_bytes, st);
     if (e == cudaSuccess && bytes > host_bytes) e = cudaMemsetAsync(dev + host_bytes, 0, bytes - host_bytes, st);
     const InterFrame* df = (const InterFrame*)(dev + o_frames);
     const WarpRec* dw = (const WarpRec*)(dev + o_w);
@@ -777,8 +777,6 @@ av1g_status inter_run(const av1g_inter_job* jobs, int n, cudaStream_t st, std::s
                                                   (int)b.size(), sb.back(), dw, ds);
         e = cudaGetLastError();
     }
-    // (a copy from pageable memory has left the staging vector when
-    // cudaMemcpyAsync returns, so the vector may go out of scope now)
     cudaFreeAsync(dev, st);
     if (e != cudaSuccess) {
         err = std::string("inter launch: ") + cudaGetErrorString(e);

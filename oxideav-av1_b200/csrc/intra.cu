@@ -585,7 +585,7 @@ av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t st, std::s
     memcpy(host.data() + off_tus, all.data(), sizeof(av1g_intra_tu) * all.size());
     memcpy(host.data() + off_items, items.data(), sizeof(IntraItem) * items.size());
     if (!maps.empty()) memcpy(host.data() + off_maps, maps.data(), maps.size());
-    e = cudaMemcpyAsync(dev, host.data(), bytes, cudaMemcpyHostToDevice, st);
+    e = upload(dev, host.data(), bytes, st);
     const IntraFrame* df = (const IntraFrame*)dev;
     const av1g_intra_tu* dt = (const av1g_intra_tu*)(dev + off_tus);
     const IntraItem* di = (const IntraItem*)(dev + off_items);

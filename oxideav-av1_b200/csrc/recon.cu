@@ -160,7 +160,7 @@ av1g_status recon_run(const av1g_recon_job* jobs, int n, cudaStream_t s, std::st
         err = std::string("cudaMallocAsync: ") + cudaGetErrorString(e);
         return AV1G_EDEVICE;
     }
-    e = cudaMemcpyAsync(dev, host.data(), bytes, cudaMemcpyHostToDevice, s);
+    e = upload(dev, host.data(), bytes, s);
     if (e == cudaSuccess) {
         int nt = (int)tasks.size();
         int grid = nt < kSMs * 16 ? nt : kSMs * 16;

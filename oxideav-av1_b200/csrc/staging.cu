@@ -1,0 +1,75 @@
+// staging.cu — pinned host staging for descriptor uploads.
+//
+// The entry points build their device records (frame records, call lists,
+// tile prefixes) in host vectors.  A cudaMemcpyAsync from pageable memory
+// waits for the stream to drain before it starts, which would stall every
+// entry point until the GPU caught up and defeat the pipelining of the serving
+// engine.  upload() instead copies the bytes into a pinned block and enqueues
+// the copy from there; a block is reused once the event recorded after its
+// copy has completed.
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+
+namespace av1g {
+
+namespace {
+
+struct Block {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaEvent_t ev = nullptr;
+    int device = -1;
+};
+
+constexpr size_t kMinBlock = 64 << 10;
+constexpr size_t kMaxPinned = (size_t)2 << 30;  // beyond this, copy from pageable memory
+
+std::mutex g_mu;
+std::vector<Block> g_blocks;
+size_t g_pinned = 0;
+
+}  // namespace
+
+cudaError_t upload(void* dev, const void* host, size_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(g_mu);
+    Block* pick = nullptr;
+    for (Block& b : g_blocks) {
+        if (b.device != device || b.cap < n) continue;
+        cudaError_t q = cudaEventQuery(b.ev);
+        if (q == cudaSuccess) {
+            if (!pick || b.cap < pick->cap) pick = &b;
+        } else if (q != cudaErrorNotReady) {
+            return q;
+        }
+    }
+    if (!pick) {
+        size_t cap = kMinBlock;
+        while (cap < n) cap <<= 1;
+        if (g_pinned + cap > kMaxPinned) return cudaMemcpyAsync(dev, host, n, cudaMemcpyHostToDevice, s);
+        Block b;
+        b.device = device;
+        b.cap = cap;
+        e = cudaHostAlloc(&b.p, cap, cudaHostAllocPortable);
+        if (e != cudaSuccess) return e;
+        e = cudaEventCreateWithFlags(&b.ev, cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            cudaFreeHost(b.p);
+            return e;
+        }
+        g_pinned += cap;
+        g_blocks.push_back(b);
+        pick = &g_blocks.back();
+    }
+    memcpy(pick->p, host, n);
+    e = cudaMemcpyAsync(dev, pick->p, n, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return e;
+    return cudaEventRecord(pick->ev, s);
+}
+
+}  // namespace av1g

@@ -697,6 +697,7 @@ def make_inter_frame(seed, width=176, height=144, bit_depth=8, ssx=1, ssy=1, mon
         mi_map[r0:r0 + bh // 4, c0:c0 + bw // 4] = bi
 
     preds, nbs, warps = [], [], []
+    f.intra_blocks = [blk for bi, blk in enumerate(blocks) if info[bi]["intra"]]
     for bi, (x0, y0, bw, bh) in enumerate(blocks):
         b = info[bi]
         if b["intra"]:
@@ -817,3 +818,130 @@ def custom_inter_frame(width, height, refs, calls, neighbours=(), warps=(), bit_
         for k, v in c.items():
             f.warps[i][k] = v
     return f
+
+
+
+# ---------------------------------------------------------------------------
+# Streams of whole frames for the serving engine
+# ---------------------------------------------------------------------------
+
+class StreamFrame:
+    """One av1g_frame_desc: header, quantizer, post-filter side data, the
+    prediction and residual lists, and the reference / refresh / show fields."""
+
+    def __init__(self):
+        self.hdr = None
+        self.quant = None
+        self.grid = None
+        self.cdef_idx = None
+        self.lr_units = [None, None, None]
+        self.preds = self.neighbours = self.warps = None
+        self.inter_tus = self.intra_tus = None
+        self.palette_maps = None
+        self.coeffs = None
+        self.ref_frame_idx = [0] * 7
+        self.refresh = 0
+        self.show = 1
+        self.show_existing = 0
+        self.show_idx = 0
+
+
+def _intra_tus_for_blocks(rng, h, quant, blocks, sb_size, coeff_base):
+    """Intra TUs (modes, residuals) for the intra blocks of an inter frame, in
+    decode order (superblocks in raster order, blocks in partition order,
+    planes per block).  Above-right / below-left stay off so that every edge
+    sample read was decoded earlier in block order."""
+    tus, coeffs, off = [], [], coeff_base
+    ok_segs = [s for s in range(8) if not quant.lossless[s]]
+    sbs = {}
+    for b in blocks:
+        sbs.setdefault((b[1] // sb_size, b[0] // sb_size), []).append(b)
+    for key in sorted(sbs):
+        for (x0, y0, bw, bh) in sbs[key]:
+            for p in range(h.num_planes):
+                sx_, sy_ = (h.subsampling_x, h.subsampling_y) if p else (0, 0)
+                bx, by, w, hh = x0 >> sx_, y0 >> sy_, bw >> sx_, bh >> sy_
+                if w < 4 or hh < 4:
+                    continue
+                tw, th = min(w, 32), min(hh, 32)
+                if (tw, th) not in TX_OF:
+                    tw = th = min(tw, th)
+                tx = TX_OF[(tw, th)]
+                mode = int(rng.integers(0, 13))
+                ad = int(rng.integers(-3, 4)) if 1 <= mode <= 8 else 0
+                pw = (h.mi_cols * 4) >> sx_
+                ph = (h.mi_rows * 4) >> sy_
+                for ty in range(by, by + hh, th):
+                    for tx_ in range(bx, bx + w, tw):
+                        if ty >= ph or tx_ >= pw:
+                            continue
+                        flags = abi.INTRA_EDGE_FILTER
+                        if ty > 0:
+                            flags |= abi.INTRA_HAVE_ABOVE
+                        if tx_ > 0:
+                            flags |= abi.INTRA_HAVE_LEFT
+                        res = (tx_, ty, p, tx, 0, 0, 0, (0, 0, 0), 0)
+                        if ok_segs and rng.random() < 0.7:
+                            seg = int(rng.choice(ok_segs))
+                            flags |= abi.INTRA_RESIDUAL
+                            lv = _levels(rng, min(32, tw), min(32, th), False)
+                            res = (tx_, ty, p, tx, _tx_type_for(rng, tw, th), seg, int(rng.integers(1, 256)),
+                                   (0, 0, 0), off)
+                            coeffs.append(lv)
+                            off += len(lv)
+                        tus.append((tx_, ty, p, tx, mode, flags, ad, 0, 255, 0, 0, 0, res, (0, 0), 0, 0, 0, 0,
+                                    [0] * 8))
+    return np.array(tus, dtype=INTRA_TU_DTYPE) if tus else np.zeros(0, INTRA_TU_DTYPE), coeffs
+
+
+def make_stream(seed, n_frames=4, width=176, height=144, bit_depth=8, ssx=1, ssy=1, mono=False, superres_denom=8,
+                film_grain=False, sb_size=64, show_existing_at=(), palette=0.1):
+    """A key frame (intra TUs, palette blocks) then inter frames (inter calls
+    over a random partition with some intra blocks, residual TUs), each with
+    the post-filter side data of make_frame, random references among the
+    eight slots and random refresh flags.  Frames listed in show_existing_at
+    are show_existing_frame outputs of a random slot instead."""
+    rng = np.random.default_rng(seed)
+    frames = []
+    for k in range(n_frames):
+        fs = seed * 1000 + k
+        if k in show_existing_at:
+            fr = StreamFrame()
+            fr.hdr = frames[0].hdr
+            fr.show_existing = 1
+            fr.show_idx = int(rng.integers(0, 8))
+            fr.refresh = 0
+            frames.append(fr)
+            continue
+        base = make_frame(fs, width, height, bit_depth, ssx, ssy, mono, superres_denom, film_grain)
+        h = base.hdr
+        fw = h.frame_width
+        fr = StreamFrame()
+        fr.hdr, fr.grid, fr.cdef_idx, fr.lr_units = h, base.grid, base.cdef_idx, base.lr_units
+        if k == 0:
+            it = make_intra_frame(fs, fw, height, bit_depth, ssx, ssy, mono, sb_size, palette=palette)
+            fr.quant, fr.intra_tus, fr.coeffs, fr.palette_maps = it.quant, it.tus, it.coeffs, it.palette_maps
+            fr.refresh = 0xFF
+        else:
+            inter = make_inter_frame(fs, fw, height, bit_depth, ssx, ssy, mono, scaled=False, sb_size=sb_size,
+                                     p_intra=0.1, ref_dims=[(h.upscaled_width, height)] * 7)
+            preds = inter.preds.copy()
+            ii = preds["kind"] == abi.INTER_INTRA   # inter-intra needs its intra half inside the wavefront
+            preds["kind"][ii] = abi.INTER_SINGLE
+            fr.preds, fr.neighbours, fr.warps = preds, inter.neighbours, inter.warps
+            rec = make_recon_frame(fs + 500, fw, height, bit_depth, ssx, ssy, mono)
+            fr.quant, fr.inter_tus = rec.quant, rec.tus
+            itus, icoeffs = _intra_tus_for_blocks(rng, h, rec.quant, inter.intra_blocks, sb_size, len(rec.coeffs))
+            fr.intra_tus = itus
+            fr.coeffs = np.concatenate([rec.coeffs] + icoeffs).astype(np.int32)
+            fr.ref_frame_idx = [int(v) for v in rng.integers(0, 8, size=7)]
+            fr.refresh = int(rng.integers(0, 256)) & int(rng.integers(0, 256))
+        frames.append(fr)
+    return frames
+
+
+def stream_seq(frames, sb_size=64):
+    h = frames[0].hdr
+    return {"max_width": h.upscaled_width, "max_height": h.frame_height, "bit_depth": h.bit_depth,
+            "subsampling_x": h.subsampling_x, "subsampling_y": h.subsampling_y, "num_planes": h.num_planes,
+            "sb_size": sb_size}
