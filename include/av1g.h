@@ -491,8 +491,10 @@ typedef struct av1g_config {
     int32_t device;              /* CUDA device ordinal                           */
     int32_t max_batch;           /* frames (one per stream) per step; 0 = 64      */
     int64_t hbm_budget_bytes;    /* admission budget; 0 = 80% of free memory      */
-    int32_t max_inflight_steps;  /* steps enqueued ahead of completion; 0 = 3     */
-    int32_t pad;
+    int32_t max_inflight_steps;  /* steps enqueued ahead of completion, per lane;
+                                    0 = 3                                         */
+    int32_t lanes;               /* worker threads, each with a CUDA stream; a
+                                    stream of frames stays on one lane; 0 = 4     */
 } av1g_config;
 
 /* What a stream's sequence header fixes: the largest upscaled frame and the
@@ -566,6 +568,10 @@ typedef struct av1g_engine_stats {
     int64_t budget;
     int32_t streams_open;
     int32_t pad;
+    double host_ms;             /* worker time spent preparing and enqueuing steps */
+    double device_ms;           /* device time of the finished steps (events)      */
+    double host_stage_ms[6];    /* host_ms by part: uploads, inter, residual, intra,
+                                   post-filter, slots + outputs                    */
 } av1g_engine_stats;
 
 av1g_status av1g_engine_create(const av1g_config* cfg, av1g_engine** out);

@@ -166,7 +166,7 @@ INTER_SINGLE, INTER_COMPOUND, INTER_INTRA = 0, 1, 2
 
 class Config(C.Structure):
     _fields_ = [("device", C.c_int32), ("max_batch", C.c_int32), ("hbm_budget_bytes", C.c_int64),
-                ("max_inflight_steps", C.c_int32), ("pad", C.c_int32)]
+                ("max_inflight_steps", C.c_int32), ("lanes", C.c_int32)]
 
 
 class SeqInfo(C.Structure):
@@ -195,7 +195,8 @@ class FrameOut(C.Structure):
 class EngineStats(C.Structure):
     _fields_ = [("frames_done", C.c_int64), ("steps_done", C.c_int64), ("bytes_reserved", C.c_int64),
                 ("bytes_in_flight", C.c_int64), ("budget", C.c_int64), ("streams_open", C.c_int32),
-                ("pad", C.c_int32)]
+                ("pad", C.c_int32), ("host_ms", C.c_double), ("device_ms", C.c_double),
+                ("host_stage_ms", C.c_double * 6)]
 
 INTRA_HAVE_ABOVE, INTRA_HAVE_LEFT, INTRA_HAVE_ABOVE_RIGHT, INTRA_HAVE_BELOW_LEFT = 1, 2, 4, 8
 INTRA_EDGE_FILTER, INTRA_FILTER_TYPE, INTRA_RESIDUAL, INTRA_CFL = 16, 32, 64, 128

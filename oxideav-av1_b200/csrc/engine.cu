@@ -8,11 +8,13 @@
 // (reference_frame_update, src/decoder/frame_driver.rs:1409) and returns the
 // output frame (frame_driver.rs:1101-1116, output_existing_frame at 1495).
 //
-// Here a worker thread forms steps: it takes the oldest pending frame of each
-// stream that has one (up to max_batch frames, round robin), and enqueues for
-// the whole step one inter launch, one residual launch, the intra wavefront
-// and the post-filter chain (one launch per stage), then the slot refreshes
-// and the output copies, all on one CUDA stream.  A stream's next frame can
+// Worker threads ("lanes", each with its own CUDA stream; a stream of frames
+// belongs to one lane) form steps: a lane takes the oldest pending frame of
+// each of its streams that has one (up to max_batch frames, round robin), and
+// enqueues for the whole step one inter launch, one residual launch, the
+// intra wavefront and the post-filter chain (one launch per stage), then the
+// slot refreshes and the output copies, on its CUDA stream; lanes overlap
+// their host preparation and their device work.  A stream's next frame can
 // join the very next step: its references are the slot buffers the previous
 // step writes, and stream order on the device keeps the two in sequence.  A
 // completion thread retires steps in order through their events and wakes
@@ -69,6 +71,7 @@ int r2u(int v, int s) { return (v + s) >> s; }
 // output_existing_frame needs (grain parameters, format).
 struct SlotBuf {
     av1g_engine* eng = nullptr;
+    cudaStream_t cs = nullptr;  // the lane stream every use of the slot is ordered on
     uint8_t* dev = nullptr;
     size_t bytes = 0;
     av1g_plane planes[3] = {};
@@ -110,15 +113,27 @@ struct Ticket {
 };
 
 struct Step {
-    cudaEvent_t ev = nullptr;
+    cudaEvent_t ev = nullptr, ev0 = nullptr;
     std::vector<std::shared_ptr<Ticket>> tickets;
     size_t work_bytes = 0;
+    Clock::time_point t_enqueued;
+};
+
+// A worker thread with its own CUDA stream.  Each stream of frames belongs to
+// one lane, so its frames and slot updates stay ordered on that CUDA stream
+// while lanes prepare and run steps concurrently.
+struct Lane {
+    int idx = 0;
+    cudaStream_t cs = nullptr;
+    std::deque<Step> steps;
+    std::thread thread;
 };
 
 }  // namespace
 
 struct av1g_stream {
     av1g_engine* eng = nullptr;
+    int lane = 0;
     av1g_seq_info seq = {};
     std::shared_ptr<SlotBuf> slots[8];
     std::deque<std::shared_ptr<Ticket>> pending;
@@ -129,19 +144,19 @@ struct av1g_stream {
 
 struct av1g_engine {
     int device = 0;
-    cudaStream_t cs = nullptr;
     size_t budget = 0, reserved = 0, inflight_bytes = 0;
     int max_batch = 64, max_steps = 3;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::vector<av1g_stream*> streams;
-    size_t rr = 0;
+    size_t rr = 0, next_lane = 0;
     std::unordered_map<uint64_t, std::shared_ptr<Ticket>> tickets;
-    std::deque<Step> steps;
-    std::thread worker, completer;
+    std::vector<std::unique_ptr<Lane>> lanes;
+    std::thread completer;
     bool stop = false, worker_done = false;
     uint64_t next_id = 1;
     int64_t frames_done = 0, steps_done = 0;
+    double host_ms = 0, device_ms = 0, host_stage_ms[6] = {};
     // pinned output blocks by size
     std::mutex pin_mu;
     std::multimap<size_t, uint8_t*> pinned_free;
@@ -170,7 +185,7 @@ struct av1g_engine {
 SlotBuf::~SlotBuf() {
     if (dev && eng) {
         DeviceGuard g(eng->device);
-        cudaFreeAsync(dev, eng->cs);
+        cudaFreeAsync(dev, cs);
     }
 }
 
@@ -307,8 +322,14 @@ void run_stage(std::vector<Work*>& ws, std::vector<Job>& jobs, Fn fn, cudaStream
     }
 }
 
-void enqueue_step(av1g_engine* E, std::vector<std::shared_ptr<Ticket>>& batch, Step& step) {
-    cudaStream_t cs = E->cs;
+void enqueue_step(av1g_engine* E, cudaStream_t cs, std::vector<std::shared_ptr<Ticket>>& batch, Step& step,
+                  double part_ms[6]) {
+    auto tp = Clock::now();
+    auto lap = [&](int k) {
+        auto now = Clock::now();
+        part_ms[k] += std::chrono::duration<double, std::milli>(now - tp).count();
+        tp = now;
+    };
     std::vector<Work> works(batch.size());
     for (size_t i = 0; i < batch.size(); i++) {
         Work& w = works[i];
@@ -387,6 +408,7 @@ void enqueue_step(av1g_engine* E, std::vector<std::shared_ptr<Ticket>>& batch, S
             if (e != cudaSuccess) fail_work(w, AV1G_EDEVICE, std::string("upload: ") + cudaGetErrorString(e));
         }
     }
+    lap(0);
     // prediction and residual stages, batched across the step's frames
     {
         std::vector<Work*> ws;
@@ -408,6 +430,7 @@ void enqueue_step(av1g_engine* E, std::vector<std::shared_ptr<Ticket>>& batch, S
         }
         run_stage(ws, jobs, inter_run, cs);
     }
+    lap(1);
     {
         std::vector<Work*> ws;
         std::vector<av1g_recon_job> jobs;
@@ -425,6 +448,7 @@ void enqueue_step(av1g_engine* E, std::vector<std::shared_ptr<Ticket>>& batch, S
         }
         run_stage(ws, jobs, recon_run, cs);
     }
+    lap(2);
     {
         std::vector<Work*> ws;
         std::vector<av1g_intra_job> jobs;
@@ -445,6 +469,7 @@ void enqueue_step(av1g_engine* E, std::vector<std::shared_ptr<Ticket>>& batch, S
         }
         run_stage(ws, jobs, intra_run, cs);
     }
+    lap(3);
     // the §7.4 chain
     std::vector<av1g_frame_job> fjobs(works.size());
     {
@@ -481,6 +506,7 @@ void enqueue_step(av1g_engine* E, std::vector<std::shared_ptr<Ticket>>& batch, S
         }
         run_stage(ws, jobs, postfilter_run, cs);
     }
+    lap(4);
     // slot refreshes and outputs
     for (size_t i = 0; i < works.size(); i++) {
         Work& w = works[i];
@@ -500,6 +526,7 @@ void enqueue_step(av1g_engine* E, std::vector<std::shared_ptr<Ticket>>& batch, S
                 payload = std::make_shared<SlotBuf>();
                 SlotBuf& sl = *payload;
                 sl.eng = E;
+                sl.cs = cs;
                 sl.upscaled_width = t.hdr.upscaled_width;
                 sl.frame_height = t.hdr.frame_height;
                 sl.grain = t.hdr.film_grain;
@@ -567,18 +594,21 @@ void enqueue_step(av1g_engine* E, std::vector<std::shared_ptr<Ticket>>& batch, S
         }
         if (w.B.dev) cudaFreeAsync(w.B.dev, cs);
     }
+    lap(5);
 }
 
-void worker_loop(av1g_engine* E) {
+void worker_loop(av1g_engine* E, Lane* L) {
     cudaSetDevice(E->device);
     std::unique_lock<std::mutex> lk(E->mu);
+    size_t rr = 0;
     while (!E->stop) {
         std::vector<std::shared_ptr<Ticket>> batch;
         size_t extra = 0;
-        if ((int)E->steps.size() < E->max_steps) {
+        if ((int)L->steps.size() < E->max_steps) {
             size_t n = E->streams.size();
             for (size_t k = 0; k < n && (int)batch.size() < E->max_batch; k++) {
-                av1g_stream* S = E->streams[(E->rr + k) % n];
+                av1g_stream* S = E->streams[(rr + k) % n];
+                if (S->lane != L->idx) continue;
                 // reset markers are applied in order, between frames
                 while (!S->pending.empty() && S->pending.front()->reset_marker) {
                     std::shared_ptr<Ticket> r = S->pending.front();
@@ -606,7 +636,7 @@ void worker_loop(av1g_engine* E) {
                 extra += t->work_bytes;
                 batch.push_back(t);
             }
-            if (n) E->rr = (E->rr + 1) % n;
+            if (n) rr = (rr + 1) % n;
         }
         if (batch.empty()) {
             E->cv_work.wait_for(lk, std::chrono::milliseconds(20));
@@ -614,8 +644,12 @@ void worker_loop(av1g_engine* E) {
         }
         E->inflight_bytes += extra;
         lk.unlock();
+        auto h0 = Clock::now();
         Step step;
-        enqueue_step(E, batch, step);
+        cudaEventCreate(&step.ev0);
+        cudaEventRecord(step.ev0, L->cs);
+        double part[6] = {};
+        enqueue_step(E, L->cs, batch, step, part);
         // the descriptor copies have been staged; keep only the outputs
         for (auto& t : batch) {
             for (auto& g : t->grid) std::vector<uint8_t>().swap(g);
@@ -631,10 +665,14 @@ void worker_loop(av1g_engine* E) {
         }
         step.tickets = batch;
         step.work_bytes = extra;
-        cudaEventCreateWithFlags(&step.ev, cudaEventDisableTiming);
-        cudaEventRecord(step.ev, E->cs);
+        cudaEventCreate(&step.ev);
+        cudaEventRecord(step.ev, L->cs);
+        step.t_enqueued = Clock::now();
+        double hms = std::chrono::duration<double, std::milli>(Clock::now() - h0).count();
         lk.lock();
-        E->steps.push_back(std::move(step));
+        E->host_ms += hms;
+        for (int k = 0; k < 6; k++) E->host_stage_ms[k] += part[k];
+        L->steps.push_back(std::move(step));
         E->cv_done.notify_all();
     }
 }
@@ -643,39 +681,55 @@ void completer_loop(av1g_engine* E) {
     cudaSetDevice(E->device);
     std::unique_lock<std::mutex> lk(E->mu);
     for (;;) {
-        if (E->steps.empty()) {
+        bool any = false;
+        for (auto& L : E->lanes) any = any || !L->steps.empty();
+        if (!any) {
             if (E->worker_done) break;
             E->cv_done.wait_for(lk, std::chrono::milliseconds(20));
             continue;
         }
-        cudaEvent_t ev = E->steps.front().ev;
-        lk.unlock();
-        // bounded wait: a step that has not finished after a minute is failed
-        cudaError_t q = cudaEventQuery(ev);
-        auto t0 = Clock::now();
-        while (q == cudaErrorNotReady && Clock::now() - t0 < std::chrono::seconds(60)) {
-            std::this_thread::sleep_for(std::chrono::microseconds(50));
-            q = cudaEventQuery(ev);
-        }
-        lk.lock();
-        Step step = std::move(E->steps.front());
-        E->steps.pop_front();
-        auto now = Clock::now();
-        for (auto& t : step.tickets) {
-            if (q != cudaSuccess && t->status == AV1G_OK) {
-                t->status = q == cudaErrorNotReady ? AV1G_TIMEOUT : AV1G_EDEVICE;
-                t->err = q == cudaErrorNotReady ? "step did not finish within 60 s" : cudaGetErrorString(q);
+        // retire, per lane and in order, every step whose event has completed;
+        // a step still running a minute after it was enqueued is failed
+        bool progressed = false;
+        for (auto& L : E->lanes) {
+            while (!L->steps.empty()) {
+                Step& front = L->steps.front();
+                cudaError_t q = cudaEventQuery(front.ev);
+                bool expired = q == cudaErrorNotReady && Clock::now() - front.t_enqueued > std::chrono::seconds(60);
+                if (q == cudaErrorNotReady && !expired) break;
+                Step step = std::move(front);
+                L->steps.pop_front();
+                auto now = Clock::now();
+                for (auto& t : step.tickets) {
+                    if (q != cudaSuccess && t->status == AV1G_OK) {
+                        t->status = expired ? AV1G_TIMEOUT : AV1G_EDEVICE;
+                        t->err = expired ? "step did not finish within 60 s" : cudaGetErrorString(q);
+                    }
+                    t->done = true;
+                    t->t_done = now;
+                    t->st->inflight--;
+                    E->frames_done++;
+                }
+                E->steps_done++;
+                E->inflight_bytes -= step.work_bytes;
+                float dms = 0.f;
+                if (q == cudaSuccess && cudaEventElapsedTime(&dms, step.ev0, step.ev) == cudaSuccess)
+                    E->device_ms += dms;
+                if (!expired) {
+                    cudaEventDestroy(step.ev);
+                    cudaEventDestroy(step.ev0);
+                }
+                progressed = true;
             }
-            t->done = true;
-            t->t_done = now;
-            t->st->inflight--;
-            E->frames_done++;
         }
-        E->steps_done++;
-        E->inflight_bytes -= step.work_bytes;
-        if (q != cudaErrorNotReady) cudaEventDestroy(step.ev);
-        E->cv_done.notify_all();
-        E->cv_work.notify_all();
+        if (progressed) {
+            E->cv_done.notify_all();
+            E->cv_work.notify_all();
+        } else {
+            lk.unlock();
+            std::this_thread::sleep_for(std::chrono::microseconds(50));
+            lk.lock();
+        }
     }
 }
 
@@ -711,12 +765,19 @@ av1g_status av1g_engine_create(const av1g_config* cfg, av1g_engine** out) {
     E->device = cfg->device;
     E->max_batch = cfg->max_batch > 0 ? cfg->max_batch : 64;
     E->max_steps = cfg->max_inflight_steps > 0 ? cfg->max_inflight_steps : 3;
+    int nl = cfg->lanes > 0 ? cfg->lanes : 4;
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     E->budget = cfg->hbm_budget_bytes > 0 ? (size_t)cfg->hbm_budget_bytes : free_b / 10 * 8;
-    if (cudaStreamCreateWithFlags(&E->cs, cudaStreamNonBlocking) != cudaSuccess) {
-        delete E;
-        return AV1G_EDEVICE;
+    for (int i = 0; i < nl; i++) {
+        auto L = std::make_unique<Lane>();
+        L->idx = i;
+        if (cudaStreamCreateWithFlags(&L->cs, cudaStreamNonBlocking) != cudaSuccess) {
+            for (auto& l : E->lanes) cudaStreamDestroy(l->cs);
+            delete E;
+            return AV1G_EDEVICE;
+        }
+        E->lanes.push_back(std::move(L));
     }
     // keep freed stream-ordered memory in the pool between steps
     cudaMemPool_t pool;
@@ -724,7 +785,7 @@ av1g_status av1g_engine_create(const av1g_config* cfg, av1g_engine** out) {
         uint64_t thr = E->budget;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
     }
-    E->worker = std::thread(worker_loop, E);
+    for (auto& L : E->lanes) L->thread = std::thread(worker_loop, E, L.get());
     E->completer = std::thread(completer_loop, E);
     *out = E;
     return AV1G_OK;
@@ -737,7 +798,8 @@ void av1g_engine_destroy(av1g_engine* E) {
         // let queued frames drain (bounded)
         auto t0 = Clock::now();
         while (Clock::now() - t0 < std::chrono::seconds(120)) {
-            bool busy = !E->steps.empty();
+            bool busy = false;
+            for (auto& L : E->lanes) busy = busy || !L->steps.empty();
             for (auto* S : E->streams) busy = busy || !S->pending.empty();
             if (!busy) break;
             E->cv_done.wait_for(lk, std::chrono::milliseconds(20));
@@ -745,7 +807,7 @@ void av1g_engine_destroy(av1g_engine* E) {
         E->stop = true;
     }
     E->cv_work.notify_all();
-    E->worker.join();
+    for (auto& L : E->lanes) L->thread.join();
     {
         std::lock_guard<std::mutex> lk(E->mu);
         E->worker_done = true;
@@ -759,9 +821,9 @@ void av1g_engine_destroy(av1g_engine* E) {
     }
     for (auto& kv : E->tickets) E->pinned_put(kv.second->host_out);
     E->tickets.clear();
-    cudaStreamSynchronize(E->cs);
+    for (auto& L : E->lanes) cudaStreamSynchronize(L->cs);
     for (auto& kv : E->pinned_free) cudaFreeHost(kv.second - sizeof(size_t));
-    cudaStreamDestroy(E->cs);
+    for (auto& L : E->lanes) cudaStreamDestroy(L->cs);
     delete E;
 }
 
@@ -775,6 +837,9 @@ av1g_status av1g_engine_get_stats(av1g_engine* E, av1g_engine_stats* o) {
     o->budget = (int64_t)E->budget;
     o->streams_open = (int32_t)E->streams.size();
     o->pad = 0;
+    o->host_ms = E->host_ms;
+    o->device_ms = E->device_ms;
+    for (int k = 0; k < 6; k++) o->host_stage_ms[k] = E->host_stage_ms[k];
     return AV1G_OK;
 }
 
@@ -791,6 +856,7 @@ av1g_status av1g_stream_open(av1g_engine* E, const av1g_seq_info* q, av1g_stream
     if (E->reserved + need > E->budget) return AV1G_ENOMEM_BUDGET;
     auto* S = new av1g_stream();
     S->eng = E;
+    S->lane = (int)(E->next_lane++ % E->lanes.size());
     S->seq = *q;
     S->reserved = need;
     E->reserved += need;

@@ -21,13 +21,14 @@ struct Block {
     size_t cap = 0;
     cudaEvent_t ev = nullptr;
     int device = -1;
+    bool busy = false;  // taken by a caller that has not recorded its event yet
 };
 
 constexpr size_t kMinBlock = 64 << 10;
 constexpr size_t kMaxPinned = (size_t)2 << 30;  // beyond this, copy from pageable memory
 
 std::mutex g_mu;
-std::vector<Block> g_blocks;
+std::vector<Block*> g_blocks;  // stable addresses: callers hold a block outside the lock
 size_t g_pinned = 0;
 
 }  // namespace
@@ -37,39 +38,48 @@ cudaError_t upload(void* dev, const void* host, size_t n, cudaStream_t s) {
     int device = 0;
     cudaError_t e = cudaGetDevice(&device);
     if (e != cudaSuccess) return e;
-    std::lock_guard<std::mutex> lk(g_mu);
     Block* pick = nullptr;
-    for (Block& b : g_blocks) {
-        if (b.device != device || b.cap < n) continue;
-        cudaError_t q = cudaEventQuery(b.ev);
-        if (q == cudaSuccess) {
-            if (!pick || b.cap < pick->cap) pick = &b;
-        } else if (q != cudaErrorNotReady) {
-            return q;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        for (Block* b : g_blocks) {
+            if (b->busy || b->device != device || b->cap < n) continue;
+            cudaError_t q = cudaEventQuery(b->ev);
+            if (q == cudaSuccess) {
+                if (!pick || b->cap < pick->cap) pick = b;
+            } else if (q != cudaErrorNotReady) {
+                return q;
+            }
         }
-    }
-    if (!pick) {
-        size_t cap = kMinBlock;
-        while (cap < n) cap <<= 1;
-        if (g_pinned + cap > kMaxPinned) return cudaMemcpyAsync(dev, host, n, cudaMemcpyHostToDevice, s);
-        Block b;
-        b.device = device;
-        b.cap = cap;
-        e = cudaHostAlloc(&b.p, cap, cudaHostAllocPortable);
-        if (e != cudaSuccess) return e;
-        e = cudaEventCreateWithFlags(&b.ev, cudaEventDisableTiming);
-        if (e != cudaSuccess) {
-            cudaFreeHost(b.p);
-            return e;
+        if (!pick) {
+            size_t cap = kMinBlock;
+            while (cap < n) cap <<= 1;
+            if (g_pinned + cap > kMaxPinned) return cudaMemcpyAsync(dev, host, n, cudaMemcpyHostToDevice, s);
+            auto* b = new Block();
+            b->device = device;
+            b->cap = cap;
+            e = cudaHostAlloc(&b->p, cap, cudaHostAllocPortable);
+            if (e != cudaSuccess) {
+                delete b;
+                return e;
+            }
+            e = cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming);
+            if (e != cudaSuccess) {
+                cudaFreeHost(b->p);
+                delete b;
+                return e;
+            }
+            g_pinned += cap;
+            g_blocks.push_back(b);
+            pick = b;
         }
-        g_pinned += cap;
-        g_blocks.push_back(b);
-        pick = &g_blocks.back();
+        pick->busy = true;
     }
     memcpy(pick->p, host, n);
     e = cudaMemcpyAsync(dev, pick->p, n, cudaMemcpyHostToDevice, s);
-    if (e != cudaSuccess) return e;
-    return cudaEventRecord(pick->ev, s);
+    if (e == cudaSuccess) e = cudaEventRecord(pick->ev, s);
+    std::lock_guard<std::mutex> lk(g_mu);
+    pick->busy = false;
+    return e;
 }
 
 }  // namespace av1g
