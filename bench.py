@@ -91,16 +91,25 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def dram_traffic(kernel, workload):
-    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, or None."""
+def dram_traffic(kernel, workload, kind=None):
+    """Per-frame DRAM bytes (kind None) or warp instructions (kind "inst") of
+    `kernel` from the committed ncu summary, or None."""
     p = ROOT / "profiles" / "dram_traffic.txt"
     if not p.exists():
         return None
     for line in p.read_text().splitlines():
         parts = line.split()
-        if len(parts) >= 3 and not line.startswith("#") and parts[0] == kernel and parts[1] == workload:
+        if line.startswith("#"):
+            continue
+        if kind:
+            if len(parts) >= 4 and parts[0] == kind and parts[1] == kernel and parts[2] == workload:
+                return int(parts[3])
+        elif len(parts) >= 3 and parts[0] == kernel and parts[1] == workload:
             return int(parts[2])
     return None
+
+
+SMS, SCHEDULERS_PER_SM = 148, 4
 
 
 class ClockSampler:
@@ -250,12 +259,13 @@ def run_gpu(args):
     torch.cuda.synchronize()
     ev_start = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ev_stage = [[torch.cuda.Event(enable_timing=True) for _ in stages] for _ in range(args.steps)]
-    with ClockSampler(local) as clk:
-        with torch.cuda.stream(stream):
-            for k in range(args.steps):
-                ev_start[k].record(stream)
-                step(ev_stage[k])
-        torch.cuda.synchronize()
+    clk = ClockSampler(local)
+    clk.__enter__()   # clocks sampled over the timed steps and the per-frame / e2e runs that follow
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            ev_start[k].record(stream)
+            step(ev_stage[k])
+    torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     stage_ms = {name: 0.0 for name, _ in stages}
@@ -287,6 +297,8 @@ def run_gpu(args):
     per_frame_ms = e0.elapsed_time(e1) / args.steps
 
     e2e = run_e2e(args, frames, dframes, jobs, stream, dev, world)
+    clk.__exit__(None, None, None)
+    clocks = clk.summary()
 
     # roofline of the dominant kernel
     ab = algorithmic_bytes(frames[0])
@@ -299,6 +311,15 @@ def run_gpu(args):
     traffic = dram_traffic(kernel_name, workload)
     if traffic is not None:
         traffic = traffic * n  # summary holds bytes per frame
+    inst = dram_traffic(kernel_name, workload, "inst")
+    issue = None
+    if inst is not None and clocks.get("sm_mhz"):
+        peak_inst = SMS * SCHEDULERS_PER_SM * clocks["sm_mhz"] * 1e6
+        ach_inst = inst * n / (launch_ms / 1e3)
+        issue = {"achieved_warp_inst_per_s": ach_inst, "peak_warp_inst_per_s": peak_inst,
+                 "frac": ach_inst / peak_inst,
+                 "note": "the kernel's real ceiling: 148 SMs x 4 warp instructions per clock at the sampled SM "
+                         "clock; instruction count from the committed ncu capture"}
     stage_frac = {}
     for name in stage_ms:
         a = ab[name] * n / (stage_ms[name] / args.steps / 1e3) / 1e9
@@ -311,13 +332,13 @@ def run_gpu(args):
         "config": config_block(args, n),
         "roofline": {"bound": "hbm", "kernel": kernel_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
-                     if peak_kind == "measured" else "fallback 6650 GB/s"},
+                     if peak_kind == "measured" else "fallback 6650 GB/s", "issue": issue},
         "stages": stage_frac,
         "per_frame_path": {"value": world * n / (per_frame_ms / 1e3), "unit": UNIT, "ms_per_step": per_frame_ms,
                            "launches_per_step": None},
         "e2e": e2e,
         "gpu_launches": len(stages) * args.steps,
-        "clocks": clk.summary(),
+        "clocks": clocks,
     }
     if rank == 0 and world == 1 and not args.no_serving:
         line["serving"] = run_serving(args, local)
@@ -462,52 +483,96 @@ def run_serving(args, local):
     return out
 
 
-def run_e2e(args, frames, dframes, jobs, stream, dev, world):
-    """Frames/s through the C-ABI with host buffers: inputs H2D from pinned memory
-    and the restored (cropped) planes D2H every step."""
+def run_e2e(args, frames, dframes, jobs, stream, dev, world, chunks=8):
+    """Frames/s through the C-ABI with host buffers: every step copies all
+    inputs from pinned host memory, runs av1g_run_postfilter and copies the
+    restored (cropped) planes back.  The batch is cut into `chunks` groups of
+    frames so that the copies of one group overlap the kernels of the next
+    (three CUDA streams: host-to-device, compute, device-to-host), the way a
+    serving loop feeds the engine; every byte is still copied every step."""
     import torch
     from oxideav_av1_b200 import postfilter
 
     lib = abi.load()
-    sp = C.c_void_p(stream.cuda_stream)
     n = len(dframes)
-    # pinned host copies of every input the chain reads, and of every output
+    per = (n + chunks - 1) // chunks
+    groups = [list(range(c * per, min(n, (c + 1) * per))) for c in range(chunks) if c * per < n]
+
+    def arena(tensors):
+        """Moves the tensors into views of one device buffer (256-byte aligned
+        offsets), so that a group's inputs or outputs cross PCIe as one copy."""
+        offs, total = [], 0
+        for t in tensors:
+            offs.append(total)
+            total = (total + t.numel() * t.element_size() + 255) // 256 * 256
+        buf = torch.empty(total, dtype=torch.uint8, device=dev)
+        views = []
+        for t, o in zip(tensors, offs):
+            v = buf[o:o + t.numel() * t.element_size()].view(t.dtype).view(t.shape)
+            v.copy_(t)
+            views.append(v)
+        return buf, views
+
     h_in, d_in, h_out, d_out = [], [], [], []
-    for f, d in zip(frames, dframes):
-        for p, pl in enumerate(d.recon):
-            h_in.append(pl.t.cpu().pin_memory())
-            d_in.append(pl.t)
-        for k in d.GRID_KEYS:
-            h_in.append(d.grid[k].cpu().pin_memory())
-            d_in.append(d.grid[k])
-        h_in.append(d.cdef_idx.cpu().pin_memory())
-        d_in.append(d.cdef_idx)
-        for u in d.lr_units:
-            if u is not None:
-                h_in.append(u.cpu().pin_memory())
-                d_in.append(u)
-        for p, pl in enumerate(d.stage_planes()["lr"]):
-            h_out.append(torch.empty_like(pl.t, device="cpu").pin_memory())
-            d_out.append(pl.t)
-    h2d = sum(t.numel() * t.element_size() for t in h_in)
-    d2h = sum(t.numel() * t.element_size() for t in h_out)
+    for g in groups:
+        ins, outs = [], []
+        for i in g:
+            d = dframes[i]
+            ins += [pl.t for pl in d.recon] + [d.grid[k] for k in d.GRID_KEYS] + [d.cdef_idx]
+            ins += [u for u in d.lr_units if u is not None]
+            outs += [pl.t for pl in d.stage_planes()["lr"]]
+        buf_in, vin = arena(ins)
+        buf_out, vout = arena(outs)
+        it_in, it_out = iter(vin), iter(vout)
+        for i in g:       # re-point the frames at the arena views, in the same order
+            d = dframes[i]
+            for pl in d.recon:
+                pl.t = next(it_in)
+            for k in d.GRID_KEYS:
+                d.grid[k] = next(it_in)
+            d.cdef_idx = next(it_in)
+            d.lr_units = [next(it_in) if u is not None else None for u in d.lr_units]
+            for pl in d.stage_planes()["lr"]:
+                pl.t = next(it_out)
+        d_in.append(buf_in)
+        d_out.append(buf_out)
+        h_in.append(buf_in.cpu().pin_memory())
+        h_out.append(torch.empty_like(buf_out, device="cpu").pin_memory())
+    gjobs = [postfilter.jobs_array([dframes[i] for i in g]) for g in groups]
+    s_in, s_out = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
+    h2d = sum(t.numel() for t in h_in)
+    d2h = sum(t.numel() for t in h_out)
+    sp = C.c_void_p(stream.cuda_stream)
+
+    ev_comp = [torch.cuda.Event() for _ in groups]   # group's kernels done (inputs free)
+    ev_d2h = [torch.cuda.Event() for _ in groups]    # group's outputs copied out (outputs free)
+    ev_in = [torch.cuda.Event() for _ in groups]
 
     def step():
-        for h, d in zip(h_in, d_in):
-            d.copy_(h, non_blocking=True)
-        abi.check(lib.av1g_run_postfilter(jobs, n, abi.MODE_BATCHED, sp, None))
-        for h, d in zip(h_out, d_out):
-            h.copy_(d, non_blocking=True)
+        for gi in range(len(groups)):
+            with torch.cuda.stream(s_in):
+                s_in.wait_event(ev_comp[gi])
+                d_in[gi].copy_(h_in[gi], non_blocking=True)
+                ev_in[gi].record(s_in)
+            stream.wait_event(ev_in[gi])
+            stream.wait_event(ev_d2h[gi])
+            abi.check(lib.av1g_run_postfilter(gjobs[gi], len(groups[gi]), abi.MODE_BATCHED, sp, None))
+            ev_comp[gi].record(stream)
+            with torch.cuda.stream(s_out):
+                s_out.wait_event(ev_comp[gi])
+                h_out[gi].copy_(d_out[gi], non_blocking=True)
+                ev_d2h[gi].record(s_out)
 
-    with torch.cuda.stream(stream):
-        for _ in range(max(args.warmup, 3)):
-            step()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.steps):
-            step()
-        e1.record(stream)
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s_in.wait_event(e0)
+    for _ in range(args.steps):
+        step()
+    stream.wait_stream(s_out)
+    e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
     t = torch.tensor([ms], device=dev)
@@ -516,7 +581,10 @@ def run_e2e(args, frames, dframes, jobs, stream, dev, world):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms = float(t.item())
     return {"value": world * n / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-            "ms_per_step": ms, "path": "av1g_run_postfilter with pinned-host inputs/outputs copied every step"}
+            "ms_per_step": ms,
+            "path": f"av1g_run_postfilter with pinned-host inputs/outputs copied every step, {len(groups)} groups "
+                    f"of frames (one copy in and one copy out per group) pipelined over copy-in / compute / "
+                    f"copy-out streams"}
 
 
 def main():

@@ -8,10 +8,12 @@
 // marking samples outside the plane as unavailable (the reference's
 // CdefAvailable == 0 arm, cdef.rs:564-590).
 //
-// Direction search (cdef.rs:366-456): eight threads per 8x8 luma block, one
-// per direction, each accumulating its own partial-sum line set and cost;
-// the block's direction is the arg-max over the eight lanes with the lowest
-// index winning ties, exactly the reference's first-strictly-greater scan.
+// Direction search (cdef.rs:366-456): one thread per (8x8 luma block,
+// direction), laid out so that every warp evaluates a single direction for
+// 32 blocks (the cost's bin pattern is fixed at compile time per direction,
+// so a warp never diverges); the block's direction is then the arg-max over
+// the eight costs with the lowest index winning ties, exactly the reference's
+// first-strictly-greater scan.
 // Filtering (cdef.rs:465-590): one thread per sample with the block's
 // primary / secondary tap offsets read from a per-direction table; tiles
 // whose halo lies inside the plane take a path without availability tests.
@@ -36,25 +38,34 @@ struct BlockParams {
     int8_t active;  // 0: copy through
     int8_t ydir;
     int8_t uvdir;
-    int8_t pad;
+    int8_t padj_y;  // primary damping shift of pri_y
     int32_t pri_y;  // variance-scaled luma primary strength
 };
 
-// Cost of direction D over an 8x8 block (cdef.rs:366-440), bins fixed at compile time.
+// Cost of direction D over an 8x8 block (cdef.rs:366-440), bins fixed at
+// compile time.  blk: the block's 64 samples, row-major, already shifted to
+// 8 bits and centred ((v >> (bitDepth - 8)) - 128), 8-byte aligned.
 template <int D>
-__device__ __forceinline__ int dir_cost(const int16_t* w, int shift) {
+__device__ __forceinline__ int dir_cost(const int16_t* blk) {
     constexpr int NB = (D == 2 || D == 6) ? 8 : ((D & 1) ? 11 : 15);
     int p[NB];
 #pragma unroll
     for (int k = 0; k < NB; k++) p[k] = 0;
+    const uint2* q = reinterpret_cast<const uint2*>(blk);
 #pragma unroll
     for (int i = 0; i < 8; i++)
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
-            int x = (w[i * WP + j] >> shift) - 128;
-            int b = D == 0 ? i + j : D == 1 ? i + j / 2 : D == 2 ? i : D == 3 ? 3 + i - j / 2
-                  : D == 4 ? 7 + i - j : D == 5 ? 3 - i / 2 + j : D == 6 ? j : i / 2 + j;
-            p[b] += x;
+        for (int hh = 0; hh < 2; hh++) {
+            const uint2 w = q[i * 2 + hh];
+            const int xs[4] = {(int)(int16_t)(w.x & 0xffffu), (int)w.x >> 16, (int)(int16_t)(w.y & 0xffffu),
+                               (int)w.y >> 16};
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const int j = hh * 4 + e;
+                const int b = D == 0 ? i + j : D == 1 ? i + j / 2 : D == 2 ? i : D == 3 ? 3 + i - j / 2
+                            : D == 4 ? 7 + i - j : D == 5 ? 3 - i / 2 + j : D == 6 ? j : i / 2 + j;
+                p[b] += xs[e];
+            }
         }
     int cost = 0;
     if (D == 2 || D == 6) {
@@ -84,25 +95,43 @@ __device__ __forceinline__ int constrain_adj(int diff, int threshold, int adj) {
     return diff < 0 ? -v : v;
 }
 
+// Tap offsets of one direction: primary (k = 0, 1), then the two secondary
+// directions (dir + 2, dir - 2) for k = 0, 1.
+struct Taps {
+    int p0, p1, a0, a1, b0, b1;
+};
+
+__device__ __forceinline__ Taps taps_of(const int16_t* toff, int dir) {
+    const int da = (dir + 2) & 7, db = (dir + 6) & 7;
+    return Taps{toff[dir * 2], toff[dir * 2 + 1], toff[da * 2], toff[da * 2 + 1], toff[db * 2], toff[db * 2 + 1]};
+}
+
+// One tap pair (+o and -o) of weight w: constrain (cdef.rs:592-606) with the
+// damping shift precomputed, accumulated into sum; min / max of the samples
+// taken (the reference's clip range, cdef.rs:540-560).
 template <bool BORDER>
-__device__ __forceinline__ int filter_px(const int16_t* c, int xv, const int16_t* toff, int dir, int pri, int sec,
-                                         int padj, int sadj, int pt0, int pt1) {
-    int sum = 0, mx = xv, mn = xv;
-    const int d2a = (dir + 2) & 7, d2b = (dir + 6) & 7;
+__device__ __forceinline__ void tap2(const int16_t* c, int o, int xv, int w, int thr, int adj, int& sum, int& mn,
+                                     int& mx) {
 #pragma unroll
-    for (int k = 0; k < 2; k++) {
-        const int op = toff[dir * 2 + k], oa = toff[d2a * 2 + k], ob = toff[d2b * 2 + k];
-        const int v[6] = {c[op], c[-op], c[oa], c[-oa], c[ob], c[-ob]};
-#pragma unroll
-        for (int t = 0; t < 6; t++) {
-            int x = v[t];
-            if (BORDER && x == NA) continue;
-            if (t < 2) sum += (k ? pt1 : pt0) * constrain_adj(x - xv, pri, padj);
-            else sum += (k ? 1 : 2) * constrain_adj(x - xv, sec, sadj);
-            mx = max(mx, x);
-            mn = min(mn, x);
-        }
+    for (int s = 0; s < 2; s++) {
+        const int x = s ? c[-o] : c[o];
+        if (BORDER && x == NA) continue;
+        sum += w * constrain_adj(x - xv, thr, adj);
+        mx = max(mx, x);
+        mn = min(mn, x);
     }
+}
+
+template <bool BORDER>
+__device__ __forceinline__ int filter_px(const int16_t* c, int xv, const Taps& T, int pri, int sec, int padj,
+                                         int sadj, int pt0, int pt1) {
+    int sum = 0, mx = xv, mn = xv;
+    tap2<BORDER>(c, T.p0, xv, pt0, pri, padj, sum, mn, mx);
+    tap2<BORDER>(c, T.p1, xv, pt1, pri, padj, sum, mn, mx);
+    tap2<BORDER>(c, T.a0, xv, 2, sec, sadj, sum, mn, mx);
+    tap2<BORDER>(c, T.b0, xv, 2, sec, sadj, sum, mn, mx);
+    tap2<BORDER>(c, T.a1, xv, 1, sec, sadj, sum, mn, mx);
+    tap2<BORDER>(c, T.b1, xv, 1, sec, sadj, sum, mn, mx);
     return clip3(mn, mx, xv + ((8 + sum - (sum < 0)) >> 4));
 }
 
@@ -110,6 +139,10 @@ __global__ void __launch_bounds__(256, 3) cdef_kernel(const FrameDev* __restrict
                                                       const int32_t* __restrict__ starts, int n, int total) {
     __shared__ int16_t win[3][WMAX * WP];
     __shared__ BlockParams bp[64];
+    __shared__ int costs[64][8];
+    // luma of the 64 8x8 blocks, block-major with a 136-byte block stride so
+    // that 32 lanes reading 8 bytes each from 32 blocks hit distinct banks
+    __shared__ __align__(16) int16_t blkx[64][68];
     __shared__ int16_t toff[16];
     if (threadIdx.x < 16) toff[threadIdx.x] = c_cdef_dirs[threadIdx.x >> 1][threadIdx.x & 1][0] * WP +
                                               c_cdef_dirs[threadIdx.x >> 1][threadIdx.x & 1][1];
@@ -134,64 +167,111 @@ __global__ void __launch_bounds__(256, 3) cdef_kernel(const FrameDev* __restrict
             int x0 = lx0 >> px, y0 = ly0 >> py;
             const PlaneDev& S = F.deb[p];
             int ww = bw + 2 * H2, wh = bh + 2 * H2;
-            for (int i = threadIdx.x; i < WMAX * wh; i += blockDim.x) {
-                int r = i / WMAX, c = i - r * WMAX;
-                if (c >= ww) continue;
-                int gy = y0 - H2 + r, gx = x0 - H2 + c;
-                win[p][r * WP + c] = (gy >= 0 && gy < S.h && gx >= 0 && gx < S.w) ? (int16_t)ld_px(S, hbd, gy, gx) : NA;
+            if (x0 >= 4 && y0 >= H2 && x0 + bw + 4 <= S.w && y0 + bh + H2 <= S.h) {
+                // interior: aligned 4-sample loads over [x0 - 4, x0 + bw + 4),
+                // every one inside the plane
+                const int ng = (bw + 8) >> 2;
+                const unsigned mag = (1u << 16) / ng + 1;  // i / ng for i < 4096
+                int16_t* wrow = win[p];
+                for (int i = threadIdx.x; i < wh * ng; i += blockDim.x) {
+                    int r = (int)(((unsigned)i * mag) >> 16), g = i - r * ng;
+                    const uint8_t* row = S.p + (size_t)(y0 - H2 + r) * S.stride;
+                    int v[4];
+                    if (hbd) {
+                        uint2 q = *reinterpret_cast<const uint2*>(row + 2 * (x0 - 4 + 4 * g));
+                        v[0] = q.x & 0xffff;
+                        v[1] = q.x >> 16;
+                        v[2] = q.y & 0xffff;
+                        v[3] = q.y >> 16;
+                    } else {
+                        uint32_t q = *reinterpret_cast<const uint32_t*>(row + x0 - 4 + 4 * g);
+                        v[0] = q & 0xff;
+                        v[1] = (q >> 8) & 0xff;
+                        v[2] = (q >> 16) & 0xff;
+                        v[3] = q >> 24;
+                    }
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        int c = 4 * g + e - 2;
+                        if (c >= 0 && c < ww) wrow[r * WP + c] = (int16_t)v[e];
+                    }
+                }
+            } else {
+                for (int i = threadIdx.x; i < WMAX * wh; i += blockDim.x) {
+                    int r = i / WMAX, c = i - r * WMAX;
+                    if (c >= ww) continue;
+                    int gy = y0 - H2 + r, gx = x0 - H2 + c;
+                    win[p][r * WP + c] =
+                        (gy >= 0 && gy < S.h && gx >= 0 && gx < S.w) ? (int16_t)ld_px(S, hbd, gy, gx) : NA;
+                }
             }
         }
         __syncthreads();
-        // direction search: 8 lanes per block, 32 blocks per pass
-        for (int b0 = 0; b0 < 64; b0 += 32) {
-            int blk = b0 + (threadIdx.x >> 3), d = threadIdx.x & 7;
-            int bi = blk >> 3, bj = blk & 7;
-            int r = fbr * 16 + bi * 2, c = fbc * 16 + bj * 2;
+        // block-major centred luma for the direction search (only blocks
+        // inside the mi grid are searched, and those lie inside the plane)
+        for (int k = threadIdx.x; k < 64 * 64; k += blockDim.x) {
+            int b = k >> 6, e = k & 63;
+            int r = ((b >> 3) << 3) + (e >> 3), c = ((b & 7) << 3) + (e & 7);
+            blkx[b][e] = (int16_t)((win[0][(r + H2) * WP + c + H2] >> cs) - 128);
+        }
+        __syncthreads();
+        // direction search: each warp computes one direction for 32 blocks
+        // (warp-uniform direction, no divergence); costs go to shared memory
+        // and one thread per block takes the arg-max
+        for (int q = threadIdx.x; q < 64 * 8; q += blockDim.x) {
+            const int d = (q >> 5) & 7, blk = (q >> 8) * 32 + (q & 31);
+            const int bi = blk >> 3, bj = blk & 7;
+            const int r = fbr * 16 + bi * 2, c = fbc * 16 + bj * 2;
             bool live = idx >= 0 && r < h.mi_rows && c < h.mi_cols;
-            bool skip = true;
             if (live) {
                 const uint8_t* sk = F.g.skip;
                 int mc = h.mi_cols;
-                skip = sk[r * mc + c] && (r + 1 >= h.mi_rows || sk[(r + 1) * mc + c]) &&
-                       (c + 1 >= mc || sk[r * mc + c + 1]) &&
-                       (r + 1 >= h.mi_rows || c + 1 >= mc || sk[(r + 1) * mc + c + 1]);
+                bool skip = sk[r * mc + c] && (r + 1 >= h.mi_rows || sk[(r + 1) * mc + c]) &&
+                            (c + 1 >= mc || sk[r * mc + c + 1]) &&
+                            (r + 1 >= h.mi_rows || c + 1 >= mc || sk[(r + 1) * mc + c + 1]);
+                live = !skip;
             }
-            int cost = 0;
-            if (live && !skip) {
-                const int16_t* w = &win[0][(H2 + bi * 8) * WP + H2 + bj * 8];
+            int cost = -1;  // marks a block that is not filtered
+            if (live) {
+                const int16_t* w = blkx[blk];
                 switch (d) {
-                    case 0: cost = dir_cost<0>(w, cs); break;
-                    case 1: cost = dir_cost<1>(w, cs); break;
-                    case 2: cost = dir_cost<2>(w, cs); break;
-                    case 3: cost = dir_cost<3>(w, cs); break;
-                    case 4: cost = dir_cost<4>(w, cs); break;
-                    case 5: cost = dir_cost<5>(w, cs); break;
-                    case 6: cost = dir_cost<6>(w, cs); break;
-                    default: cost = dir_cost<7>(w, cs); break;
+                    case 0: cost = dir_cost<0>(w); break;
+                    case 1: cost = dir_cost<1>(w); break;
+                    case 2: cost = dir_cost<2>(w); break;
+                    case 3: cost = dir_cost<3>(w); break;
+                    case 4: cost = dir_cost<4>(w); break;
+                    case 5: cost = dir_cost<5>(w); break;
+                    case 6: cost = dir_cost<6>(w); break;
+                    default: cost = dir_cost<7>(w); break;
                 }
             }
-            int best = cost, bd = d;
+            costs[blk][d] = cost;
+        }
+        __syncthreads();
+        if (threadIdx.x < 64) {
+            const int blk = threadIdx.x;
+            BlockParams b{0, 0, 0, 0, 0};
+            if (costs[blk][0] >= 0) {
+                // first strictly greater wins (cdef.rs:440-456)
+                int best = costs[blk][0], bd = 0;
 #pragma unroll
-            for (int o = 1; o < 8; o <<= 1) {
-                int oc = __shfl_xor_sync(0xffffffff, best, o, 8);
-                int od = __shfl_xor_sync(0xffffffff, bd, o, 8);
-                if (oc > best || (oc == best && od < bd)) { best = oc; bd = od; }
+                for (int d = 1; d < 8; d++)
+                    if (costs[blk][d] > best) {
+                        best = costs[blk][d];
+                        bd = d;
+                    }
+                int opp = costs[blk][(bd + 4) & 7];
+                int var = (best - opp) >> 10;
+                int pri_y = h.cdef_y_pri[idx] << cs;
+                int vs = (var >> 6) > 0 ? min(floor_log2u((unsigned)(var >> 6)), 12) : 0;
+                b.active = 1;
+                b.pri_y = var != 0 ? (pri_y * (4 + vs) + 8) >> 4 : 0;
+                b.padj_y = (int8_t)(b.pri_y ? max(h.cdef_damping + cs - floor_log2u((unsigned)b.pri_y), 0) : 0);
+                b.ydir = (int8_t)(pri_y == 0 ? 0 : bd);
+                int pri_uv = h.cdef_uv_pri[idx] << cs;
+                b.uvdir = (int8_t)(pri_uv == 0 ? 0 : c_uv_dir[ssx][ssy][bd]);
             }
-            int opp = __shfl_sync(0xffffffff, cost, (threadIdx.x & ~7) | ((bd + 4) & 7), 32);
-            if (d == 0) {
-                BlockParams b{0, 0, 0, 0, 0};
-                if (live && !skip) {
-                    int var = (best - opp) >> 10;
-                    int pri_y = h.cdef_y_pri[idx] << cs;
-                    int vs = (var >> 6) > 0 ? min(floor_log2u((unsigned)(var >> 6)), 12) : 0;
-                    b.active = 1;
-                    b.pri_y = var != 0 ? (pri_y * (4 + vs) + 8) >> 4 : 0;
-                    b.ydir = (int8_t)(pri_y == 0 ? 0 : bd);
-                    int pri_uv = h.cdef_uv_pri[idx] << cs;
-                    b.uvdir = (int8_t)(pri_uv == 0 ? 0 : c_uv_dir[ssx][ssy][bd]);
-                }
-                bp[blk] = b;
-            }
+            bp[blk] = b;
         }
         __syncthreads();
         const int sec_y = idx >= 0 ? h.cdef_y_sec[idx] << cs : 0;
@@ -207,24 +287,33 @@ __global__ void __launch_bounds__(256, 3) cdef_kernel(const FrameDev* __restrict
             const int damping = h.cdef_damping + cs - (p ? 1 : 0);
             const int sadj = (p ? sec_uv : sec_y) ? max(damping - floor_log2u((unsigned)(p ? sec_uv : sec_y)), 0) : 0;
             const int sec = p ? sec_uv : sec_y;
+            const int padj_uv = pri_uv ? max(damping - floor_log2u((unsigned)pri_uv), 0) : 0;
             const int lbw = 6 - px;  // log2 of the block width in this plane
-            for (int i = threadIdx.x; i < bw * bh; i += blockDim.x) {
-                int r = i >> lbw, c = i & (bw - 1);
+            // two horizontally adjacent samples per thread: same 8x8 block,
+            // so one parameter and tap-offset fetch serves both
+            for (int i = threadIdx.x; i < (bw * bh) >> 1; i += blockDim.x) {
+                int r = (2 * i) >> lbw, c = (2 * i) & (bw - 1);
                 int gy = y0 + r, gx = x0 + c;
                 if (gy >= dh || gx >= dw) continue;
                 const int16_t* cp = W + (r + H2) * WP + c + H2;
-                int xv = *cp;
+                int xv0 = cp[0], xv1 = cp[1];
                 const BlockParams b = bp[(r >> (3 - py)) * 8 + (c >> (3 - px))];
-                int out = xv;
+                int out0 = xv0, out1 = xv1;
                 if (b.active) {
-                    int pri = p ? pri_uv : b.pri_y;
-                    int dir = p ? b.uvdir : b.ydir;
-                    int prow = (pri >> cs) & 1;
-                    int padj = pri ? max(damping - floor_log2u((unsigned)pri), 0) : 0;
-                    out = border ? filter_px<true>(cp, xv, toff, dir, pri, sec, padj, sadj, prow ? 3 : 4, prow ? 3 : 2)
-                                 : filter_px<false>(cp, xv, toff, dir, pri, sec, padj, sadj, prow ? 3 : 4, prow ? 3 : 2);
+                    const int pri = p ? pri_uv : b.pri_y;
+                    const int padj = p ? padj_uv : b.padj_y;
+                    const Taps T = taps_of(toff, p ? b.uvdir : b.ydir);
+                    const int prow = (pri >> cs) & 1, pt0 = prow ? 3 : 4, pt1 = prow ? 3 : 2;
+                    if (border) {
+                        out0 = filter_px<true>(cp, xv0, T, pri, sec, padj, sadj, pt0, pt1);
+                        out1 = filter_px<true>(cp + 1, xv1, T, pri, sec, padj, sadj, pt0, pt1);
+                    } else {
+                        out0 = filter_px<false>(cp, xv0, T, pri, sec, padj, sadj, pt0, pt1);
+                        out1 = filter_px<false>(cp + 1, xv1, T, pri, sec, padj, sadj, pt0, pt1);
+                    }
                 }
-                st_px(D, hbd, gy, gx, out);
+                st_px(D, hbd, gy, gx, out0);
+                if (gx + 1 < dw) st_px(D, hbd, gy, gx + 1, out1);
             }
         }
     }
