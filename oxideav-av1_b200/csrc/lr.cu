@@ -77,7 +77,9 @@ __device__ __forceinline__ int count_units(int us, int sz) {
 
 // Box sums, a/b coefficients (box_filter, loop_restoration.rs:594-700) for
 // radius r over the A/B grid rows i in [-1, th] (stored at i + 1), columns
-// j in [-1, tw].  odd_only: only rows whose plane row is odd.
+// j in [-1, tw].  odd_only: only rows whose plane row is odd.  Column sums
+// slide down the rows and row sums slide along the columns, so each sum
+// costs two loads instead of 2r + 1.
 __device__ void box_coeffs(Smem& s, int th, int tw, int bd, int r, int eps, bool odd_only, int y0) {
     const int n = (2 * r + 1) * (2 * r + 1);
     const long long n2e = (long long)n * n * eps;
@@ -85,71 +87,126 @@ __device__ void box_coeffs(Smem& s, int th, int tw, int bd, int r, int eps, bool
     const int one_over_n = ((1 << 12) + n / 2) / n;
     const int sa = 2 * (bd - 8), sb = bd - 8;
     const int vw = tw + 2 * H3;
-    // column sums over the 2r+1 rows centred on each needed A/B row
-    for (int k = threadIdx.x; k < (th + 2) * VW; k += blockDim.x) {
-        int row = k / VW, jj = k - row * VW, i = row - 1;
-        if (jj >= vw || (odd_only && !((y0 + i) & 1))) continue;
-        const uint16_t* c = s.src + (i + H3 - r) * SP + jj;
+    const int rows = th + 2;
+    // column sums: one thread per (column, run of 8 grid rows)
+    constexpr int RUN = 8;
+    const int runs = (rows + RUN - 1) / RUN;
+    for (int k = threadIdx.x; k < runs * VW; k += blockDim.x) {
+        const int ru = k / VW, jj = k - ru * VW;
+        if (jj >= vw) continue;
+        const int ra = ru * RUN, rb = min(rows, ra + RUN);
+        const uint16_t* c = s.src + jj;
+        int top = ra - 1 + H3 - r;  // first source row of grid row ra's window
         int s1 = 0, s2 = 0;
         for (int d = 0; d <= 2 * r; d++) {
-            int v = c[d * SP];
+            int v = c[(top + d) * SP];
             s1 += v;
             s2 += v * v;
         }
-        s.v1[(i + 1) * VW + jj] = s1;
-        s.v2[(i + 1) * VW + jj] = s2;
+        for (int row = ra;; row++) {
+            if (!odd_only || ((y0 + row - 1) & 1)) {
+                s.v1[row * VW + jj] = s1;
+                s.v2[row * VW + jj] = s2;
+            }
+            if (row + 1 >= rb) break;
+            const int vo = c[top * SP], vn = c[(top + 2 * r + 1) * SP];
+            s1 += vn - vo;
+            s2 += vn * vn - vo * vo;
+            top++;
+        }
     }
     __syncthreads();
-    constexpr int GW = TW + 2;
-    for (int k = threadIdx.x; k < (th + 2) * GW; k += blockDim.x) {
-        int row = k / GW, col = k - row * GW, i = row - 1, j = col - 1;
-        if (col >= tw + 2 || (odd_only && !((y0 + i) & 1))) continue;
-        const int* c1 = s.v1 + (i + 1) * VW + (j + H3 - r);
-        const int* c2 = s.v2 + (i + 1) * VW + (j + H3 - r);
+    // row sums and coefficients: one thread per (grid row, run of 8 columns)
+    constexpr int SEGS = (TW + 2 + RUN - 1) / RUN;
+    for (int k = threadIdx.x; k < rows * SEGS; k += blockDim.x) {
+        const int row = k / SEGS, sg = k - row * SEGS;
+        if (odd_only && !((y0 + row - 1) & 1)) continue;
+        const int ja = sg * RUN - 1, jb = min(tw + 1, ja + RUN);  // j in [ja, jb)
+        if (ja >= jb) continue;
+        const int* c1 = s.v1 + row * VW;
+        const int* c2 = s.v2 + row * VW;
+        int left = ja + H3 - r;
         int b = 0, a = 0;
         for (int d = 0; d <= 2 * r; d++) {
-            b += c1[d];
-            a += c2[d];
+            b += c1[left + d];
+            a += c2[left + d];
         }
-        int ar = sa ? (a + (1 << (sa - 1))) >> sa : a;
-        int dr = sb ? (b + (1 << (sb - 1))) >> sb : b;
-        int p = ar * n - dr * dr;
-        if (p < 0) p = 0;
-        unsigned z = (unsigned)(((unsigned long long)(unsigned)p * sm + (1u << 19)) >> 20);
-        int a2 = z >= 255 ? 256 : s.a2lut[z];
-        // b2 uses the raw box sum b, as the reference does (loop_restoration.rs:660-661)
-        long long b2 = (long long)((256 - a2) * b) * one_over_n;
-        s.A[(i + 1) * AP + j + 1] = (uint16_t)a2;
-        s.B[(i + 1) * AP + j + 1] = (int)((b2 + (1 << 11)) >> 12);
+        for (int j = ja;; j++) {
+            int ar = sa ? (a + (1 << (sa - 1))) >> sa : a;
+            int dr = sb ? (b + (1 << (sb - 1))) >> sb : b;
+            int p = ar * n - dr * dr;
+            if (p < 0) p = 0;
+            unsigned z = (unsigned)(((unsigned long long)(unsigned)p * sm + (1u << 19)) >> 20);
+            int a2 = z >= 255 ? 256 : s.a2lut[z];
+            // b2 uses the raw box sum b, as the reference does (loop_restoration.rs:660-661)
+            long long b2 = (long long)((256 - a2) * b) * one_over_n;
+            s.A[row * AP + j + 1] = (uint16_t)a2;
+            s.B[row * AP + j + 1] = (int)((b2 + (1 << 11)) >> 12);
+            if (j + 1 >= jb) break;
+            b += c1[left + 2 * r + 1] - c1[left];
+            a += c2[left + 2 * r + 1] - c2[left];
+            left++;
+        }
     }
     __syncthreads();
 }
 
-// 3x3 weighting of A/B at output (i, j) (loop_restoration.rs:700-736).
-__device__ __forceinline__ int box_weight(const Smem& s, int i, int j, int u, int pass, int y0) {
-    int as, bs, shift;
-    const uint16_t* a = s.A + i * AP + j;  // top-left of the 3x3 window
-    const int* b = s.B + i * AP + j;
+// 3x3 weighting of A/B (loop_restoration.rs:700-736) for the four outputs
+// (i, j0 .. j0 + 3), reading each A/B column once.
+__device__ __forceinline__ void box_weight4(const Smem& s, int i, int j0, const int u[4], int pass, int y0,
+                                            int out[4]) {
+    const uint16_t* a = s.A + i * AP + j0;  // top-left of the first 3x3 window
+    const int* b = s.B + i * AP + j0;
+    int ac[3][6], bc[3][6];
+    int shift;
     if (pass == 0) {
-        if ((y0 + i) & 1) {  // odd output row: centre row only, weights 5 6 5
-            as = 5 * (a[AP] + a[AP + 2]) + 6 * a[AP + 1];
-            bs = 5 * (b[AP] + b[AP + 2]) + 6 * b[AP + 1];
-            shift = 4;
-        } else {             // even output row: rows above and below
-            as = 5 * (a[0] + a[2] + a[2 * AP] + a[2 * AP + 2]) + 6 * (a[1] + a[2 * AP + 1]);
-            bs = 5 * (b[0] + b[2] + b[2 * AP] + b[2 * AP + 2]) + 6 * (b[1] + b[2 * AP + 1]);
-            shift = 5;
+        const bool odd = (y0 + i) & 1;
+        shift = odd ? 4 : 5;
+        if (odd) {  // centre row only, weights 5 6 5
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                ac[1][c] = a[AP + c];
+                bc[1][c] = b[AP + c];
+            }
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                int as = 5 * (ac[1][e] + ac[1][e + 2]) + 6 * ac[1][e + 1];
+                int bs = 5 * (bc[1][e] + bc[1][e + 2]) + 6 * bc[1][e + 1];
+                int v = as * u[e] + bs, sh = 8 + shift - 4;
+                out[e] = (v + (1 << (sh - 1))) >> sh;
+            }
+        } else {    // rows above and below
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                ac[0][c] = a[c] + a[2 * AP + c];
+                bc[0][c] = b[c] + b[2 * AP + c];
+            }
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                int as = 5 * (ac[0][e] + ac[0][e + 2]) + 6 * ac[0][e + 1];
+                int bs = 5 * (bc[0][e] + bc[0][e + 2]) + 6 * bc[0][e + 1];
+                int v = as * u[e] + bs, sh = 8 + shift - 4;
+                out[e] = (v + (1 << (sh - 1))) >> sh;
+            }
         }
-    } else {
-        int ca = a[1] + a[AP] + a[AP + 1] + a[AP + 2] + a[2 * AP + 1];
-        int cb = b[1] + b[AP] + b[AP + 1] + b[AP + 2] + b[2 * AP + 1];
-        as = 3 * (a[0] + a[2] + a[2 * AP] + a[2 * AP + 2]) + 4 * ca;
-        bs = 3 * (b[0] + b[2] + b[2 * AP] + b[2 * AP + 2]) + 4 * cb;
-        shift = 5;
+        return;
     }
-    int v = as * u + bs;
-    int sh = 8 + shift - 4;
-    return (v + (1 << (sh - 1))) >> sh;
+#pragma unroll
+    for (int rr = 0; rr < 3; rr++)
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            ac[rr][c] = a[rr * AP + c];
+            bc[rr][c] = b[rr * AP + c];
+        }
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        int ca = ac[0][e + 1] + ac[1][e] + ac[1][e + 1] + ac[1][e + 2] + ac[2][e + 1];
+        int cb = bc[0][e + 1] + bc[1][e] + bc[1][e + 1] + bc[1][e + 2] + bc[2][e + 1];
+        int as = 3 * (ac[0][e] + ac[0][e + 2] + ac[2][e] + ac[2][e + 2]) + 4 * ca;
+        int bs = 3 * (bc[0][e] + bc[0][e + 2] + bc[2][e] + bc[2][e + 2]) + 4 * cb;
+        int v = as * u[e] + bs, sh = 8 + 5 - 4;
+        out[e] = (v + (1 << (sh - 1))) >> sh;
+    }
 }
 
 __global__ void __launch_bounds__(256) lr_kernel(const FrameDev* __restrict__ frames,
@@ -210,15 +267,60 @@ __global__ void __launch_bounds__(256) lr_kernel(const FrameDev* __restrict__ fr
         }
         // source window: get_source_sample (loop_restoration.rs:862-883)
         const int sw = tw + 2 * H3;
-        for (int k = threadIdx.x; k < (th + 2 * H3) * SW; k += blockDim.x) {
-            int i = k / SW, j = k - i * SW;
-            if (j >= sw) continue;
-            int x = clip3(0, pw - 1, x0 - H3 + j), y = clip3(0, ph - 1, y0 - H3 + i);
-            int v;
-            if (y < sstart) v = ld_px(Dq, hbd, clip3(0, Dq.h - 1, max(y, sstart - 2)), min(x, Dq.w - 1));
-            else if (y > send) v = ld_px(Dq, hbd, clip3(0, Dq.h - 1, min(y, send + 2)), min(x, Dq.w - 1));
-            else v = ld_px(C, hbd, min(y, C.h - 1), min(x, C.w - 1));
-            s.src[i * SP + j] = (uint16_t)v;
+        if (x0 >= 4 && x0 + tw + 4 <= pw && !(x0 & 3) && !(tw & 3)) {
+            // columns [x0 - 4, x0 + tw + 4) lie inside the plane (and inside
+            // both source planes, which are at least pw wide): aligned
+            // 4-sample loads, the row routed once per load
+            const int ng = (tw + 8) >> 2;
+            const unsigned mag = (1u << 16) / ng + 1;  // k / ng for k < 38 * ng
+            for (int k = threadIdx.x; k < (th + 2 * H3) * ng; k += blockDim.x) {
+                const int i = (int)(((unsigned)k * mag) >> 16), g = k - i * ng;
+                const int y = clip3(0, ph - 1, y0 - H3 + i);
+                const PlaneDev* P;
+                int yy;
+                if (y < sstart) {
+                    P = &Dq;
+                    yy = clip3(0, Dq.h - 1, max(y, sstart - 2));
+                } else if (y > send) {
+                    P = &Dq;
+                    yy = clip3(0, Dq.h - 1, min(y, send + 2));
+                } else {
+                    P = &C;
+                    yy = min(y, C.h - 1);
+                }
+                const uint8_t* row = P->p + (size_t)yy * P->stride;
+                const int xs = x0 - 4 + 4 * g;
+                int v[4];
+                if (hbd) {
+                    uint2 q = *reinterpret_cast<const uint2*>(row + 2 * xs);
+                    v[0] = q.x & 0xffff;
+                    v[1] = q.x >> 16;
+                    v[2] = q.y & 0xffff;
+                    v[3] = q.y >> 16;
+                } else {
+                    uint32_t q = *reinterpret_cast<const uint32_t*>(row + xs);
+                    v[0] = q & 0xff;
+                    v[1] = (q >> 8) & 0xff;
+                    v[2] = (q >> 16) & 0xff;
+                    v[3] = q >> 24;
+                }
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const int j = 4 * g + e - 1;
+                    if (j >= 0 && j < sw) s.src[i * SP + j] = (uint16_t)v[e];
+                }
+            }
+        } else {
+            for (int k = threadIdx.x; k < (th + 2 * H3) * SW; k += blockDim.x) {
+                int i = k / SW, j = k - i * SW;
+                if (j >= sw) continue;
+                int x = clip3(0, pw - 1, x0 - H3 + j), y = clip3(0, ph - 1, y0 - H3 + i);
+                int v;
+                if (y < sstart) v = ld_px(Dq, hbd, clip3(0, Dq.h - 1, max(y, sstart - 2)), min(x, Dq.w - 1));
+                else if (y > send) v = ld_px(Dq, hbd, clip3(0, Dq.h - 1, min(y, send + 2)), min(x, Dq.w - 1));
+                else v = ld_px(C, hbd, min(y, C.h - 1), min(x, C.w - 1));
+                s.src[i * SP + j] = (uint16_t)v;
+            }
         }
         __syncthreads();
         const int maxv = (1 << bd) - 1;
@@ -259,25 +361,38 @@ __global__ void __launch_bounds__(256) lr_kernel(const FrameDev* __restrict__ fr
         const int r0 = c_sgr_params[set][0], e0 = c_sgr_params[set][1];
         const int r1 = c_sgr_params[set][2], e1 = c_sgr_params[set][3];
         const int w0 = u.sgr_xqd[0], w1 = u.sgr_xqd[1], w2 = 128 - w0 - w1;
+        // outputs in runs of four along a row
+        constexpr int Q = TW / 4;
         if (r0) {
             box_coeffs(s, th, tw, bd, r0, e0, true, y0);
-            for (int k = threadIdx.x; k < th * TW; k += blockDim.x) {
-                int i = k >> 6, j = k & (TW - 1);
-                if (j >= tw) continue;
-                s.F0[k] = box_weight(s, i, j, s.src[(i + H3) * SP + j + H3], 0, y0);
+            for (int k = threadIdx.x; k < th * Q; k += blockDim.x) {
+                int i = k / Q, j0 = (k - i * Q) * 4;
+                if (j0 >= tw) continue;
+                int u[4], f[4];
+#pragma unroll
+                for (int e = 0; e < 4; e++) u[e] = s.src[(i + H3) * SP + j0 + e + H3];
+                box_weight4(s, i, j0, u, 0, y0, f);
+#pragma unroll
+                for (int e = 0; e < 4; e++) s.F0[i * TW + j0 + e] = f[e];
             }
             __syncthreads();
         }
         if (r1) box_coeffs(s, th, tw, bd, r1, e1, false, y0);
-        for (int k = threadIdx.x; k < th * TW; k += blockDim.x) {
-            int i = k >> 6, j = k & (TW - 1);
-            if (j >= tw) continue;
-            int cu = s.src[(i + H3) * SP + j + H3];
-            int uu = cu << 4;
-            int f0 = r0 ? s.F0[k] : uu;
-            int f1 = r1 ? box_weight(s, i, j, cu, 1, y0) : uu;
-            int v = w1 * uu + w0 * f0 + w2 * f1;
-            st_px(O, hbd, y0 + i, x0 + j, clip3(0, maxv, (v + (1 << 10)) >> 11));
+        for (int k = threadIdx.x; k < th * Q; k += blockDim.x) {
+            int i = k / Q, j0 = (k - i * Q) * 4;
+            if (j0 >= tw) continue;
+            int u[4], f1[4];
+#pragma unroll
+            for (int e = 0; e < 4; e++) u[e] = s.src[(i + H3) * SP + j0 + e + H3];
+            if (r1) box_weight4(s, i, j0, u, 1, y0, f1);
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                if (j0 + e >= tw) break;
+                int uu = u[e] << 4;
+                int f0 = r0 ? s.F0[i * TW + j0 + e] : uu;
+                int v = w1 * uu + w0 * f0 + w2 * (r1 ? f1[e] : uu);
+                st_px(O, hbd, y0 + i, x0 + j0 + e, clip3(0, maxv, (v + (1 << 10)) >> 11));
+            }
         }
     }
 }
