@@ -284,10 +284,13 @@ __global__ void __launch_bounds__(256) deblock_kernel(const FrameDev* __restrict
             eh[i] = decode_code(code >> 8, sharp);
         }
         __syncthreads();
-        // vertical pass: window rows x edge columns 8..88
-        constexpr int VE = CELLS - 3;  // cells 2..22
-        for (int i = threadIdx.x; i < WIN * VE; i += blockDim.x) {
-            int r = i % WIN, cc = 2 + i / WIN;
+        // vertical pass: window rows x edge columns 12..84 (cells 3..21: a
+        // filter moves at most 6 samples from its edge, so only those edges
+        // move tile columns; all window rows keep each warp's rows aligned to
+        // the 4-row cells)
+        constexpr int VR = WIN, VE = CELLS - 5;
+        for (int i = threadIdx.x; i < VR * VE; i += blockDim.x) {
+            int r = i % VR, cc = 3 + i / VR;
             uint32_t prm = ev[(r >> 2) * CELLS + cc];
             if (prm & 0xff) filter_line(&win[r * PITCH + cc * 4], 1, prm, plane, bd);
         }
@@ -300,10 +303,24 @@ __global__ void __launch_bounds__(256) deblock_kernel(const FrameDev* __restrict
             if (prm & 0xff) filter_line(&win[cr * 4 * PITCH + c], PITCH, prm, plane, bd);
         }
         __syncthreads();
-        for (int i = threadIdx.x; i < TILE * TILE; i += blockDim.x) {
-            int r = i / TILE, c = i % TILE;
+        // write the tile, four samples per thread (one vector store inside the plane)
+        const int dh = min(D.h, S.h), dw = min(D.w, S.w);
+        for (int i = threadIdx.x; i < TILE * (TILE / 4); i += blockDim.x) {
+            int r = i / (TILE / 4), c = (i % (TILE / 4)) * 4;
             int gy = ty * TILE + r, gx = tx * TILE + c;
-            if (gy < min(D.h, S.h) && gx < min(D.w, S.w)) st_px(D, hbd, gy, gx, win[(r + HALO) * PITCH + c + HALO]);
+            if (gy >= dh) continue;
+            const int* w = &win[(r + HALO) * PITCH + c + HALO];
+            uint8_t* row = D.p + (size_t)gy * D.stride;
+            if (gx + 3 < dw) {
+                if (hbd)
+                    *reinterpret_cast<uint2*>(row + 2 * gx) =
+                        make_uint2((uint32_t)w[0] | ((uint32_t)w[1] << 16), (uint32_t)w[2] | ((uint32_t)w[3] << 16));
+                else
+                    *reinterpret_cast<uint32_t*>(row + gx) =
+                        (uint32_t)w[0] | ((uint32_t)w[1] << 8) | ((uint32_t)w[2] << 16) | ((uint32_t)w[3] << 24);
+            } else {
+                for (int k = 0; k < 4 && gx + k < dw; k++) st_px(D, hbd, gy, gx + k, w[k]);
+            }
         }
     }
 }
