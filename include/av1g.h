@@ -294,7 +294,14 @@ av1g_status av1g_run_recon(const av1g_recon_job* jobs, int32_t n, void* stream);
  * cdf.rs:19235): the TU-sized piece at (x, y) of a block predicted from the
  * pre-filter CurrFrame with the block's mv = {row, col} (1/8 luma samples);
  * list one piece per transform-sized part of the block, before its residual
- * TUs. */
+ * TUs.
+ * interintra != 0: the TU is a whole inter-intra block of one plane (tx_size
+ * = the block size, mode = the intra mode of interintra_mode: DC, V, H or
+ * SMOOTH): its intra prediction is blended with the inter prediction the
+ * inter pass left in the job's interintra_in plane (mask_blend_interintra,
+ * inter_pred.rs:3272), which is what predict_inter does with the intra
+ * prediction in CurrFrame; list the block's residual TUs after it (mode
+ * AV1G_INTRA_MODE_NONE). */
 typedef struct av1g_intra_tu {
     uint16_t x;
     uint16_t y;
@@ -315,6 +322,11 @@ typedef struct av1g_intra_tu {
     uint8_t palette_size;
     uint8_t pad2;
     uint16_t palette_colors[8];
+    uint8_t interintra;          /* 0, or the intra half of an inter-intra block:
+                                    1 smooth mask, 2 wedge mask */
+    uint8_t interintra_mode;     /* II_DC_PRED..II_SMOOTH_PRED (mask of kind 1) */
+    uint8_t wedge_index;         /* kind 2 (wedge_sign 0) */
+    uint8_t mi_size;             /* kind 2: the luma block size */
 } av1g_intra_tu;
 
 /* A frame's intra work, reconstructed in place on top of whatever the
@@ -330,6 +342,7 @@ typedef struct av1g_intra_job {
     av1g_plane planes[3];            /* device, updated in place */
     const uint8_t* palette_maps;     /* host: colour-index pool of palette TUs */
     int64_t palette_map_bytes;
+    av1g_plane interintra_in[3];     /* device: inter halves of inter-intra blocks */
 } av1g_intra_job;
 
 /* §7.11.2 intra prediction (DC, V, H, directional with edge filter and
@@ -401,7 +414,11 @@ typedef struct av1g_obmc_neighbour {
  * wedge uses wedge_sign 0.  A DIFFWTD chroma call reads the mask its block's
  * plane-0 call computed (the mask of the luma samples at (x << ss, y << ss)),
  * so list the plane-0 call of each DIFFWTD block too.  AV1G_INTER_INTRA
- * blends with the intra prediction the CurrFrame region holds on entry.
+ * blends with the intra prediction the CurrFrame region holds on entry — or,
+ * when the job's interintra_out plane of that plane is given, stores its
+ * clipped inter prediction Clip1(Round2(preds[0], InterPostRound)) there
+ * instead (CurrFrame untouched) for av1g_run_intra to blend once the intra
+ * half exists (no OBMC on such calls).
  * warp: index into the job's warps (-1: no warp context).  motion_mode 1
  * (OBMC) uses obmc_above + obmc_left neighbours from obmc_first (above ones
  * first) with the ObmcParams fields below (inter_pred.rs:1438-1450).
@@ -454,6 +471,7 @@ typedef struct av1g_inter_job {
     const av1g_warp_ctx* warps;             /* host */
     int32_t num_warps;
     av1g_plane planes[3];                   /* CurrFrame, device, written */
+    av1g_plane interintra_out[3];           /* device or NULL, see below */
 } av1g_inter_job;
 
 /* WarpSampleCand (src/inter_pred.rs:4030): one §7.10.4 warp sample. */

@@ -225,9 +225,11 @@ def intra_rc(frame):
     tus = np.ascontiguousarray(frame.tus)
     coeffs = np.ascontiguousarray(frame.coeffs, dtype=np.int32)
     maps = np.ascontiguousarray(getattr(frame, "palette_maps", np.zeros(1, np.uint8)), dtype=np.uint8)
+    side = getattr(frame, "interintra_side", None)
+    side = None if side is None else [None if a is None else np.ascontiguousarray(a, dtype=np.int32) for a in side]
     rc = lib.ora_intra_frame(C.byref(frame.hdr), C.byref(frame.quant), tus.ctypes.data_as(C.c_void_p), len(tus),
                              _ptr(coeffs), _planes(planes), maps.ctypes.data_as(C.c_void_p),
-                             C.c_int64(len(getattr(frame, "palette_maps", []))))
+                             C.c_int64(len(getattr(frame, "palette_maps", []))), _side_planes(side))
     return planes, rc
 
 
@@ -252,8 +254,21 @@ def _struct_ptr(a):
     return a.ctypes.data_as(C.c_void_p) if len(a) else None
 
 
-def inter(frame):
+def _side_planes(side):
+    """OraPlane[3] over int32 arrays (None entries: no side plane), or None."""
+    if side is None:
+        return None
+    arr = (OraPlane * 3)()
+    for p, a in enumerate(side):
+        if a is not None:
+            arr[p] = OraPlane(_ptr(a), a.shape[0], a.shape[1])
+    return arr
+
+
+def inter(frame, side=None):
     """Every inter prediction call in list order on int32 copies of the planes.
+    side: None, or a list of int32 arrays (CurrFrame shape) that receive the
+    inter halves of inter-intra calls instead of the blend.
 
     Returns (planes, rc): rc is 0, or 1 + the index of the first call the
     reference rejects."""
@@ -274,7 +289,8 @@ def inter(frame):
     nb = np.ascontiguousarray(frame.neighbours)
     warps = np.ascontiguousarray(frame.warps)
     rc = lib.ora_inter_frame(C.byref(frame.hdr), refs, ref_planes, _struct_ptr(preds), len(preds),
-                             _struct_ptr(nb), len(nb), _struct_ptr(warps), len(warps), _planes(planes))
+                             _struct_ptr(nb), len(nb), _struct_ptr(warps), len(warps), _planes(planes),
+                             _side_planes(side))
     return planes, rc
 
 
@@ -342,6 +358,11 @@ def decode_stream(frames):
         h = fr.hdr
         ph = lambda p: ((h.mi_rows * 4) >> (h.subsampling_y if p else 0), (h.mi_cols * 4) >> (h.subsampling_x if p else 0))
         planes = [np.zeros(ph(p), np.int32) for p in range(h.num_planes)]
+        side = None
+        if fr.preds is not None and (fr.preds["kind"] == 2).any():
+            # inter halves of inter-intra blocks wait for their intra halves
+            # (the reference's per-block order; see tests/test_oracle_interintra_split.py)
+            side = [np.zeros(ph(p), np.int32) for p in range(h.num_planes)]
         if fr.preds is not None and len(fr.preds):
             o = _Obj()
             o.hdr, o.preds, o.neighbours, o.warps, o.planes = h, fr.preds, fr.neighbours, fr.warps, planes
@@ -350,7 +371,7 @@ def decode_stream(frames):
                 sl = slots[fr.ref_frame_idx[r]]
                 pls = list(sl["planes"]) + [np.zeros((1, 1), np.int32)] * (3 - len(sl["planes"]))
                 o.refs.append({"planes": pls, "upscaled_width": sl["uw"], "frame_height": sl["fh"]})
-            planes, rc = inter(o)
+            planes, rc = inter(o, side=side)
             if rc:
                 raise RuntimeError(f"oracle rejected inter call {rc - 1}")
         if fr.inter_tus is not None and len(fr.inter_tus):
@@ -361,6 +382,7 @@ def decode_stream(frames):
             o = _Obj()
             o.hdr, o.quant, o.tus, o.coeffs, o.planes = h, fr.quant, fr.intra_tus, fr.coeffs, planes
             o.palette_maps = fr.palette_maps if fr.palette_maps is not None else np.zeros(0, np.uint8)
+            o.interintra_side = side
             planes = intra(o)
         sf = synth.SyntheticFrame()
         sf.hdr, sf.grid, sf.cdef_idx, sf.lr_units, sf.recon = h, fr.grid, fr.cdef_idx, fr.lr_units, planes

@@ -417,7 +417,7 @@ static int obmc_axis(const ctx_t* c, const av1g_inter_pred* d, int left, const a
 /* predict_inter, inter_pred.rs:2100, for one call; out holds the CurrFrame
  * region on entry (read by the inter-intra blend) and the prediction on
  * return. */
-static int predict_inter(const ctx_t* c, const av1g_inter_pred* d, uint16_t* out) {
+static int predict_inter(const ctx_t* c, const av1g_inter_pred* d, uint16_t* out, uint16_t* side_out) {
     const av1g_frame_header* hdr = c->hdr;
     int plane = d->plane, w = d->w, h = d->h, bd = hdr->bit_depth;
     if (plane > 2 || (bd != 8 && bd != 10 && bd != 12)) return ERR;
@@ -478,6 +478,12 @@ static int predict_inter(const ctx_t* c, const av1g_inter_pred* d, uint16_t* out
                     mask[i * w + j] = (uint8_t)m;
                 }
             mstride = w;
+        }
+        if (side_out) {
+            /* the blend's inter operand, kept for the intra half (no OBMC on such calls) */
+            if (d->motion_mode == 1) { rc = ERR; goto done; }
+            for (size_t i = 0; i < n; i++) side_out[i] = (uint16_t)clip3(0, maxv, (int32_t)rnd2(p0[i], post));
+            goto done;
         }
         for (int y = 0; y < h; y++)
             for (int x = 0; x < w; x++) {
@@ -562,7 +568,7 @@ done:
 
 int ora_inter_frame(const av1g_frame_header* hdr, const av1g_ref_frame* refs, const ora_plane* ref_planes,
                     const av1g_inter_pred* preds, int n, const av1g_obmc_neighbour* nb, int n_nb,
-                    const av1g_warp_ctx* warps, int n_warps, ora_plane planes[3]) {
+                    const av1g_warp_ctx* warps, int n_warps, ora_plane planes[3], ora_plane* side) {
     ctx_t c = {hdr, refs, ref_planes, nb, n_nb, warps, n_warps, NULL, 0, 0};
     c.dw_stride = planes[0].cols + 256;
     c.dw_rows = planes[0].rows + 256;
@@ -579,11 +585,17 @@ int ora_inter_frame(const av1g_frame_header* hdr, const av1g_ref_frame* refs, co
         uint16_t* out = (uint16_t*)calloc((size_t)w * h, sizeof(uint16_t));
         for (int i = 0; i < fh; i++)
             for (int j = 0; j < fw; j++) out[i * w + j] = (uint16_t)P->s[(size_t)(d->y + i) * P->cols + d->x + j];
-        if (predict_inter(&c, d, out)) rc = k + 1;
+        ora_plane* S = (side && d->kind == AV1G_INTER_INTRA && side[d->plane].s) ? &side[d->plane] : NULL;
+        uint16_t* so = S ? (uint16_t*)calloc((size_t)w * h, sizeof(uint16_t)) : NULL;
+        if (predict_inter(&c, d, out, so)) rc = k + 1;
         else
             for (int i = 0; i < fh; i++)
-                for (int j = 0; j < fw; j++) P->s[(size_t)(d->y + i) * P->cols + d->x + j] = out[i * w + j];
+                for (int j = 0; j < fw; j++) {
+                    if (S) S->s[(size_t)(d->y + i) * S->cols + d->x + j] = so[i * w + j];
+                    else P->s[(size_t)(d->y + i) * P->cols + d->x + j] = out[i * w + j];
+                }
         free(out);
+        free(so);
     }
     free(c.diffwtd);
     return rc;
@@ -700,4 +712,53 @@ int ora_warp_estimation(const av1g_warp_sample* cand, int n, int mi_row, int mi_
     params[0] = (int32_t)(vx < -tc ? -tc : (vx > tc - 1 ? tc - 1 : vx));
     params[1] = (int32_t)(vy < -tc ? -tc : (vy > tc - 1 ? tc - 1 : vy));
     return 1;
+}
+
+/* The intra half of an inter-intra block of one plane: intra (the block's
+ * intra prediction, w x h) blended with the stored inter half in side,
+ * written to out within the plane (mask_blend_interintra,
+ * inter_pred.rs:3272, with the masks of predict_inter's inter-intra arm,
+ * inter_pred.rs:2230-2290).  Returns 0 or ERR. */
+int ora_interintra_blend(const av1g_frame_header* hdr, const av1g_intra_tu* t, int w, int h, const uint16_t* intra,
+                         const ora_plane* side, ora_plane* out) {
+    int ssx = t->plane ? hdr->subsampling_x : 0, ssy = t->plane ? hdr->subsampling_y : 0;
+    int maxv = (1 << hdr->bit_depth) - 1;
+    uint8_t* mask = NULL;
+    int mstride, msx = 0, msy = 0;
+    if (t->interintra == 2) {
+        if (t->mi_size >= 22) return ERR;
+        int lw = N4W[t->mi_size] * 4, lh = N4H[t->mi_size] * 4;
+        mask = (uint8_t*)malloc((size_t)lw * lh);
+        if (wedge_mask(t->mi_size, t->wedge_index, 0, mask) || (ssx ? 2 * w : w) > lw ||
+            (size_t)lw * ((ssy ? 2 * h : h) - 1) + (ssx ? 2 * w : w) > (size_t)lw * lh) {
+            free(mask);
+            return ERR;
+        }
+        msx = ssx;
+        msy = ssy;
+        mstride = lw;
+    } else {
+        mask = (uint8_t*)malloc((size_t)w * h);
+        int scale = 128 / (w > h ? w : h);
+        for (int i = 0; i < h; i++)
+            for (int j = 0; j < w; j++) {
+                int m = 32;
+                if (t->interintra_mode == 1) m = II_W[i * scale];
+                else if (t->interintra_mode == 2) m = II_W[j * scale];
+                else if (t->interintra_mode == 3) m = II_W[(i < j ? i : j) * scale];
+                mask[i * w + j] = (uint8_t)m;
+            }
+        mstride = w;
+    }
+    for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++) {
+            int yy = t->y + y, xx = t->x + x;
+            if (yy >= out->rows || xx >= out->cols) continue;
+            int64_t m = mask_at(mask, mstride, msx, msy, y, x);
+            int64_t cl = side->s[(size_t)yy * side->cols + xx];
+            int32_t b = (int32_t)rnd2(m * intra[y * w + x] + (64 - m) * cl, 6);
+            out->s[(size_t)yy * out->cols + xx] = clip3(0, maxv, b);
+        }
+    free(mask);
+    return 0;
 }

@@ -361,7 +361,8 @@ void ora_recon_frame(const av1g_frame_header* hdr, const av1g_quant_params* q, c
 /* Every intra TU of a frame in decode order: predict (writing the TU area
  * inside the plane), CfL, residual. */
 int ora_intra_frame(const av1g_frame_header* hdr, const av1g_quant_params* q, const av1g_intra_tu* tus, int n,
-                    const int32_t* coeffs, ora_plane planes[3], const uint8_t* maps, int64_t map_bytes) {
+                    const int32_t* coeffs, ora_plane planes[3], const uint8_t* maps, int64_t map_bytes,
+                    const ora_plane* side) {
     uint16_t* pred = (uint16_t*)malloc(sizeof(uint16_t) * 64 * 64);
     int rc = 0;
     for (int k = 0; k < n; k++) {
@@ -369,7 +370,20 @@ int ora_intra_frame(const av1g_frame_header* hdr, const av1g_quant_params* q, co
         ora_plane* p = &planes[t->plane];
         int w = TW_[t->tx_size], h = TH_[t->tx_size];
         int have_pred = t->mode < INTRA_MODES;
-        if (t->mode == AV1G_INTRA_MODE_PALETTE) {
+        if (t->interintra) {
+            static const int ii_to_intra[4] = {0, 1, 2, 9};
+            if (t->interintra > 2 || t->interintra_mode > 3 || t->mode != ii_to_intra[t->interintra_mode] ||
+                t->filter_intra_mode < 5 || (t->flags & AV1G_INTRA_CFL) || !side || !side[t->plane].s) {
+                rc = k + 1;
+                break;
+            }
+            ora_intra_predict(p, t->x, t->y, t->tx_size, t->mode, 0, hdr->bit_depth, t->flags, 255, pred);
+            if (ora_interintra_blend(hdr, t, w, h, pred, &side[t->plane], p)) {
+                rc = k + 1;
+                break;
+            }
+            have_pred = 0;  /* already written */
+        } else if (t->mode == AV1G_INTRA_MODE_PALETTE) {
             /* predict_palette (cdf.rs:11907) */
             int64_t last = (int64_t)t->palette_map + (int64_t)(h - 1) * t->palette_stride + (w - 1);
             if (t->palette_size == 0 || t->palette_size > 8 || t->palette_stride < w || last >= map_bytes) {

@@ -96,7 +96,13 @@ void ora_intra_predict(const ora_plane* p, int sx, int sy, int tx, int mode, int
  * (transform_block_emit order, src/cdf.rs:32540-32910).  Returns 0, or
  * 1 + the index of the first TU the reference rejects. */
 int ora_intra_frame(const av1g_frame_header* hdr, const av1g_quant_params* q, const av1g_intra_tu* tus, int n,
-                    const int32_t* coeffs, ora_plane planes[3], const uint8_t* maps, int64_t map_bytes);
+                    const int32_t* coeffs, ora_plane planes[3], const uint8_t* maps, int64_t map_bytes,
+                    const ora_plane* side);
+
+/* The intra half of an inter-intra block: intra blended with the inter half
+ * in side (mask_blend_interintra, inter_pred.rs:3272), written to out. */
+int ora_interintra_blend(const av1g_frame_header* hdr, const av1g_intra_tu* t, int w, int h, const uint16_t* intra,
+                         const ora_plane* side, ora_plane* out);
 
 /* predict_intrabc_leaf_into_curr_frame (cdf.rs:19235) for one w x h region. */
 int ora_intrabc_predict(const ora_plane* p, int plane, int ssx, int ssy, int mi_cols, int mi_rows, int x, int y,
@@ -105,11 +111,13 @@ int ora_intrabc_predict(const ora_plane* p, int plane, int ssx, int ssy, int mi_
 /* Every inter prediction call of a frame in list order (predict_inter,
  * src/inter_pred.rs:2100, with the CurrFrame copy of its
  * reconstruct_inter_block* caller).  refs: dims of the 7 references;
- * ref_planes: their int32 planes, [ref * 3 + plane].  Returns 0, or
- * 1 + the index of the first call the reference rejects. */
+ * ref_planes: their int32 planes, [ref * 3 + plane].  side: NULL, or 3
+ * planes; an inter-intra call whose plane has one stores its clipped inter
+ * prediction there instead of blending.  Returns 0, or 1 + the index of the
+ * first call the reference rejects. */
 int ora_inter_frame(const av1g_frame_header* hdr, const av1g_ref_frame* refs, const ora_plane* ref_planes,
                     const av1g_inter_pred* preds, int n, const av1g_obmc_neighbour* nb, int n_nb,
-                    const av1g_warp_ctx* warps, int n_warps, ora_plane planes[3]);
+                    const av1g_warp_ctx* warps, int n_warps, ora_plane planes[3], ora_plane* side);
 
 /* motion_vector_scaling (inter_pred.rs:318): out = startX, startY, stepX, stepY. */
 int ora_mv_scaling(int plane, int ssx, int ssy, int fw, int fh, int ruw, int rh, int x, int y, int mv_row,

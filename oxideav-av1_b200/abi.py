@@ -114,13 +114,14 @@ class IntraTu(C.Structure):
                 ("filter_intra_mode", C.c_uint8), ("pad", C.c_uint8), ("max_luma_w", C.c_uint16),
                 ("max_luma_h", C.c_uint16), ("res", Tu), ("mv", C.c_int16 * 2), ("palette_map", C.c_uint32),
                 ("palette_stride", C.c_uint16), ("palette_size", C.c_uint8), ("pad2", C.c_uint8),
-                ("palette_colors", C.c_uint16 * 8)]
+                ("palette_colors", C.c_uint16 * 8), ("interintra", C.c_uint8), ("interintra_mode", C.c_uint8),
+                ("wedge_index", C.c_uint8), ("mi_size", C.c_uint8)]
 
 
 class IntraJob(C.Structure):
     _fields_ = [("hdr", C.POINTER(FrameHeader)), ("quant", C.POINTER(QuantParams)), ("tus", C.c_void_p),
                 ("num_tus", C.c_int32), ("sb_size", C.c_int32), ("coeffs", C.c_void_p), ("planes", Plane * 3),
-                ("palette_maps", C.c_void_p), ("palette_map_bytes", C.c_int64)]
+                ("palette_maps", C.c_void_p), ("palette_map_bytes", C.c_int64), ("interintra_in", Plane * 3)]
 
 
 class RefFrame(C.Structure):
@@ -158,7 +159,8 @@ class WarpSample(C.Structure):
 class InterJob(C.Structure):
     _fields_ = [("hdr", C.POINTER(FrameHeader)), ("refs", C.POINTER(RefFrame)), ("preds", C.c_void_p),
                 ("num_preds", C.c_int32), ("neighbours", C.c_void_p), ("num_neighbours", C.c_int32),
-                ("warps", C.c_void_p), ("num_warps", C.c_int32), ("planes", Plane * 3)]
+                ("warps", C.c_void_p), ("num_warps", C.c_int32), ("planes", Plane * 3),
+                ("interintra_out", Plane * 3)]
 
 
 INTER_SINGLE, INTER_COMPOUND, INTER_INTRA = 0, 1, 2

@@ -103,6 +103,7 @@ struct Ticket {
     std::vector<int32_t> coeffs;
     uint8_t ref_frame_idx[7] = {};
     uint8_t refresh = 0, show = 0, show_existing = 0, show_idx = 0;
+    bool has_interintra = false;  // inter halves wait in side planes for the intra pass
     // output
     uint8_t* host_out = nullptr;
     size_t host_bytes = 0;
@@ -206,6 +207,7 @@ struct FrameBufs {
     uint8_t* dev = nullptr;
     size_t bytes = 0;
     av1g_plane recon[3] = {}, deb[3] = {}, cdef[3] = {}, upcdef[3] = {}, updeb[3] = {}, lr[3] = {}, out[3] = {};
+    av1g_plane side[3] = {};  // inter halves of inter-intra blocks (only when the frame has some)
     uint8_t* grid[9] = {};
     int8_t* cdef_idx = nullptr;
     av1g_lr_unit* lr_units[3] = {};
@@ -266,6 +268,7 @@ size_t plan_frame(const Ticket& t, FrameBufs& B, std::vector<size_t>& blob_off) 
             plane(B.lr[p], pw, ph);
         }
         plane(B.out[p], uw, fh);
+        if (t.has_interintra) plane(B.side[p], pw, ph);
     }
     B.bytes = off;
     return off;
@@ -283,6 +286,7 @@ void rebase(FrameBufs& B, const std::vector<size_t>& blob_off, const Ticket& t) 
     fix(B.updeb);
     fix(B.lr);
     fix(B.out);
+    fix(B.side);
     for (int g = 0; g < 9; g++) B.grid[g] = t.grid[g].empty() ? nullptr : B.dev + blob_off[g];
     B.cdef_idx = t.cdef_idx.empty() ? nullptr : (int8_t*)(B.dev + blob_off[9]);
     for (int p = 0; p < 3; p++)
@@ -424,7 +428,10 @@ void enqueue_step(av1g_engine* E, cudaStream_t cs, std::vector<std::shared_ptr<T
             j.num_neighbours = (int32_t)w.t->nbs.size();
             j.warps = w.t->warps.empty() ? nullptr : w.t->warps.data();
             j.num_warps = (int32_t)w.t->warps.size();
-            for (int p = 0; p < 3; p++) j.planes[p] = w.B.recon[p];
+            for (int p = 0; p < 3; p++) {
+                j.planes[p] = w.B.recon[p];
+                j.interintra_out[p] = w.B.side[p];
+            }
             jobs.push_back(j);
             ws.push_back(&w);
         }
@@ -464,6 +471,7 @@ void enqueue_step(av1g_engine* E, cudaStream_t cs, std::vector<std::shared_ptr<T
             for (int p = 0; p < 3; p++) j.planes[p] = w.B.recon[p];
             j.palette_maps = w.t->maps.empty() ? nullptr : w.t->maps.data();
             j.palette_map_bytes = (int64_t)w.t->maps.size();
+            for (int p = 0; p < 3; p++) j.interintra_in[p] = w.B.side[p];
             jobs.push_back(j);
             ws.push_back(&w);
         }
@@ -941,6 +949,7 @@ av1g_status av1g_submit_frame(av1g_stream* S, const av1g_frame_desc* d, uint64_t
         for (int p = 0; p < 3; p++)
             if (h.uses_lr && p < h.num_planes && h.lr_type[p]) copy_in(t->lr_units[p], d->lr_units[p], lr_unit_count(h, p));
         copy_in(t->preds, d->inter_preds, d->num_inter_preds);
+        for (const av1g_inter_pred& pr : t->preds) t->has_interintra |= pr.kind == AV1G_INTER_INTRA;
         copy_in(t->nbs, d->neighbours, d->num_neighbours);
         copy_in(t->warps, d->warps, d->num_warps);
         copy_in(t->inter_tus, d->inter_tus, d->num_inter_tus);

@@ -28,6 +28,7 @@
 
 #include "av1_spec_tables.h"
 #include "common.cuh"
+#include "wedge.cuh"
 
 namespace av1g {
 namespace {
@@ -69,38 +70,9 @@ constexpr ObmcMasks make_obmc_masks() {
 }
 __device__ const ObmcMasks g_obmc = make_obmc_masks();
 
-// The six 64x64 wedge master masks (build_master_mask, inter_pred.rs:2712),
-// built at compile time so host and device share one definition.
-struct Master {
-    uint8_t m[6][64][64];
-};
-constexpr int cclip(int lo, int hi, int v) { return v < lo ? lo : (v > hi ? hi : v); }
-constexpr Master make_master() {
-    Master M{};
-    const uint8_t odd[] = AV1T_WEDGE_MASTER_OBLIQUE_ODD_INIT;
-    const uint8_t even[] = AV1T_WEDGE_MASTER_OBLIQUE_EVEN_INIT;
-    const uint8_t vert[] = AV1T_WEDGE_MASTER_VERTICAL_INIT;
-    for (int j = 0; j < 64; j++) {
-        int shift = 16;
-        for (int i = 0; i < 64; i += 2) {
-            M.m[3][i][j] = even[cclip(0, 63, j - shift)];
-            shift -= 1;
-            M.m[3][i + 1][j] = odd[cclip(0, 63, j - shift)];
-            M.m[1][i][j] = vert[j];
-            M.m[1][i + 1][j] = vert[j];
-        }
-    }
-    for (int i = 0; i < 64; i++)
-        for (int j = 0; j < 64; j++) {
-            uint8_t v = M.m[3][i][j];
-            M.m[2][j][i] = v;
-            M.m[4][i][63 - j] = (uint8_t)(64 - v);
-            M.m[5][63 - j][i] = (uint8_t)(64 - v);
-            M.m[0][j][i] = M.m[1][i][j];
-        }
-    return M;
-}
-constexpr Master kMaster = make_master();
+// The wedge master masks (wedge.cuh), one device copy for this kernel.
+using wedge::Master;
+using wedge::kMaster;
 __device__ const Master g_master = kMaster;
 
 // ---- device records -------------------------------------------------------
@@ -113,6 +85,7 @@ struct RefPlane {
 
 struct InterFrame {
     PlaneDev planes[3];
+    PlaneDev side[3];    // inter halves of inter-intra calls (when requested)
     RefPlane refs[7][3];
     uint8_t* mask;       // luma-grid DIFFWTD mask plane
     int32_t mask_stride;
@@ -145,7 +118,7 @@ struct Call {
     uint16_t x, y, w, h;
     uint8_t plane, nref, blend, r0, r1, post, ssx, ssy;
     uint8_t fwd, bck, mask_type, ii_mode, ii_scale, wdir, wxoff, wyoff;
-    uint8_t winv, nseg, pad[2];
+    uint8_t winv, nseg, side, pad;  // side: store the inter half of an inter-intra call
     uint32_t seg_first;
     RefCall ref[2];
 };
@@ -333,6 +306,10 @@ __global__ void __launch_bounds__(kWarps * 32) inter_kernel(const InterFrame* __
         case B_II:
         case B_II_WEDGE: {
             // mask_blend_interintra, inter_pred.rs:3272
+            if (C.side) {  // the blend happens once the intra half exists
+                v = min(max(rnd(a, C.post), 0), maxv);
+                break;
+            }
             int m;
             if (C.blend == B_II_WEDGE) m = wedge_mask_px(C, bi, bj);
             else if (C.ii_mode == 1) m = g_ii[bi * C.ii_scale];
@@ -375,7 +352,7 @@ __global__ void __launch_bounds__(kWarps * 32) inter_kernel(const InterFrame* __
         int p = lane + 32 * k, i = p >> 3, j = p & 7;
         if (i >= th || j >= tw) continue;
         int gy = C.y + r0 + i, gx = C.x + c0 + j;
-        if (gy < P.h && gx < P.w) st_px(P, hbd, gy, gx, val[k]);
+        if (gy < P.h && gx < P.w) st_px(C.side ? F.side[C.plane] : P, hbd, gy, gx, val[k]);
     }
 }
 
@@ -635,6 +612,10 @@ struct Builder {
                 c.ii_mode = d.interintra_mode;
                 c.ii_scale = (uint8_t)(128 / std::max(d.w, d.h));
             }
+            if (job.interintra_out[d.plane].data) {
+                if (d.motion_mode == 1) return bad(k, "inter-intra call with OBMC cannot use the side plane");
+                c.side = 1;
+            }
         } else if (comp) {
             switch (d.compound_type) {
             case 2: c.blend = B_AVG; break;
@@ -708,6 +689,15 @@ av1g_status inter_run(const av1g_inter_job* jobs, int n, cudaStream_t st, std::s
                 return AV1G_EINVAL;
             }
             F.planes[p] = PlaneDev{(uint8_t*)pl.data, pl.stride, pl.width, pl.height};
+            const av1g_plane& sp = j.interintra_out[p];
+            if (sp.data) {
+                if (sp.width < pl.width || sp.height < pl.height || sp.stride < pl.width * (F.hbd ? 2 : 1) ||
+                    (sp.stride & 15) || ((uintptr_t)sp.data & 15)) {
+                    err = "inter job " + std::to_string(i) + ": inter-intra side plane " + std::to_string(p);
+                    return AV1G_EINVAL;
+                }
+                F.side[p] = PlaneDev{(uint8_t*)sp.data, sp.stride, pl.width, pl.height};
+            }
             for (int r = 0; r < 7; r++) {
                 const av1g_ref_frame& R = j.refs[r];
                 int sx = p ? h.subsampling_x : 0, sy = p ? h.subsampling_y : 0;

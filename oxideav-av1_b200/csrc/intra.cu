@@ -25,6 +25,7 @@
 
 #include "common.cuh"
 #include "itx.cuh"
+#include "wedge.cuh"
 
 namespace av1g {
 
@@ -50,7 +51,34 @@ struct IntraFrame {
     ReconFrame rf;
     int32_t ssx, ssy;
     const uint8_t* maps;  // palette colour-index pool
+    PlaneDev side[3];     // inter halves of inter-intra blocks
 };
+
+__device__ const AV1T_II_WEIGHTS_1D_TYPE g_ii_w AV1T_II_WEIGHTS_1D_DIMS = AV1T_II_WEIGHTS_1D_INIT;
+__device__ const wedge::Master g_wmaster = wedge::kMaster;
+
+// The intra half of an inter-intra block: blend of the intra prediction
+// with the inter half (mask_blend_interintra, src/inter_pred.rs:3272).  The
+// mask is the §7.11.3.13 smooth mask on the plane block (read at [i][j]
+// directly) or the §7.11.3.11 wedge mask on the luma grid (orientation
+// resolved by the host into palette_map).
+template <int W, int H>
+__device__ __forceinline__ int interintra_px(const IntraFrame& F, const av1g_intra_tu& t, int i, int j, int intra,
+                                             int inter, int maxv) {
+    int m;
+    if (t.interintra == 2) {
+        const uint32_t o = t.palette_map;
+        const wedge::Orient w{(uint8_t)(o & 0xff), (uint8_t)((o >> 8) & 0xff), (uint8_t)((o >> 16) & 0xff),
+                              (uint8_t)(o >> 24)};
+        m = wedge::mask_px(g_wmaster, w, t.plane ? F.ssx : 0, t.plane ? F.ssy : 0, i, j);
+    } else {
+        constexpr int scale = 128 / (W > H ? W : H);
+        const int mode = t.interintra_mode;
+        m = mode == 1 ? __ldg(&g_ii_w[i * scale]) : mode == 2 ? __ldg(&g_ii_w[j * scale])
+          : mode == 3 ? __ldg(&g_ii_w[min(i, j) * scale]) : 32;
+    }
+    return min(max((m * intra + (64 - m) * inter + 32) >> 6, 0), maxv);
+}
 
 struct IntraItem {
     int32_t frame, first, count, level;
@@ -293,9 +321,20 @@ __device__ void intra_tu(Smem& s, const IntraFrame& F, const av1g_intra_tu& t) {
             }
         }
         __syncthreads();
-        for (int k = tid; k < W * H; k += kT) {
-            int i = k >> LW, j = k & (W - 1);
-            if (sy + i < P.h && sx + j < P.w) st_px(P, hbd, sy + i, sx + j, s.pred[k]);
+        if (t.interintra) {
+            const PlaneDev& SD = F.side[t.plane];
+            const int maxv = (1 << bd) - 1;
+            for (int k = tid; k < W * H; k += kT) {
+                int i = k >> LW, j = k & (W - 1);
+                if (sy + i < P.h && sx + j < P.w)
+                    st_px(P, hbd, sy + i, sx + j,
+                          interintra_px<W, H>(F, t, i, j, s.pred[k], ld_px(SD, hbd, sy + i, sx + j), maxv));
+            }
+        } else {
+            for (int k = tid; k < W * H; k += kT) {
+                int i = k >> LW, j = k & (W - 1);
+                if (sy + i < P.h && sx + j < P.w) st_px(P, hbd, sy + i, sx + j, s.pred[k]);
+            }
         }
         __syncthreads();
     }
@@ -428,6 +467,7 @@ av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t st, std::s
     std::vector<IntraFrame> frames(n);
     std::vector<av1g_intra_tu> all;
     std::vector<IntraItem> items;
+    std::vector<std::pair<size_t, uint32_t>> wedge_pack;  // (TU index, packed wedge window)
     std::vector<uint8_t> maps;            // palette colour indices of all jobs
     std::vector<size_t> map_base(n, 0);
     for (int i = 0; i < n; i++) {
@@ -489,6 +529,28 @@ av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t st, std::s
             }
             const int tw = kTxW[t.tx_size], th = kTxH[t.tx_size];
             const int pss_x = t.plane ? h.subsampling_x : 0, pss_y = t.plane ? h.subsampling_y : 0;
+            if (t.interintra) {
+                // the intra half of an inter-intra block: an II mode's intra
+                // mode (DC, V, H, SMOOTH) over the whole block, then the blend
+                static const uint8_t ii_to_intra[4] = {0, 1, 2, 9};
+                const av1g_plane& sp = j.interintra_in[t.plane];
+                wedge::Orient o{};
+                bool ok = t.interintra <= 2 && t.interintra_mode <= 3 && t.mode == ii_to_intra[t.interintra_mode] &&
+                          t.filter_intra_mode >= 5 && !(t.flags & AV1G_INTRA_CFL) && sp.data &&
+                          sp.width >= F.rf.planes[t.plane].w && sp.height >= F.rf.planes[t.plane].h &&
+                          sp.stride >= F.rf.planes[t.plane].w * (F.rf.hbd ? 2 : 1) && !(sp.stride & 15);
+                if (ok && t.interintra == 2)
+                    ok = wedge::orient(t.mi_size, t.wedge_index, 0, tw, th, pss_x, pss_y, o);
+                if (!ok) {
+                    err = "intra job " + std::to_string(i) + ": inter-intra TU " + std::to_string(k) + " is malformed";
+                    return AV1G_EINVAL;
+                }
+                F.side[t.plane] = PlaneDev{(uint8_t*)sp.data, sp.stride, F.rf.planes[t.plane].w, F.rf.planes[t.plane].h};
+                // the device copy of the TU carries the wedge window in
+                // palette_map (an inter-intra TU has no palette)
+                wedge_pack.emplace_back((size_t)(base + k), (uint32_t)o.dir | ((uint32_t)o.xoff << 8) |
+                                                                ((uint32_t)o.yoff << 16) | ((uint32_t)o.invert << 24));
+            }
             if (t.mode == AV1G_INTRA_MODE_PALETTE) {
                 // predict_palette's checks (cdf.rs:11907-11960)
                 long long last = (long long)t.palette_map + (long long)(th - 1) * t.palette_stride + (tw - 1);
@@ -568,6 +630,7 @@ av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t st, std::s
         }
     }
     if (items.empty()) return AV1G_OK;
+    for (const auto& wp : wedge_pack) all[wp.first].palette_map = wp.second;
     std::stable_sort(items.begin(), items.end(), [](const IntraItem& a, const IntraItem& b) { return a.level < b.level; });
     size_t off_tus = (sizeof(IntraFrame) * n + 255) & ~(size_t)255;
     size_t off_items = (off_tus + sizeof(av1g_intra_tu) * all.size() + 255) & ~(size_t)255;

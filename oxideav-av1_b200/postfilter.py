@@ -217,6 +217,8 @@ class DeviceIntra(DeviceRecon):
         self._maps = np.ascontiguousarray(getattr(self.frame, "palette_maps", np.zeros(0, np.uint8)), np.uint8)
         j.palette_maps = self._maps.ctypes.data if len(self._maps) else None
         j.palette_map_bytes = len(self._maps)
+        for p, sp in enumerate(getattr(self, "side", None) or []):
+            j.interintra_in[p] = sp.cplane()
         return j
 
 
@@ -233,11 +235,13 @@ class DeviceInter:
     """An inter frame on the GPU: CurrFrame planes (written in place), the 7
     reference planes, and the host call / neighbour / warp lists."""
 
-    def __init__(self, frame, device="cuda"):
+    def __init__(self, frame, device="cuda", side=False):
         self.frame = frame
         h = frame.hdr
         hbd = h.bit_depth > 8
         self.planes = [DevPlane(*frame.plane_dims(p), hbd, device, frame.planes[p]) for p in range(h.num_planes)]
+        # inter halves of inter-intra calls, when their blend is left to av1g_run_intra
+        self.side = [DevPlane(*frame.plane_dims(p), hbd, device) for p in range(h.num_planes)] if side else None
         self.refs = (abi.RefFrame * 7)()
         self.ref_planes = []
         for r, ref in enumerate(frame.refs):
@@ -264,6 +268,8 @@ class DeviceInter:
         j.num_warps = len(self.warps)
         for p, pl in enumerate(self.planes):
             j.planes[p] = pl.cplane()
+            if self.side:
+                j.interintra_out[p] = self.side[p].cplane()
         return j
 
     def download(self):

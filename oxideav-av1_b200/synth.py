@@ -425,7 +425,8 @@ INTRA_TU_DTYPE = np.dtype([("x", np.uint16), ("y", np.uint16), ("plane", np.uint
                            ("filter_intra_mode", np.uint8), ("pad", np.uint8), ("max_luma_w", np.uint16),
                            ("max_luma_h", np.uint16), ("res", TU_DTYPE), ("mv", np.int16, (2,)),
                            ("palette_map", np.uint32), ("palette_stride", np.uint16), ("palette_size", np.uint8),
-                           ("pad2", np.uint8), ("palette_colors", np.uint16, (8,))])
+                           ("pad2", np.uint8), ("palette_colors", np.uint16, (8,)), ("interintra", np.uint8),
+                           ("interintra_mode", np.uint8), ("wedge_index", np.uint8), ("mi_size", np.uint8)])
 assert INTRA_TU_DTYPE.itemsize == C.sizeof(abi.IntraTu)
 
 
@@ -568,7 +569,8 @@ def make_intra_frame(seed, width=176, height=144, bit_depth=8, ssx=1, ssy=1, mon
                             if pal is not None:
                                 pm += (ty - by) * bw + (tx_ - bx)
                             tus.append((tx_, ty, p, tx, mode, flags, ad, int(rng.integers(-16, 17)) if cfl else 0,
-                                        fim, 0, mlw, mlh, res, bc_mv if bc_mv else (0, 0), pm, ps, pn, 0, pc))
+                                        fim, 0, mlw, mlh, res, bc_mv if bc_mv else (0, 0), pm, ps, pn, 0, pc,
+                                        0, 0, 0, 0))
                             decoded[p][cy:cy + (th + 3) // 4, cx:cx + (tw + 3) // 4] = True
     f.tus = np.array(tus, dtype=INTRA_TU_DTYPE)
     f.coeffs = np.concatenate(coeffs).astype(np.int32) if coeffs else np.zeros(1, np.int32)
@@ -634,7 +636,7 @@ def _subsampled(mi_size, ssx, ssy):
 
 
 def make_inter_frame(seed, width=176, height=144, bit_depth=8, ssx=1, ssy=1, mono=False, scaled=True,
-                     sb_size=64, overhang=True, p_intra=0.12, ref_dims=None):
+                     sb_size=64, overhang=True, p_intra=0.12, ref_dims=None, p_ii=0.10):
     """A frame of inter blocks over a random partition: single, compound
     (average / distance / wedge / difference weight), inter-intra (smooth and
     wedge), OBMC with neighbour lists walked like obmc_dispatch_leaf
@@ -698,6 +700,9 @@ def make_inter_frame(seed, width=176, height=144, bit_depth=8, ssx=1, ssy=1, mon
 
     preds, nbs, warps = [], [], []
     f.intra_blocks = [blk for bi, blk in enumerate(blocks) if info[bi]["intra"]]
+    f.block_list = list(blocks)                                  # decode order
+    f.block_intra = [bool(info[bi]["intra"]) for bi in range(len(blocks))]
+    pred_block = []                                              # block of each call
     for bi, (x0, y0, bw, bh) in enumerate(blocks):
         b = info[bi]
         if b["intra"]:
@@ -711,7 +716,7 @@ def make_inter_frame(seed, width=176, height=144, bit_depth=8, ssx=1, ssy=1, mon
             kind = abi.INTER_COMPOUND
             choices = [2, 4, 1] + ([0] if mi_size in WEDGE_OK else [])
             ctype = int(rng.choice(choices))
-        elif big and r < 0.45 and bw <= 32 and bh <= 32:
+        elif big and r < 0.35 + p_ii and bw <= 32 and bh <= 32:
             kind = abi.INTER_INTRA
             ii_mode = int(rng.integers(0, 4))
             wii = int(mi_size in WEDGE_OK and rng.random() < 0.5)
@@ -771,6 +776,7 @@ def make_inter_frame(seed, width=176, height=144, bit_depth=8, ssx=1, ssy=1, mon
             if cw < 2 or chh < 2:
                 continue
             ge8 = _subsampled(mi_size, sx_, sy_) >= 3
+            pred_block.append(bi)
             preds.append(((x0 >> sx_), (y0 >> sy_), cw, chh, p, kind, mmode, b["fx"], b["fy"], b["ref"], ctype,
                           b["mv"], mi_size, wedge_index, wedge_sign, mask_type, ii_mode, wii, fwd, bck, warp,
                           obmc_first, n_above, n_left, avail_u, avail_l, int(ge8), (bw // 4).bit_length() - 1,
@@ -778,6 +784,7 @@ def make_inter_frame(seed, width=176, height=144, bit_depth=8, ssx=1, ssy=1, mon
     f.preds = np.zeros(len(preds), INTER_DTYPE)
     for i, t in enumerate(preds):
         f.preds[i] = t
+    f.pred_block = np.array(pred_block, np.int64)
     f.neighbours = np.zeros(len(nbs), NB_DTYPE)
     for i, (mv, pos, ref, step4, fx, fy) in enumerate(nbs):
         f.neighbours[i] = (mv, pos, ref, step4, fx, fy, (0, 0))
@@ -890,7 +897,7 @@ def _intra_tus_for_blocks(rng, h, quant, blocks, sb_size, coeff_base):
                             coeffs.append(lv)
                             off += len(lv)
                         tus.append((tx_, ty, p, tx, mode, flags, ad, 0, 255, 0, 0, 0, res, (0, 0), 0, 0, 0, 0,
-                                    [0] * 8))
+                                    [0] * 8, 0, 0, 0, 0))
     return np.array(tus, dtype=INTRA_TU_DTYPE) if tus else np.zeros(0, INTRA_TU_DTYPE), coeffs
 
 
@@ -925,14 +932,25 @@ def make_stream(seed, n_frames=4, width=176, height=144, bit_depth=8, ssx=1, ssy
         else:
             inter = make_inter_frame(fs, fw, height, bit_depth, ssx, ssy, mono, scaled=False, sb_size=sb_size,
                                      p_intra=0.1, ref_dims=[(h.upscaled_width, height)] * 7)
-            preds = inter.preds.copy()
-            ii = preds["kind"] == abi.INTER_INTRA   # inter-intra needs its intra half inside the wavefront
-            preds["kind"][ii] = abi.INTER_SINGLE
-            fr.preds, fr.neighbours, fr.warps = preds, inter.neighbours, inter.warps
+            fr.preds, fr.neighbours, fr.warps = inter.preds, inter.neighbours, inter.warps
             rec = make_recon_frame(fs + 500, fw, height, bit_depth, ssx, ssy, mono)
             fr.quant, fr.inter_tus = rec.quant, rec.tus
-            itus, icoeffs = _intra_tus_for_blocks(rng, h, rec.quant, inter.intra_blocks, sb_size, len(rec.coeffs))
-            fr.intra_tus = itus
+            # intra TUs in decode order: intra blocks, and the intra halves
+            # (+ residuals) of inter-intra blocks
+            parts, icoeffs, off = [], [], len(rec.coeffs)
+            ii_calls = np.nonzero(inter.preds["kind"] == abi.INTER_INTRA)[0]
+            for bi, blk in enumerate(inter.block_list):
+                if inter.block_intra[bi]:
+                    t, c = _intra_tus_for_blocks(rng, h, rec.quant, [blk], sb_size, off)
+                else:
+                    calls = ii_calls[inter.pred_block[ii_calls] == bi]
+                    if not len(calls):
+                        continue
+                    t, c = interintra_tus(inter, 0, rec.quant, off, calls=calls, rng=rng)
+                parts.append(t)
+                icoeffs += c
+                off += sum(len(x) for x in c)
+            fr.intra_tus = np.concatenate(parts) if parts else np.zeros(0, INTRA_TU_DTYPE)
             fr.coeffs = np.concatenate([rec.coeffs] + icoeffs).astype(np.int32)
             fr.ref_frame_idx = [int(v) for v in rng.integers(0, 8, size=7)]
             fr.refresh = int(rng.integers(0, 256)) & int(rng.integers(0, 256))
@@ -945,3 +963,46 @@ def stream_seq(frames, sb_size=64):
     return {"max_width": h.upscaled_width, "max_height": h.frame_height, "bit_depth": h.bit_depth,
             "subsampling_x": h.subsampling_x, "subsampling_y": h.subsampling_y, "num_planes": h.num_planes,
             "sb_size": sb_size}
+
+
+
+II_TO_INTRA = [0, 1, 2, 9]   # II_DC/V/H/SMOOTH -> DC_PRED, V_PRED, H_PRED, SMOOTH_PRED
+
+
+def interintra_tus(f, seed, quant=None, coeff_base=0, calls=None, rng=None):
+    """For each inter-intra call of an InterFrame (or of the call indices
+    `calls`), in list order (block decode order), the TU of its intra half
+    (the block's intra prediction blended with the inter half) and a residual
+    TU over the block.  Returns (tus, coeffs)."""
+    rng = rng if rng is not None else np.random.default_rng(seed)
+    h = f.hdr
+    q = quant if quant is not None else f.quant
+    ok_segs = [s_ for s_ in range(8) if not q.lossless[s_]]
+    tus, coeffs, off = [], [], coeff_base
+    for d in (f.preds if calls is None else f.preds[calls]):
+        if d["kind"] != abi.INTER_INTRA:
+            continue
+        x, y, w, hh, p = int(d["x"]), int(d["y"]), int(d["w"]), int(d["h"]), int(d["plane"])
+        if (w, hh) not in TX_OF:
+            continue
+        tx = TX_OF[(w, hh)]
+        flags = abi.INTRA_EDGE_FILTER
+        if y > 0:
+            flags |= abi.INTRA_HAVE_ABOVE
+        if x > 0:
+            flags |= abi.INTRA_HAVE_LEFT
+        iim = int(d["interintra_mode"])
+        kind = 2 if d["wedge_interintra"] else 1
+        none_res = (x, y, p, tx, 0, 0, 0, (0, 0, 0), 0)
+        tus.append((x, y, p, tx, II_TO_INTRA[iim], flags, 0, 0, 255, 0, 0, 0, none_res, (0, 0), 0, 0, 0, 0,
+                    [0] * 8, kind, iim, int(d["wedge_index"]), int(d["mi_size"])))
+        if ok_segs and rng.random() < 0.8:
+            seg = int(rng.choice(ok_segs))
+            lv = _levels(rng, min(32, w), min(32, hh), False)
+            res = (x, y, p, tx, _tx_type_for(rng, w, hh), seg, int(rng.integers(1, 256)), (0, 0, 0), off)
+            coeffs.append(lv)
+            off += len(lv)
+            tus.append((x, y, p, tx, abi.INTRA_MODE_NONE, abi.INTRA_RESIDUAL, 0, 0, 255, 0, 0, 0, res, (0, 0), 0,
+                        0, 0, 0, [0] * 8, 0, 0, 0, 0))
+    arr = np.array(tus, dtype=INTRA_TU_DTYPE) if tus else np.zeros(0, INTRA_TU_DTYPE)
+    return arr, coeffs

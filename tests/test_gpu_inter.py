@@ -81,3 +81,29 @@ def test_inter_rejects_caller_bugs():
         d = postfilter.DeviceInter(f)
         with pytest.raises(abi.Av1gError):
             postfilter.run_inter([d])
+
+
+II_CASES = [dict(seed=311), dict(seed=312, bit_depth=10), dict(seed=313, ssx=0, ssy=0), dict(seed=314, mono=True),
+            dict(seed=315, width=200, height=120, bit_depth=12)]
+
+
+@pytest.mark.parametrize("case", II_CASES, ids=[f"s{c['seed']}" for c in II_CASES])
+def test_interintra_two_pass_on_gpu(case):
+    # the inter pass leaves inter-intra blocks' inter halves in side planes;
+    # the intra wavefront blends them with the intra halves, as in
+    # tests/test_oracle_interintra_split.py
+    from test_oracle_interintra_split import ii_case, split_order
+    abi.load()
+    f, quant, tus, coeffs = ii_case(**case)
+    want = split_order(f, quant, tus, coeffs)
+    d = postfilter.DeviceInter(f, side=True)
+    postfilter.run_inter([d])
+    it = synth.IntraFrame()
+    it.hdr, it.quant, it.tus, it.coeffs, it.planes = f.hdr, quant, tus, coeffs, f.planes
+    di = postfilter.DeviceIntra(it)
+    di.planes, di.side = d.planes, d.side
+    postfilter.run_intra([di])
+    torch.cuda.synchronize()
+    for p, (g, e) in enumerate(zip(di.download(), want)):
+        diff = np.argwhere(g.astype(np.int64) != e)
+        assert len(diff) == 0, f"plane {p}: {len(diff)} samples differ, first {tuple(diff[0])}"
