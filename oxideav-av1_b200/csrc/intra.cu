@@ -1,5 +1,5 @@
 // intra.cu — §7.11.2 intra prediction, §7.11.5 chroma from luma and intra
-// reconstruction as a superblock-diagonal wavefront.
+// reconstruction as one persistent superblock-wavefront launch.
 //
 // Replaces predict_intra_into_curr_frame (src/cdf.rs:16789),
 // intra_predict_block_samples (cdf.rs:16990-17250), the mode kernels
@@ -7,23 +7,35 @@
 // (cdf.rs:17256) in the order transform_block_emit runs them per TU
 // (cdf.rs:32540-32910): predict, CfL, dequant + inverse transform + merge.
 //
-// An intra TU reads the final samples of the row above and the column to its
-// left, up to twice its size (above-right / below-left when already decoded).
-// Within a superblock that forces decode order; across superblocks every
-// reference points at the same or an earlier superblock row and at most one
-// superblock to the right in the row above, so superblock (c, r) only depends
-// on superblocks of level c + 2r - 1 or lower.  The host groups each frame's
-// TUs by superblock and launches one kernel per level over all frames of the
-// batch (no inter-CTA waiting); one 64-thread CTA runs its superblock's TUs in
-// decode order, parallel within each TU.
+// Dependencies.  An intra TU reads final samples of the row above and the
+// column to its left (up to twice its size), the co-located luma for CfL and,
+// for intra block copy, a window of the frame.  The host walks each frame's
+// TUs in decode order and records every area a TU reads:
+//  - between superblocks, B waits for A when a TU of one of them reads the
+//    other's area and A comes first in decode order (a read of a later
+//    superblock's area orders the later one after the reader, as sequential
+//    decoding does), so the waits form a DAG ordered by decode order;
+//  - inside a superblock, a TU's level is one above the last writer of each
+//    4x4 cell it reads or writes and the last reader of each cell it writes,
+//    so the TUs of one level are independent of one another.
+// One persistent launch covers the batch.  A CTA claims superblocks from an
+// atomic counter in a topological order (dependency depth, frame, decode
+// order), stages the superblock's samples in shared memory, waits (bounded)
+// for the superblocks it depends on, runs the levels — a level's small TUs one
+// per warp, then its large TUs with the whole CTA — writes the samples back and
+// publishes a done flag.  A CTA only waits for superblocks claimed before its
+// own, by CTAs that are running, so every wait ends; the time bound only
+// guards against a broken invariant (it sets a sticky fault word and the
+// launch drains).
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <unordered_map>
-#include <unordered_set>
 #include <vector>
 
 #include "common.cuh"
+#include "intra_plan.h"
 #include "itx.cuh"
 #include "wedge.cuh"
 
@@ -33,8 +45,11 @@ namespace {
 
 using namespace itx;
 
-constexpr int kT = 64;
-constexpr int kEdge = 272;  // 2 * (64 + 64) + 2 rounded up; index 0 == position -2
+constexpr int kT = 128;             // threads per CTA
+constexpr int kNW = kT / 32;        // warps per CTA
+constexpr int kSmallPx = kIntraSmallPx;
+constexpr int kLvChunk = 256;       // level-table entries staged at a time
+constexpr long long kWaitNs = 2000000000LL;
 
 __constant__ AV1T_MODE_TO_ANGLE_TYPE c_mode_angle AV1T_MODE_TO_ANGLE_DIMS = AV1T_MODE_TO_ANGLE_INIT;
 __constant__ AV1T_DR_INTRA_DERIVATIVE_TYPE c_dr AV1T_DR_INTRA_DERIVATIVE_DIMS = AV1T_DR_INTRA_DERIVATIVE_INIT;
@@ -47,15 +62,14 @@ __constant__ AV1T_SM_WEIGHTS_TX_32X32_TYPE c_sm32 AV1T_SM_WEIGHTS_TX_32X32_DIMS 
 __constant__ AV1T_SM_WEIGHTS_TX_64X64_TYPE c_sm64 AV1T_SM_WEIGHTS_TX_64X64_DIMS = AV1T_SM_WEIGHTS_TX_64X64_INIT;
 __constant__ AV1T_SUBPEL_FILTERS_TYPE c_subpel AV1T_SUBPEL_FILTERS_DIMS = AV1T_SUBPEL_FILTERS_INIT;
 
-struct IntraFrame {
-    ReconFrame rf;
-    int32_t ssx, ssy;
-    const uint8_t* maps;  // palette colour-index pool
-    PlaneDev side[3];     // inter halves of inter-intra blocks
+// The superblock's area in each plane and where the shared-memory copy keeps it.
+struct SbCtx {
+    int x0[3], y0[3], w[3], h[3], off[3];
 };
 
 __device__ const AV1T_II_WEIGHTS_1D_TYPE g_ii_w AV1T_II_WEIGHTS_1D_DIMS = AV1T_II_WEIGHTS_1D_INIT;
 __device__ const wedge::Master g_wmaster = wedge::kMaster;
+__device__ unsigned g_wave_fault;  // sticky: a dependency wait ran out of time
 
 // The intra half of an inter-intra block: blend of the intra prediction
 // with the inter half (mask_blend_interintra, src/inter_pred.rs:3272).  The
@@ -80,33 +94,73 @@ __device__ __forceinline__ int interintra_px(const IntraFrame& F, const av1g_int
     return min(max((m * intra + (64 - m) * inter + 32) >> 6, 0), maxv);
 }
 
-struct IntraItem {
-    int32_t frame, first, count, level;
+// A TU is run either by one warp or by the whole CTA; both expose a rank,
+// a size and a barrier over exactly the threads that run the TU.
+struct WarpG {
+    static constexpr int N = 32;
+    int r;
+    __device__ __forceinline__ void sync() const { __syncwarp(); }
+};
+struct CtaG {
+    static constexpr int N = kT;
+    int r;
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
 };
 
-struct Smem {
-    uint16_t above[kEdge], left[kEdge], dup[kEdge];
-    uint16_t pred[64 * 64];
-    int buf[64 * 64];
-    long long red[kT / 32];
+// Per-group scratch: edge arrays (index 0 == position -2), the dense
+// coefficient / residual block, the reduction slots and the TU record.
+template <int E, int PX>
+struct Scr {
+    uint16_t above[E], left[E], dup[E];
+    int buf[PX];
+    long long red[kNW];
     av1g_intra_tu tu;
 };
+using WScr = Scr<96, kSmallPx>;  // W + H <= 40 for the small sizes: 2 + 2 * 40 entries at most
+using CScr = Scr<272, 64 * 64>;  // 2 * (64 + 64) + 2 rounded up
+
+struct alignas(16) Shared {
+    union {
+        WScr w[kNW];
+        CScr c;
+    } s;
+    int2 lv[kLvChunk + 1];
+    SbCtx sb;
+    int idx, abort_seen;
+};
+constexpr size_t kSharedBytes = (sizeof(Shared) + 15) & ~(size_t)15;
 
 __device__ __forceinline__ const uint8_t* sm_weights(int log2n) {
     return log2n == 2 ? c_sm4 : log2n == 3 ? c_sm8 : log2n == 4 ? c_sm16 : log2n == 5 ? c_sm32 : c_sm64;
 }
 
-// CTA-wide sum (all threads call)
-__device__ long long block_sum(Smem& s, long long v) {
+// Sum over the group (every thread of it calls).
+template <class G, class S>
+__device__ __forceinline__ long long gsum(const G& g, S& s, long long v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffff, v, o);
-    if ((threadIdx.x & 31) == 0) s.red[threadIdx.x >> 5] = v;
-    __syncthreads();
-    long long t = 0;
+    if constexpr (G::N > 32) {
+        if ((g.r & 31) == 0) s.red[g.r >> 5] = v;
+        __syncthreads();
+        long long t = 0;
 #pragma unroll
-    for (int k = 0; k < kT / 32; k++) t += s.red[k];
-    __syncthreads();
-    return t;
+        for (int k = 0; k < G::N / 32; k++) t += s.red[k];
+        __syncthreads();
+        return t;
+    } else {
+        return v;
+    }
+}
+
+// A sample of plane p at (y, x), inside the plane: from the shared-memory
+// copy when it lies in the current superblock, else from HBM (an earlier
+// superblock's final samples, published by its done flag; read past L1).
+__device__ __forceinline__ int rdp(const IntraFrame& F, const SbCtx& c, const uint16_t* cache, int p, int y, int x) {
+    const int ly = y - c.y0[p], lx = x - c.x0[p];
+    if ((unsigned)ly < (unsigned)c.h[p] && (unsigned)lx < (unsigned)c.w[p]) return cache[c.off[p] + ly * c.w[p] + lx];
+    const PlaneDev& P = F.planes[p];
+    const uint8_t* row = P.p + (size_t)y * P.stride;
+    return F.hbd ? (int)__ldcg(reinterpret_cast<const unsigned short*>(row) + x) : (int)__ldcg(row + x);
 }
 
 // intra_edge_filter_strength_selection (cdf.rs:2610)
@@ -134,51 +188,178 @@ __device__ int upsample_sel(int w, int h, int ft, int delta) {
 }
 
 // intra_edge_filter (cdf.rs:2760) on an edge array (index 0 == position -2), in parallel
-__device__ void edge_filter(Smem& s, uint16_t* e, int sz, int strength) {
-    if (strength == 0 || sz == 0) return;  // uniform
-    for (int i = threadIdx.x; i < sz; i += kT) s.dup[i] = e[i + 1];
-    __syncthreads();
-    for (int i = 1 + threadIdx.x; i < sz; i += kT) {
+template <class G, class S>
+__device__ void edge_filter(const G& g, S& s, uint16_t* e, int sz, int strength) {
+    if (strength == 0 || sz == 0) return;  // uniform over the group
+    for (int i = g.r; i < sz; i += G::N) s.dup[i] = e[i + 1];
+    g.sync();
+    for (int i = 1 + g.r; i < sz; i += G::N) {
         int acc = 0;
 #pragma unroll
         for (int j = 0; j < 5; j++) acc += c_edge_k[strength - 1][j] * s.dup[clip3(0, sz - 1, i - 2 + j)];
         e[i + 1] = (uint16_t)max((acc + 8) >> 4, 0);
     }
-    __syncthreads();
+    g.sync();
 }
 
 // intra_edge_upsample (cdf.rs:2700), in parallel
-__device__ void edge_upsample(Smem& s, uint16_t* e, int n, int bd) {
-    if (threadIdx.x == 0) {
+template <class G, class S>
+__device__ void edge_upsample(const G& g, S& s, uint16_t* e, int n, int bd) {
+    if (g.r == 0) {
         s.dup[0] = e[1];
         s.dup[1] = e[1];
         s.dup[n + 2] = e[n + 1];
     }
-    for (int i = threadIdx.x; i < n; i += kT) s.dup[i + 2] = e[i + 2];
-    __syncthreads();
+    for (int i = g.r; i < n; i += G::N) s.dup[i + 2] = e[i + 2];
+    g.sync();
     const int maxv = (1 << bd) - 1;
-    if (threadIdx.x == 0) e[0] = s.dup[0];
-    for (int i = threadIdx.x; i < n; i += kT) {
+    if (g.r == 0) e[0] = s.dup[0];
+    for (int i = g.r; i < n; i += G::N) {
         int sum = -s.dup[i] + 9 * s.dup[i + 1] + 9 * s.dup[i + 2] - s.dup[i + 3];
         int r = sum >= 0 ? (sum + 8) >> 4 : -(((-sum) + 8) >> 4);
         e[2 * i + 1] = (uint16_t)clip3(0, maxv, r);
         e[2 * i + 2] = (uint16_t)min((int)s.dup[i + 2], maxv);
     }
-    __syncthreads();
+    g.sync();
 }
 
-// One TU: prediction (+ CfL) into the plane, then the residual.
-template <int TX>
-__device__ void intra_tu(Smem& s, const IntraFrame& F, const av1g_intra_tu& t) {
-    constexpr int W = kTxW[TX], H = kTxH[TX], L = W > H ? W : H;
+// Dequantize (dequantize_step1, cdf.rs:13655-13703), inverse transform
+// (transform.rs:707-789) and merge (curr_frame_step3_merge, cdf.rs:17398-17470)
+// one TU into the shared-memory copy of its superblock.  cf holds the compact
+// levels, cf[q] == level[g.r + q * G::N]; tp is the TU's top-left sample in
+// the copy (row pitch cs); samples outside the plane are left alone.
+template <int TX, class G, class S>
+__device__ __forceinline__ void residual_g(const G& g, S& s, const IntraFrame& R, const av1g_tu& tu, const int* cf, uint16_t* tp,
+                           int cs, int pw, int ph) {
+    constexpr int W = kTxW[TX], H = kTxH[TX];
     constexpr int LW = ilog2<W>(), LH = ilog2<H>();
-    const int tid = threadIdx.x;
-    const PlaneDev& P = F.rf.planes[t.plane];
-    const int hbd = F.rf.hbd, bd = F.rf.bd;
+    constexpr int TW = W < 32 ? W : 32, TH = H < 32 ? H : 32, NC = TW * TH, K = (NC + G::N - 1) / G::N;
+    constexpr int ABS_D = LW > LH ? LW - LH : LH - LW;
+    const int bd = R.bd;
+    const int seg = tu.segment_id > 7 ? 7 : tu.segment_id;
+    const bool lossless = R.q.lossless[seg] != 0;
+    for (int k = g.r; k < W * H; k += G::N) s.buf[k] = 0;
+    g.sync();
+    {
+        const av1g_quant_params& q = R.q;
+        int qidx;
+        if (q.segmentation_enabled && q.seg_alt_q_active[seg]) {
+            int data = q.seg_alt_q_data[seg];
+            qidx = clip3(0, 255, (q.delta_q_present ? tu.current_q_index : q.base_q_idx) + data);
+        } else {
+            qidx = q.delta_q_present ? tu.current_q_index : q.base_q_idx;
+        }
+        const int p = tu.plane;
+        const int ddc = p == 0 ? q.delta_q_y_dc : (p == 1 ? q.delta_q_u_dc : q.delta_q_v_dc);
+        const int dac = p == 0 ? 0 : (p == 1 ? q.delta_q_u_ac : q.delta_q_v_ac);
+        const int row = min((max(bd, 8) - 8) >> 1, 2);
+        const int dcq = c_dcq[row][clip3(0, 255, qidx + ddc)], acq = c_acq[row][clip3(0, 255, qidx + dac)];
+        const int qml = q.seg_qm_level[p][seg];
+        const bool qm = q.using_qmatrix && tu.tx_type < 9 && qml < 15;
+        constexpr int denom_sh = (TX == 3 || TX == 9 || TX == 10 || TX == 17 || TX == 18) ? 1
+                               : (TX == 4 || TX == 11 || TX == 12) ? 2 : 0;
+        const long long cmax = (1LL << (7 + bd)) - 1, cmin = -(1LL << (7 + bd));
+#pragma unroll
+        for (int qq = 0; qq < K; qq++) {
+            const int k = g.r + qq * G::N;
+            if (NC % G::N == 0 || k < NC) {
+                const int i = k / TW, j = k % TW;
+                long long qv = k == 0 ? dcq : acq;
+                if (qm) qv = (qv * g_qm[qml][p > 0][c_qm_off[TX] + k] + 16) >> 5;
+                const long long dq = (long long)cf[qq] * qv;
+                const long long mag = (dq < 0 ? -dq : dq) & 0xFFFFFF;
+                const long long v = (dq < 0 ? -mag : mag) / (1 << denom_sh);  // truncating division, as the reference
+                s.buf[i * W + j] = (int)min(max(v, cmin), cmax);
+            }
+        }
+    }
+    g.sync();
+    const Clamp rr{-(1 << (bd + 7)), (1 << (bd + 7)) - 1};
+    const int crb = bd + 6 > 16 ? bd + 6 : 16;
+    const Clamp cr{-(1 << (crb - 1)), (1 << (crb - 1)) - 1};
+    if (g.r < H && g.r < 32) {
+        int t[W];
+        int* rowp = s.buf + g.r * W;
+#pragma unroll
+        for (int j = 0; j < W; j++) t[j] = j < 32 ? rowp[j] : 0;
+        if constexpr (ABS_D == 1) {
+#pragma unroll
+            for (int j = 0; j < W; j++) t[j] = rnd12((long long)t[j] * 2896);
+        }
+        constexpr int kRs = kRowShift[TX];
+        const int rsh = lossless ? 0 : kRs;
+        if (lossless) {
+            if constexpr (W == 4) iwht4(t, 2);
+        } else {
+            tx1d<LW>(t, row_kind(tu.tx_type), rr);
+        }
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+            int v = rsh ? (t[j] + (1 << (rsh - 1))) >> rsh : t[j];
+            rowp[j] = min(max(v, cr.lo), cr.hi);
+        }
+    }
+    g.sync();
+    if (g.r < W) {
+        const int lane = g.r;
+        int t[H];
+#pragma unroll
+        for (int i = 0; i < H; i++) t[i] = s.buf[i * W + lane];
+        if (lossless) {
+            if constexpr (H == 4) iwht4(t, 0);
+        } else {
+            tx1d<LH>(t, col_kind(tu.tx_type), cr);
+        }
+        const int csh = lossless ? 0 : 4;
+        const int tt = tu.tx_type;
+        const bool fud = tt == 4 || tt == 8 || tt == 14 || tt == 6;
+        const bool flr = tt == 5 || tt == 7 || tt == 15 || tt == 6;
+        const int x = flr ? W - 1 - lane : lane;
+        const int maxv = (1 << bd) - 1;
+        if (tu.x + x < pw) {
+#pragma unroll
+            for (int i = 0; i < H; i++) {
+                const int y = fud ? H - 1 - i : i;
+                if (tu.y + y >= ph) continue;
+                const int res = csh ? (t[i] + (1 << (csh - 1))) >> csh : t[i];
+                uint16_t& px = tp[y * cs + x];
+                px = (uint16_t)min(max((int)px + res, 0), maxv);
+            }
+        }
+    }
+    g.sync();
+}
+
+// One TU: prediction (+ inter-intra blend, + CfL), then the residual, all on
+// the shared-memory copy of the superblock.
+template <int TX, class G, class S>
+__device__ void intra_tu(const G& g, S& s, const IntraFrame& F, const SbCtx& c, uint16_t* cache,
+                         const av1g_intra_tu& t) {
+    constexpr int W = kTxW[TX], H = kTxH[TX];
+    constexpr int LW = ilog2<W>(), LH = ilog2<H>();
+    constexpr int TW = W < 32 ? W : 32, TH = H < 32 ? H : 32, NC = TW * TH, K = (NC + G::N - 1) / G::N;
+    const int tid = g.r;
+    const int pl = t.plane;
+    const PlaneDev& P = F.planes[pl];
+    const int hbd = F.hbd, bd = F.bd;
     const int sx = t.x, sy = t.y;
+    const int cs = c.w[pl];
+    uint16_t* tp = cache + c.off[pl] + (sy - c.y0[pl]) * cs + (sx - c.x0[pl]);
+    const bool has_res = t.flags & AV1G_INTRA_RESIDUAL;
+    // the compact levels, fetched first so that their latency overlaps the prediction
+    int cf[K];
+    {
+        const int32_t* lv = F.coeffs + (has_res ? t.res.coeff_offset : 0);
+#pragma unroll
+        for (int q = 0; q < K; q++) {
+            const int k = tid + q * G::N;
+            cf[q] = (has_res && k < NC) ? __ldg(lv + k) : 0;
+        }
+    }
+    const int maxv = (1 << bd) - 1;
     if (t.mode < 13) {
         const int max_x = P.w - 1, max_y = P.h - 1;
-        auto rd = [&](int yy, int xx) { return ld_px(P, hbd, min(yy, max_y), min(xx, max_x)); };
+        auto rd = [&](int yy, int xx) { return rdp(F, c, cache, pl, min(yy, max_y), min(xx, max_x)); };
         const bool ha = (t.flags & AV1G_INTRA_HAVE_ABOVE) && sy > 0;
         const bool hl = (t.flags & AV1G_INTRA_HAVE_LEFT) && sx > 0;
         const bool har = t.flags & AV1G_INTRA_HAVE_ABOVE_RIGHT, hbl = t.flags & AV1G_INTRA_HAVE_BELOW_LEFT;
@@ -187,7 +368,7 @@ __device__ void intra_tu(Smem& s, const IntraFrame& F, const av1g_intra_tu& t) {
         const int corner = ha && hl ? rd(sy - 1, sx - 1) : ha ? rd(sy - 1, sx) : hl ? rd(sy, sx - 1) : 1 << (bd - 1);
         constexpr int span = W + H;
         // edge arrays (intra_predict_block_samples, cdf.rs:17030-17075)
-        for (int i = tid; i < span; i += kT) {
+        for (int i = tid; i < span; i += G::N) {
             int a, l;
             if (!ha && hl) a = rd(sy, sx - 1);
             else if (!ha && !hl) a = (1 << (bd - 1)) - 1;
@@ -199,7 +380,7 @@ __device__ void intra_tu(Smem& s, const IntraFrame& F, const av1g_intra_tu& t) {
             s.left[2 + i] = (uint16_t)l;
         }
         if (tid < 2) s.above[tid] = s.left[tid] = (uint16_t)corner;
-        __syncthreads();
+        g.sync();
         const bool dir = t.mode >= 1 && t.mode <= 8;
         const int pa = c_mode_angle[t.mode] + t.angle_delta * 3;
         int ua = 0, ul = 0;
@@ -210,68 +391,75 @@ __device__ void intra_tu(Smem& s, const IntraFrame& F, const av1g_intra_tu& t) {
                     s.above[1] = fc;
                     s.left[1] = fc;
                 }
-                __syncthreads();
+                g.sync();
             }
-            if (ha) edge_filter(s, s.above, min(W, max_x - sx + 1) + (pa < 90 ? H : 0) + 1, strength_sel(W, H, ft, pa - 90));
-            if (hl) edge_filter(s, s.left, min(H, max_y - sy + 1) + (pa > 180 ? W : 0) + 1, strength_sel(W, H, ft, pa - 180));
+            if (ha) edge_filter(g, s, s.above, min(W, max_x - sx + 1) + (pa < 90 ? H : 0) + 1, strength_sel(W, H, ft, pa - 90));
+            if (hl) edge_filter(g, s, s.left, min(H, max_y - sy + 1) + (pa > 180 ? W : 0) + 1, strength_sel(W, H, ft, pa - 180));
             ua = upsample_sel(W, H, ft, pa - 90);
-            if (ua) edge_upsample(s, s.above, W + (pa < 90 ? H : 0), bd);
+            if (ua) edge_upsample(g, s, s.above, W + (pa < 90 ? H : 0), bd);
             ul = upsample_sel(W, H, ft, pa - 180);
-            if (ul) edge_upsample(s, s.left, H + (pa > 180 ? W : 0), bd);
+            if (ul) edge_upsample(g, s, s.left, H + (pa > 180 ? W : 0), bd);
         }
         const uint16_t* A = s.above + 2;  // A[k] == AboveRow[k]
         const uint16_t* Lc = s.left + 2;
-        const int fim = (t.plane == 0 && t.filter_intra_mode < 5) ? t.filter_intra_mode : -1;
+        const int fim = (pl == 0 && t.filter_intra_mode < 5) ? t.filter_intra_mode : -1;
+        // the intra half of an inter-intra block is blended as it is stored
+        // (only inside the plane: the side plane has the plane's extent)
+        auto put = [&](int i, int j, int v) {
+            if (t.interintra && sy + i < P.h && sx + j < P.w)
+                v = interintra_px<W, H>(F, t, i, j, v, ld_px(F.side[pl], hbd, sy + i, sx + j), maxv);
+            tp[i * cs + j] = (uint16_t)v;
+        };
         if (fim >= 0) {
-            // predict_intra_recursive (cdf.rs:2145): 4x2 cells, wavefront over i2 + j4
+            // predict_intra_recursive (cdf.rs:2145): 4x2 cells, wavefront over
+            // i2 + j4, reading earlier cells back from the copy
             constexpr int W4 = W >> 2, H2 = H >> 1;
-            const int maxv = (1 << bd) - 1;
+            const int o = tid & 7, i1 = o >> 2, j1 = o & 3;
             for (int d = 0; d < W4 + H2 - 1; d++) {
-                int b = tid >> 3, o = tid & 7;
-                int i2 = max(0, d - (W4 - 1)) + b, j4 = d - i2;
-                if (i2 < H2 && j4 >= 0) {
+                for (int bb = tid >> 3;; bb += G::N >> 3) {
+                    const int i2 = max(0, d - (W4 - 1)) + bb, j4 = d - i2;
+                    if (i2 >= H2 || j4 < 0) break;
                     int p[7];
 #pragma unroll
                     for (int i = 0; i < 7; i++) {
                         if (i < 5) {
                             if (i2 == 0) p[i] = A[(j4 << 2) + i - 1];
                             else if (j4 == 0 && i == 0) p[i] = Lc[(i2 << 1) - 1];
-                            else p[i] = s.pred[((i2 << 1) - 1) * W + (j4 << 2) + i - 1];
+                            else p[i] = tp[((i2 << 1) - 1) * cs + (j4 << 2) + i - 1];
                         } else if (j4 == 0) {
                             p[i] = Lc[(i2 << 1) + i - 5];
                         } else {
-                            p[i] = s.pred[((i2 << 1) + i - 5) * W + (j4 << 2) - 1];
+                            p[i] = tp[((i2 << 1) + i - 5) * cs + (j4 << 2) - 1];
                         }
                     }
-                    int i1 = o >> 2, j1 = o & 3;
                     int acc = 0;
 #pragma unroll
                     for (int i = 0; i < 7; i++) acc += c_fi_taps[fim][(i1 << 2) + j1][i] * p[i];
                     int v = acc >= 0 ? (acc + 8) >> 4 : -(((-acc) + 8) >> 4);
-                    s.pred[((i2 << 1) + i1) * W + (j4 << 2) + j1] = (uint16_t)clip3(0, maxv, v);
+                    tp[((i2 << 1) + i1) * cs + (j4 << 2) + j1] = (uint16_t)clip3(0, maxv, v);
                 }
-                __syncthreads();
+                g.sync();
             }
         } else if (t.mode == 0) {
             // predict_intra_dc_pred (cdf.rs:1348)
             long long part = 0;
-            for (int i = tid; i < span; i += kT) {
+            for (int i = tid; i < span; i += G::N) {
                 if (hl && i < H) part += Lc[i];
                 if (ha && i < W) part += A[i];
             }
-            long long sum = block_sum(s, part);
+            long long sum = gsum(g, s, part);
             unsigned avg;
             if (hl && ha) avg = (unsigned)((sum + (span >> 1)) / span);
             else if (hl) avg = min((unsigned)((sum + (H >> 1)) >> LH), (1u << bd) - 1);
             else if (ha) avg = min((unsigned)((sum + (W >> 1)) >> LW), (1u << bd) - 1);
             else avg = 1u << (bd - 1);
-            for (int k = tid; k < W * H; k += kT) s.pred[k] = (uint16_t)avg;
+            for (int k = tid; k < W * H; k += G::N) put(k >> LW, k & (W - 1), (int)avg);
         } else {
             const int dx = pa < 90 ? c_dr[pa] : (pa < 180 ? c_dr[180 - pa] : 0);
             const int dy = (pa >= 90 && pa < 180) ? c_dr[pa - 90] : (pa > 180 ? c_dr[270 - pa] : 0);
             const uint8_t* swx = sm_weights(LW);
             const uint8_t* swy = sm_weights(LH);
-            for (int k = tid; k < W * H; k += kT) {
+            for (int k = tid; k < W * H; k += G::N) {
                 int i = k >> LW, j = k & (W - 1);
                 int v;
                 if (t.mode == 1 && t.angle_delta == 0) {
@@ -314,353 +502,329 @@ __device__ void intra_tu(Smem& s, const IntraFrame& F, const av1g_intra_tu& t) {
                     v = (int)((swx[j] * Lc[i] + (256 - swx[j]) * A[W - 1] + 128) >> 8);
                 } else {  // PAETH (cdf.rs:2077)
                     int base = A[j] + Lc[i] - corner;
-                    int pl = abs(base - Lc[i]), pt = abs(base - A[j]), ptl = abs(base - corner);
-                    v = (pl <= pt && pl <= ptl) ? Lc[i] : (pt <= ptl ? A[j] : corner);
+                    int pl_ = abs(base - Lc[i]), pt = abs(base - A[j]), ptl = abs(base - corner);
+                    v = (pl_ <= pt && pl_ <= ptl) ? Lc[i] : (pt <= ptl ? A[j] : corner);
                 }
-                s.pred[k] = (uint16_t)v;
+                put(i, j, v);
             }
         }
-        __syncthreads();
-        if (t.interintra) {
-            const PlaneDev& SD = F.side[t.plane];
-            const int maxv = (1 << bd) - 1;
-            for (int k = tid; k < W * H; k += kT) {
-                int i = k >> LW, j = k & (W - 1);
-                if (sy + i < P.h && sx + j < P.w)
-                    st_px(P, hbd, sy + i, sx + j,
-                          interintra_px<W, H>(F, t, i, j, s.pred[k], ld_px(SD, hbd, sy + i, sx + j), maxv));
-            }
-        } else {
-            for (int k = tid; k < W * H; k += kT) {
-                int i = k >> LW, j = k & (W - 1);
-                if (sy + i < P.h && sx + j < P.w) st_px(P, hbd, sy + i, sx + j, s.pred[k]);
-            }
-        }
-        __syncthreads();
+        g.sync();
     }
-    if (t.mode == AV1G_INTRA_MODE_PALETTE || t.mode == AV1G_INTRA_MODE_INTRABC) {
-        const int maxv = (1 << bd) - 1;
-        if (t.mode == AV1G_INTRA_MODE_PALETTE) {
-            // predict_palette (cdf.rs:11907); indices checked on the host
-            const uint8_t* m = F.maps + t.palette_map;
-            for (int k = tid; k < W * H; k += kT) {
-                int i = k >> LW, j = k & (W - 1);
-                s.pred[k] = s.tu.palette_colors[m[i * t.palette_stride + j]];
-            }
-        } else {
-            // predict_intrabc_leaf_into_curr_frame (cdf.rs:19235): BILINEAR
-            // block_inter_prediction from the pre-filter plane at unit scale,
-            // start = (x << 10) + (((2 * mv) >> ss) << 6) + 32, clamped to the
-            // mi-padded plane (the reference's window clamp is the same set).
-            const int pss_x = t.plane ? F.ssx : 0, pss_y = t.plane ? F.ssy : 0;
-            const int stx = (sx << 10) + ((2 * t.mv[1]) >> pss_x) * 64 + 32;
-            const int sty = (sy << 10) + ((2 * t.mv[0]) >> pss_y) * 64 + 32;
-            const int r0 = bd == 12 ? 5 : 3, r1 = bd == 12 ? 9 : 11;
-            const int hph = (stx >> 6) & 15, vph = (sty >> 6) & 15;
-            for (int k = tid; k < W * H; k += kT) {
-                int i = k >> LW, j = k & (W - 1);
-                int xi = ((stx >> 10) + j) - 3, yi = ((sty >> 10) + i) - 3;
-                int acc = 0;
-                for (int tt = 0; tt < 8; tt++) {
-                    int vc = c_subpel[3][vph][tt];
-                    if (!vc) continue;
-                    int yy = min(max(yi + tt, 0), P.h - 1);
-                    int hsum = 0;
-                    for (int u = 0; u < 8; u++) {
-                        int hc = c_subpel[3][hph][u];
-                        if (hc) hsum += hc * ld_px(P, hbd, yy, min(max(xi + u, 0), P.w - 1));
-                    }
-                    acc += vc * ((hsum + ((1 << r0) >> 1)) >> r0);
-                }
-                s.pred[k] = (uint16_t)min(max((acc + (1 << (r1 - 1))) >> r1, 0), maxv);
-            }
-        }
-        __syncthreads();
-        for (int k = tid; k < W * H; k += kT) {
+    if (t.mode == AV1G_INTRA_MODE_PALETTE) {
+        // predict_palette (cdf.rs:11907); indices checked on the host
+        const uint8_t* m = F.maps + t.palette_map;
+        for (int k = tid; k < W * H; k += G::N) {
             int i = k >> LW, j = k & (W - 1);
-            if (sy + i < P.h && sx + j < P.w) st_px(P, hbd, sy + i, sx + j, s.pred[k]);
+            tp[i * cs + j] = s.tu.palette_colors[m[i * t.palette_stride + j]];
         }
-        __syncthreads();
+        g.sync();
+    } else if (t.mode == AV1G_INTRA_MODE_INTRABC) {
+        // predict_intrabc_leaf_into_curr_frame (cdf.rs:19235): BILINEAR
+        // block_inter_prediction from the pre-filter plane at unit scale,
+        // start = (x << 10) + (((2 * mv) >> ss) << 6) + 32, clamped to the
+        // mi-padded plane (the reference's window clamp is the same set).
+        // The whole block is predicted before any of it is stored.
+        const int pss_x = pl ? F.ssx : 0, pss_y = pl ? F.ssy : 0;
+        const int stx = (sx << 10) + ((2 * t.mv[1]) >> pss_x) * 64 + 32;
+        const int sty = (sy << 10) + ((2 * t.mv[0]) >> pss_y) * 64 + 32;
+        const int r0 = bd == 12 ? 5 : 3, r1 = bd == 12 ? 9 : 11;
+        const int hph = (stx >> 6) & 15, vph = (sty >> 6) & 15;
+        for (int k = tid; k < W * H; k += G::N) {
+            int i = k >> LW, j = k & (W - 1);
+            int xi = ((stx >> 10) + j) - 3, yi = ((sty >> 10) + i) - 3;
+            int acc = 0;
+            for (int tt = 0; tt < 8; tt++) {
+                int vc = c_subpel[3][vph][tt];
+                if (!vc) continue;
+                int yy = min(max(yi + tt, 0), P.h - 1);
+                int hsum = 0;
+                for (int u = 0; u < 8; u++) {
+                    int hc = c_subpel[3][hph][u];
+                    if (hc) hsum += hc * rdp(F, c, cache, pl, yy, min(max(xi + u, 0), P.w - 1));
+                }
+                acc += vc * ((hsum + ((1 << r0) >> 1)) >> r0);
+            }
+            s.buf[k] = min(max((acc + (1 << (r1 - 1))) >> r1, 0), maxv);
+        }
+        g.sync();
+        for (int k = tid; k < W * H; k += G::N) tp[(k >> LW) * cs + (k & (W - 1))] = (uint16_t)s.buf[k];
+        g.sync();
     }
-    if ((t.flags & AV1G_INTRA_CFL) && t.plane > 0) {
+    if ((t.flags & AV1G_INTRA_CFL) && pl > 0) {
         // predict_chroma_from_luma_into_curr_frame (cdf.rs:17256-17340); luma
         // outside the luma plane reads as 0
-        const PlaneDev& Y = F.rf.planes[0];
+        const PlaneDev& Y = F.planes[0];
         const int ssx = F.ssx, ssy = F.ssy;
         const int cx = max((int)t.max_luma_w - (1 << ssx), 0), cy = max((int)t.max_luma_h - (1 << ssy), 0);
         long long part = 0;
-        for (int k = tid; k < W * H; k += kT) {
+        for (int k = tid; k < W * H; k += G::N) {
             int i = k >> LW, j = k & (W - 1);
             int ly = min((sy + i) << ssy, cy), lx = min((sx + j) << ssx, cx);
             int acc = 0;
             for (int ddy = 0; ddy <= ssy; ddy++)
                 for (int ddx = 0; ddx <= ssx; ddx++) {
                     int yy = ly + ddy, xx = lx + ddx;
-                    acc += (yy < Y.h && xx < Y.w) ? ld_px(Y, hbd, yy, xx) : 0;
+                    acc += (yy < Y.h && xx < Y.w) ? rdp(F, c, cache, 0, yy, xx) : 0;
                 }
             int v = acc << (3 - ssx - ssy);
             s.buf[k] = v;
             part += v;
         }
-        long long sum = block_sum(s, part);
+        long long sum = gsum(g, s, part);
         long long half = 1LL << (LW + LH - 1);
         long long avg = sum >= 0 ? (sum + half) >> (LW + LH) : -(((-sum) + half) >> (LW + LH));
-        const int maxv = (1 << bd) - 1;
-        for (int k = tid; k < W * H; k += kT) {
+        for (int k = tid; k < W * H; k += G::N) {
             int i = k >> LW, j = k & (W - 1);
             if (sy + i >= P.h || sx + j >= P.w) continue;
             long long d = (long long)t.cfl_alpha * (s.buf[k] - avg);
             long long sc = d >= 0 ? (d + 32) >> 6 : -(((-d) + 32) >> 6);
-            long long v = ld_px(P, hbd, sy + i, sx + j) + sc;
-            st_px(P, hbd, sy + i, sx + j, (int)min(max(v, 0LL), (long long)maxv));
+            uint16_t& px = tp[i * cs + j];
+            px = (uint16_t)min(max((long long)px + sc, 0LL), (long long)maxv);
         }
-        __syncthreads();
+        g.sync();
     }
-    if (t.flags & AV1G_INTRA_RESIDUAL) {
-        const int slot = tid / L, lane = tid % L;
-        recon_core<TX>(F.rf, t.res, slot == 0, lane, s.buf + slot * W * H);
-        __syncthreads();
+    if (has_res) residual_g<TX>(g, s, F, t.res, cf, tp, cs, P.w, P.h);
+}
+
+__device__ void run_small(const WarpG& g, WScr& s, const IntraFrame& F, const SbCtx& c, uint16_t* cache) {
+    const av1g_intra_tu t = s.tu;
+    switch (t.tx_size) {
+        case 0: intra_tu<0>(g, s, F, c, cache, t); break;
+        case 1: intra_tu<1>(g, s, F, c, cache, t); break;
+        case 2: intra_tu<2>(g, s, F, c, cache, t); break;
+        case 5: intra_tu<5>(g, s, F, c, cache, t); break;
+        case 6: intra_tu<6>(g, s, F, c, cache, t); break;
+        case 7: intra_tu<7>(g, s, F, c, cache, t); break;
+        case 8: intra_tu<8>(g, s, F, c, cache, t); break;
+        case 13: intra_tu<13>(g, s, F, c, cache, t); break;
+        case 14: intra_tu<14>(g, s, F, c, cache, t); break;
+        case 15: intra_tu<15>(g, s, F, c, cache, t); break;
+        default: intra_tu<16>(g, s, F, c, cache, t); break;
+    }
+}
+
+__device__ void run_large(const CtaG& g, CScr& s, const IntraFrame& F, const SbCtx& c, uint16_t* cache) {
+    const av1g_intra_tu t = s.tu;
+    switch (t.tx_size) {
+        case 3: intra_tu<3>(g, s, F, c, cache, t); break;
+        case 4: intra_tu<4>(g, s, F, c, cache, t); break;
+        case 9: intra_tu<9>(g, s, F, c, cache, t); break;
+        case 10: intra_tu<10>(g, s, F, c, cache, t); break;
+        case 11: intra_tu<11>(g, s, F, c, cache, t); break;
+        case 12: intra_tu<12>(g, s, F, c, cache, t); break;
+        case 17: intra_tu<17>(g, s, F, c, cache, t); break;
+        default: intra_tu<18>(g, s, F, c, cache, t); break;
+    }
+}
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ long long gtimer() {
+    long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// The superblock copy <-> HBM, two samples per thread (plane widths are even,
+// superblock origins and row pitches keep the pairs aligned).
+template <bool LOAD>
+__device__ void move_sb(const IntraFrame& F, const SbCtx& c, uint16_t* cache) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int p = 0; p < F.np; p++) {
+        const PlaneDev& P = F.planes[p];
+        const int rows = min(c.h[p], P.h - c.y0[p]), pairs = min(c.w[p], P.w - c.x0[p]) >> 1;
+        uint16_t* cp = cache + c.off[p];
+        for (int r = warp; r < rows; r += kNW) {
+            uint8_t* row = P.p + (size_t)(c.y0[p] + r) * P.stride;
+            uint16_t* crow = cp + r * c.w[p];
+            for (int q = lane; q < pairs; q += 32) {
+                if (F.hbd) {
+                    uint32_t* g = reinterpret_cast<uint32_t*>(row) + (c.x0[p] >> 1) + q;
+                    if (LOAD) {
+                        const uint32_t v = *g;
+                        crow[2 * q] = (uint16_t)v;
+                        crow[2 * q + 1] = (uint16_t)(v >> 16);
+                    } else {
+                        *g = (uint32_t)crow[2 * q] | ((uint32_t)crow[2 * q + 1] << 16);
+                    }
+                } else {
+                    uint16_t* g = reinterpret_cast<uint16_t*>(row + c.x0[p]) + q;
+                    if (LOAD) {
+                        const uint16_t v = *g;
+                        crow[2 * q] = v & 0xff;
+                        crow[2 * q + 1] = v >> 8;
+                    } else {
+                        *g = (uint16_t)(crow[2 * q] | (crow[2 * q + 1] << 8));
+                    }
+                }
+            }
+        }
     }
 }
 
 __global__ void __launch_bounds__(kT) intra_kernel(const IntraFrame* __restrict__ frames,
                                                    const av1g_intra_tu* __restrict__ tus,
-                                                   const IntraItem* __restrict__ items, int nitems) {
-    __shared__ Smem s;
-    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-        const IntraItem item = items[it];
-        const IntraFrame& F = frames[item.frame];
-        for (int k = item.first; k < item.first + item.count; k++) {
-            __syncthreads();
-            if (threadIdx.x == 0) s.tu = tus[k];
-            __syncthreads();
-            const av1g_intra_tu t = s.tu;
-            switch (t.tx_size) {
-                case 0: intra_tu<0>(s, F, t); break;
-                case 1: intra_tu<1>(s, F, t); break;
-                case 2: intra_tu<2>(s, F, t); break;
-                case 3: intra_tu<3>(s, F, t); break;
-                case 4: intra_tu<4>(s, F, t); break;
-                case 5: intra_tu<5>(s, F, t); break;
-                case 6: intra_tu<6>(s, F, t); break;
-                case 7: intra_tu<7>(s, F, t); break;
-                case 8: intra_tu<8>(s, F, t); break;
-                case 9: intra_tu<9>(s, F, t); break;
-                case 10: intra_tu<10>(s, F, t); break;
-                case 11: intra_tu<11>(s, F, t); break;
-                case 12: intra_tu<12>(s, F, t); break;
-                case 13: intra_tu<13>(s, F, t); break;
-                case 14: intra_tu<14>(s, F, t); break;
-                case 15: intra_tu<15>(s, F, t); break;
-                case 16: intra_tu<16>(s, F, t); break;
-                case 17: intra_tu<17>(s, F, t); break;
-                default: intra_tu<18>(s, F, t); break;
+                                                   const SbItem* __restrict__ items, const int2* __restrict__ lvs,
+                                                   const int* __restrict__ deps, int* done, int* ctl, int nitems) {
+    extern __shared__ __align__(16) uint8_t dsm[];
+    Shared& S = *reinterpret_cast<Shared*>(dsm);
+    uint16_t* cache = reinterpret_cast<uint16_t*>(dsm + kSharedBytes);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) S.idx = atomicAdd(&ctl[0], 1);
+        __syncthreads();
+        const int idx = S.idx;
+        if (idx >= nitems) return;
+        const SbItem it = items[idx];
+        const IntraFrame& F = frames[it.frame];
+        if (tid == 0) {
+            int off = 0;
+            for (int p = 0; p < 3; p++) {
+                const int ssx = p ? F.ssx : 0, ssy = p ? F.ssy : 0;
+                S.sb.x0[p] = it.x0 >> ssx;
+                S.sb.y0[p] = it.y0 >> ssy;
+                S.sb.w[p] = (1 << it.log2sb) >> ssx;
+                S.sb.h[p] = (1 << it.log2sb) >> ssy;
+                S.sb.off[p] = off;
+                off += p < F.np ? S.sb.w[p] * S.sb.h[p] : 0;
             }
+        }
+        __syncthreads();
+        // the superblock's own area is written only by its own TUs: stage it
+        // before waiting
+        move_sb<true>(F, S.sb, cache);
+        for (int q = tid; q < it.ndep; q += kT) {
+            const int d = __ldg(deps + it.dep_first + q);
+            const long long t0 = gtimer();
+            while (ld_acquire(done + d) == 0) {
+                if (*(volatile int*)(ctl + 1)) break;
+                if (gtimer() - t0 > kWaitNs) {
+                    atomicOr(&g_wave_fault, 1u);
+                    atomicExch(ctl + 1, 1);
+                    break;
+                }
+                __nanosleep(128);
+            }
+        }
+        __syncthreads();
+        if (tid == 0) S.abort_seen = *(volatile int*)(ctl + 1);
+        __syncthreads();
+        if (!S.abort_seen) {
+            for (int L0 = 0; L0 < it.nlv; L0 += kLvChunk) {
+                const int n = min(kLvChunk, it.nlv - L0);
+                for (int q = tid; q <= n; q += kT) S.lv[q] = lvs[it.lv_first + L0 + q];
+                __syncthreads();
+                for (int L = 0; L < n; L++) {
+                    const int b = S.lv[L].x, m = S.lv[L].y, e = S.lv[L + 1].x;
+                    for (int k = b + warp; k < m; k += kNW) {
+                        WScr& ws = S.s.w[warp];
+                        if (lane < 16)
+                            reinterpret_cast<uint32_t*>(&ws.tu)[lane] =
+                                __ldg(reinterpret_cast<const uint32_t*>(tus + k) + lane);
+                        __syncwarp();
+                        run_small(WarpG{lane}, ws, F, S.sb, cache);
+                        __syncwarp();
+                    }
+                    if (m < e) {
+                        __syncthreads();
+                        for (int k = m; k < e; k++) {
+                            if (tid < 16)
+                                reinterpret_cast<uint32_t*>(&S.s.c.tu)[tid] =
+                                    __ldg(reinterpret_cast<const uint32_t*>(tus + k) + tid);
+                            __syncthreads();
+                            run_large(CtaG{tid}, S.s.c, F, S.sb, cache);
+                            __syncthreads();
+                        }
+                    }
+                    __syncthreads();
+                }
+            }
+        }
+        __syncthreads();
+        move_sb<false>(F, S.sb, cache);
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            atomicExch(done + idx, 1);
         }
     }
 }
 
+// Pinned host mirror of g_wave_fault, per device.
+volatile unsigned* fault_mirror(int dev) {
+    static std::mutex mu;
+    static std::unordered_map<int, unsigned*> words;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = words.find(dev);
+    if (it != words.end()) return it->second;
+    unsigned* w = nullptr;
+    if (cudaHostAlloc((void**)&w, sizeof(unsigned), cudaHostAllocDefault) != cudaSuccess) return nullptr;
+    *w = 0;
+    words[dev] = w;
+    return w;
+}
+
 }  // namespace
 
-// Host side of av1g_run_intra: validation, superblock grouping, level order, launches.
+
+// Host side of av1g_run_intra: the plan (intra_plan.cu), its upload, one launch.
 av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t st, std::string& err) {
-    std::vector<IntraFrame> frames(n);
-    std::vector<av1g_intra_tu> all;
-    std::vector<IntraItem> items;
-    std::vector<std::pair<size_t, uint32_t>> wedge_pack;  // (TU index, packed wedge window)
-    std::vector<uint8_t> maps;            // palette colour indices of all jobs
-    std::vector<size_t> map_base(n, 0);
-    for (int i = 0; i < n; i++) {
-        const av1g_intra_job& j = jobs[i];
-        if (!j.hdr || !j.quant || j.num_tus < 0 || (j.num_tus > 0 && !j.tus) || (j.sb_size != 64 && j.sb_size != 128) ||
-            j.palette_map_bytes < 0 || (j.palette_map_bytes > 0 && !j.palette_maps)) {
-            err = "intra job " + std::to_string(i) + ": missing header/quantizer/TUs/maps or superblock size not 64/128";
-            return AV1G_EINVAL;
-        }
-        const av1g_frame_header& h = *j.hdr;
-        if (h.bit_depth != 8 && h.bit_depth != 10 && h.bit_depth != 12) {
-            err = "intra job " + std::to_string(i) + ": bit depth";
-            return AV1G_EINVAL;
-        }
-        IntraFrame& F = frames[i];
-        memset(&F, 0, sizeof F);
-        F.rf.bd = h.bit_depth;
-        F.rf.hbd = h.bit_depth > 8;
-        F.rf.q = *j.quant;
-        F.rf.coeffs = j.coeffs;
-        F.ssx = h.subsampling_x;
-        F.ssy = h.subsampling_y;
-        for (int p = 0; p < h.num_planes; p++) {
-            int sx = p ? h.subsampling_x : 0, sy = p ? h.subsampling_y : 0;
-            int pw = (h.mi_cols * 4) >> sx, ph = (h.mi_rows * 4) >> sy;
-            const av1g_plane& pl = j.planes[p];
-            if (!pl.data || pl.width < pw || pl.height < ph || pl.stride < pw * (F.rf.hbd ? 2 : 1) || (pl.stride & 15)) {
-                err = "intra job " + std::to_string(i) + ": plane " + std::to_string(p);
-                return AV1G_EINVAL;
-            }
-            F.rf.planes[p] = PlaneDev{(uint8_t*)pl.data, pl.stride, pw, ph};
-        }
-        map_base[i] = maps.size();
-        if (j.palette_map_bytes > 0) maps.insert(maps.end(), j.palette_maps, j.palette_maps + j.palette_map_bytes);
-        // superblocks in decode order, and the intra block copy windows
-        struct Sb {
-            int sbx, sby, seq;
-        };
-        std::vector<Sb> sbs;
-        std::unordered_map<long long, int> sb_index;
-        struct Bc {
-            int sb, x0, y0, x1, y1;  // luma-sample window, inclusive
-        };
-        std::vector<Bc> bcs;
-        int base = (int)all.size();
-        int first_item = (int)items.size();
-        long long prev = -1;
-        for (int k = 0; k < j.num_tus; k++) {
-            const av1g_intra_tu& t = j.tus[k];
-            bool res = t.flags & AV1G_INTRA_RESIDUAL;
-            bool fi_ok = !(t.plane == 0 && t.filter_intra_mode < 5) || (t.tx_size != 4 && t.tx_size != 11 &&
-                                                                        t.tx_size != 12 && t.tx_size != 17 &&
-                                                                        t.tx_size != 18);
-            if (t.tx_size >= 19 || t.plane >= h.num_planes || !fi_ok ||
-                (res && (t.res.tx_size != t.tx_size || t.res.plane != t.plane || t.res.x != t.x || t.res.y != t.y ||
-                         t.res.tx_type >= 16 || !j.coeffs))) {
-                err = "intra job " + std::to_string(i) + ": TU " + std::to_string(k) + " is malformed";
-                return AV1G_EINVAL;
-            }
-            const int tw = kTxW[t.tx_size], th = kTxH[t.tx_size];
-            const int pss_x = t.plane ? h.subsampling_x : 0, pss_y = t.plane ? h.subsampling_y : 0;
-            if (t.interintra) {
-                // the intra half of an inter-intra block: an II mode's intra
-                // mode (DC, V, H, SMOOTH) over the whole block, then the blend
-                static const uint8_t ii_to_intra[4] = {0, 1, 2, 9};
-                const av1g_plane& sp = j.interintra_in[t.plane];
-                wedge::Orient o{};
-                bool ok = t.interintra <= 2 && t.interintra_mode <= 3 && t.mode == ii_to_intra[t.interintra_mode] &&
-                          t.filter_intra_mode >= 5 && !(t.flags & AV1G_INTRA_CFL) && sp.data &&
-                          sp.width >= F.rf.planes[t.plane].w && sp.height >= F.rf.planes[t.plane].h &&
-                          sp.stride >= F.rf.planes[t.plane].w * (F.rf.hbd ? 2 : 1) && !(sp.stride & 15);
-                if (ok && t.interintra == 2)
-                    ok = wedge::orient(t.mi_size, t.wedge_index, 0, tw, th, pss_x, pss_y, o);
-                if (!ok) {
-                    err = "intra job " + std::to_string(i) + ": inter-intra TU " + std::to_string(k) + " is malformed";
-                    return AV1G_EINVAL;
-                }
-                F.side[t.plane] = PlaneDev{(uint8_t*)sp.data, sp.stride, F.rf.planes[t.plane].w, F.rf.planes[t.plane].h};
-                // the device copy of the TU carries the wedge window in
-                // palette_map (an inter-intra TU has no palette)
-                wedge_pack.emplace_back((size_t)(base + k), (uint32_t)o.dir | ((uint32_t)o.xoff << 8) |
-                                                                ((uint32_t)o.yoff << 16) | ((uint32_t)o.invert << 24));
-            }
-            if (t.mode == AV1G_INTRA_MODE_PALETTE) {
-                // predict_palette's checks (cdf.rs:11907-11960)
-                long long last = (long long)t.palette_map + (long long)(th - 1) * t.palette_stride + (tw - 1);
-                bool ok = t.palette_size >= 1 && t.palette_size <= 8 && t.palette_stride >= tw &&
-                          last < j.palette_map_bytes;
-                for (int r = 0; ok && r < th; r++)
-                    for (int c = 0; ok && c < tw; c++)
-                        ok = j.palette_maps[t.palette_map + (long long)r * t.palette_stride + c] < t.palette_size;
-                if (!ok) {
-                    err = "intra job " + std::to_string(i) + ": palette TU " + std::to_string(k) + " is malformed";
-                    return AV1G_EINVAL;
-                }
-            }
-            int lx = t.x << pss_x, ly = t.y << pss_y;
-            long long sb = ((long long)(ly / j.sb_size) << 32) | (unsigned)(lx / j.sb_size);
-            if (sb != prev) {
-                if (sb_index.count(sb)) {
-                    err = "intra job " + std::to_string(i) + ": TUs of a superblock are not contiguous in decode order";
-                    return AV1G_EINVAL;
-                }
-                int sbx = lx / j.sb_size, sby = ly / j.sb_size;
-                sb_index[sb] = (int)sbs.size();
-                sbs.push_back(Sb{sbx, sby, (int)sbs.size()});
-                items.push_back(IntraItem{i, base + k, 0, 0});
-                prev = sb;
-            }
-            if (t.mode == AV1G_INTRA_MODE_INTRABC) {
-                if (std::abs((int)t.mv[0]) >= (1 << 14) || std::abs((int)t.mv[1]) >= (1 << 14)) {
-                    err = "intra job " + std::to_string(i) + ": intra block copy TU " + std::to_string(k) +
-                          " has a motion vector out of range";
-                    return AV1G_EINVAL;
-                }
-                // the window the BILINEAR filter reads, in luma samples
-                int pw = (h.mi_cols * 4) >> pss_x, ph = (h.mi_rows * 4) >> pss_y;
-                int stx = (t.x << 10) + ((2 * t.mv[1]) >> pss_x) * 64 + 32;
-                int sty = (t.y << 10) + ((2 * t.mv[0]) >> pss_y) * 64 + 32;
-                int x0 = std::min(std::max((stx >> 10) - 3, 0), pw - 1);
-                int x1 = std::min(std::max((stx >> 10) + tw - 1 + 4, 0), pw - 1);
-                int y0 = std::min(std::max((sty >> 10) - 3, 0), ph - 1);
-                int y1 = std::min(std::max((sty >> 10) + th - 1 + 4, 0), ph - 1);
-                bcs.push_back(Bc{sb_index[sb], x0 << pss_x, y0 << pss_y, ((x1 + 1) << pss_x) - 1,
-                                 ((y1 + 1) << pss_y) - 1});
-            }
-            items.back().count++;
-            all.push_back(t);
-        }
-        // Superblock (c, r) gets level c + k r.  k = 2 covers the intra edge
-        // reads (above-right is one superblock up and right).  An intra block
-        // copy may read any earlier superblock, so every superblock its window
-        // touches must sit on the same side of it in level order as in decode
-        // order; steeper slopes follow the spec's intra-block-copy wavefront
-        // delay, and decode order itself (one superblock per level) always
-        // reproduces sequential decoding.
-        auto level_ok = [&](auto level) {
-            for (const Bc& b : bcs) {
-                const Sb& cur = sbs[b.sb];
-                for (int by = b.y0 / j.sb_size; by <= b.y1 / j.sb_size; by++)
-                    for (int bx = b.x0 / j.sb_size; bx <= b.x1 / j.sb_size; bx++) {
-                        auto it = sb_index.find(((long long)by << 32) | (unsigned)bx);
-                        if (it == sb_index.end() || it->second == b.sb) continue;
-                        const Sb& o = sbs[it->second];
-                        int lo = level(o), lc = level(cur);
-                        if (lo == lc || (o.seq < cur.seq) != (lo < lc)) return false;
-                    }
-            }
-            return true;
-        };
-        int slope = 0;
-        for (int k : {2, 3, 4, 5, 6, 8})
-            if (level_ok([k](const Sb& b) { return b.sbx + k * b.sby; })) {
-                slope = k;
-                break;
-            }
-        for (int q = first_item; q < (int)items.size(); q++) {
-            const Sb& b = sbs[q - first_item];
-            items[q].level = slope ? b.sbx + slope * b.sby : b.seq;
-        }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    volatile unsigned* fault = fault_mirror(dev);
+    if (fault && *fault) {
+        err = "an earlier intra launch on this device gave up waiting for a superblock";
+        return AV1G_EDEVICE;
     }
-    if (items.empty()) return AV1G_OK;
-    for (const auto& wp : wedge_pack) all[wp.first].palette_map = wp.second;
-    std::stable_sort(items.begin(), items.end(), [](const IntraItem& a, const IntraItem& b) { return a.level < b.level; });
-    size_t off_tus = (sizeof(IntraFrame) * n + 255) & ~(size_t)255;
-    size_t off_items = (off_tus + sizeof(av1g_intra_tu) * all.size() + 255) & ~(size_t)255;
-    size_t off_maps = (off_items + sizeof(IntraItem) * items.size() + 255) & ~(size_t)255;
-    size_t bytes = off_maps + maps.size();
-    uint8_t* dev = nullptr;
-    cudaError_t e = cudaMallocAsync((void**)&dev, bytes, st);
+    IntraPlan plan;
+    av1g_status rc = intra_plan(jobs, n, plan, err);
+    if (rc != AV1G_OK || plan.items.empty()) return rc;
+    const int nitems = (int)plan.items.size();
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t off_tus = al(sizeof(IntraFrame) * n);
+    const size_t off_items = al(off_tus + sizeof(av1g_intra_tu) * plan.tus.size());
+    const size_t off_lv = al(off_items + sizeof(SbItem) * plan.items.size());
+    const size_t off_deps = al(off_lv + sizeof(int2) * plan.lvtab.size());
+    const size_t off_done = al(off_deps + sizeof(int) * plan.deps.size());
+    const size_t off_ctl = al(off_done + sizeof(int) * plan.items.size());
+    const size_t off_maps = al(off_ctl + 2 * sizeof(int));
+    const size_t bytes = off_maps + plan.maps.size();
+    uint8_t* dev_buf = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&dev_buf, bytes, st);
     if (e != cudaSuccess) {
         err = std::string("cudaMallocAsync: ") + cudaGetErrorString(e);
         return AV1G_EDEVICE;
     }
-    for (int i = 0; i < n; i++) frames[i].maps = dev + off_maps + map_base[i];
+    for (int i = 0; i < n; i++) plan.frames[i].maps = dev_buf + off_maps + plan.map_base[i];
     std::vector<uint8_t> host(bytes);
-    memcpy(host.data(), frames.data(), sizeof(IntraFrame) * n);
-    memcpy(host.data() + off_tus, all.data(), sizeof(av1g_intra_tu) * all.size());
-    memcpy(host.data() + off_items, items.data(), sizeof(IntraItem) * items.size());
-    if (!maps.empty()) memcpy(host.data() + off_maps, maps.data(), maps.size());
-    e = upload(dev, host.data(), bytes, st);
-    const IntraFrame* df = (const IntraFrame*)dev;
-    const av1g_intra_tu* dt = (const av1g_intra_tu*)(dev + off_tus);
-    const IntraItem* di = (const IntraItem*)(dev + off_items);
-    for (size_t lo = 0; e == cudaSuccess && lo < items.size();) {
-        size_t hi = lo;
-        while (hi < items.size() && items[hi].level == items[lo].level) hi++;
-        int cnt = (int)(hi - lo);
-        intra_kernel<<<cnt, kT, 0, st>>>(df, dt, di + lo, cnt);
+    memcpy(host.data(), plan.frames.data(), sizeof(IntraFrame) * n);
+    memcpy(host.data() + off_tus, plan.tus.data(), sizeof(av1g_intra_tu) * plan.tus.size());
+    memcpy(host.data() + off_items, plan.items.data(), sizeof(SbItem) * plan.items.size());
+    memcpy(host.data() + off_lv, plan.lvtab.data(), sizeof(int2) * plan.lvtab.size());
+    if (!plan.deps.empty()) memcpy(host.data() + off_deps, plan.deps.data(), sizeof(int) * plan.deps.size());
+    memset(host.data() + off_done, 0, off_maps - off_done);  // done flags, claim counter, abort flag
+    if (!plan.maps.empty()) memcpy(host.data() + off_maps, plan.maps.data(), plan.maps.size());
+    e = upload(dev_buf, host.data(), bytes, st);
+    const size_t smem = kSharedBytes + plan.cache_bytes;
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(intra_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0, sms = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, intra_kernel, kT, smem);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) {
+        const int grid = std::max(1, std::min(nitems, std::max(per_sm, 1) * sms));
+        intra_kernel<<<grid, kT, smem, st>>>(
+            (const IntraFrame*)dev_buf, (const av1g_intra_tu*)(dev_buf + off_tus), (const SbItem*)(dev_buf + off_items),
+            (const int2*)(dev_buf + off_lv), (const int*)(dev_buf + off_deps), (int*)(dev_buf + off_done),
+            (int*)(dev_buf + off_ctl), nitems);
         e = cudaGetLastError();
-        lo = hi;
     }
-    cudaFreeAsync(dev, st);
+    if (e == cudaSuccess && fault)
+        e = cudaMemcpyFromSymbolAsync((void*)fault, g_wave_fault, sizeof(unsigned), 0, cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(dev_buf, st);
     if (e != cudaSuccess) {
         err = std::string("intra launch: ") + cudaGetErrorString(e);
         return AV1G_EDEVICE;
