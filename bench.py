@@ -433,6 +433,9 @@ def run_serving(args, local):
         out[name] = {"value": fps, "unit": UNIT, "max_frames_per_step": mb, "lanes": lanes,
                      "steps": s1.steps_done - s0.steps_done,
                      "engine_host_ms_per_frame": (s1.host_ms - s0.host_ms) / nf,
+                     "engine_host_ms_per_frame_by_part": {
+                         k: (s1.host_stage_ms[i] - s0.host_stage_ms[i]) / nf for i, k in enumerate(
+                             ["uploads", "inter", "residual", "intra", "post_filter", "slots_outputs"])},
                      "device_ms_per_frame": (s1.device_ms - s0.device_ms) / nf}
 
     # Poisson arrivals at 60% of the batched capacity

@@ -49,6 +49,8 @@ constexpr int kT = 128;             // threads per CTA
 constexpr int kNW = kT / 32;        // warps per CTA
 constexpr int kSmallPx = kIntraSmallPx;
 constexpr int kLvChunk = 256;       // level-table entries staged at a time
+constexpr int kTuWin = 128;         // TU records staged at a time
+constexpr int kWaitWin = 64;        // waits staged per superblock
 constexpr long long kWaitNs = 2000000000LL;
 
 __constant__ AV1T_MODE_TO_ANGLE_TYPE c_mode_angle AV1T_MODE_TO_ANGLE_DIMS = AV1T_MODE_TO_ANGLE_INIT;
@@ -124,10 +126,19 @@ struct alignas(16) Shared {
         WScr w[kNW];
         CScr c;
     } s;
+    IntraFrame fr;  // the superblock's frame record
     int2 lv[kLvChunk + 1];
+    int4 wv[kWaitWin];
     SbCtx sb;
     int idx, abort_seen;
 };
+static_assert(sizeof(IntraFrame) % 4 == 0, "frame record copied as words");
+
+// The batch's residual blocks (intra_res_kernel); an intra TU's device record
+// carries its block's offset in res.coeff_offset.
+struct Pool {
+    const int32_t* res;
+}; 
 constexpr size_t kSharedBytes = (sizeof(Shared) + 15) & ~(size_t)15;
 
 __device__ __forceinline__ const uint8_t* sm_weights(int log2n) {
@@ -223,14 +234,13 @@ __device__ void edge_upsample(const G& g, S& s, uint16_t* e, int n, int bd) {
     g.sync();
 }
 
-// Dequantize (dequantize_step1, cdf.rs:13655-13703), inverse transform
-// (transform.rs:707-789) and merge (curr_frame_step3_merge, cdf.rs:17398-17470)
-// one TU into the shared-memory copy of its superblock.  cf holds the compact
-// levels, cf[q] == level[g.r + q * G::N]; tp is the TU's top-left sample in
-// the copy (row pitch cs); samples outside the plane are left alone.
+// Dequantize (dequantize_step1, cdf.rs:13655-13703) and inverse transform
+// (transform.rs:707-789) one TU's residual, stored as w*h int32 in sample
+// orientation (the FLIPADST flips of curr_frame_step3_merge, cdf.rs:17398-17470,
+// already applied).  cf holds the compact levels, cf[q] == level[g.r + q * G::N].
 template <int TX, class G, class S>
-__device__ __forceinline__ void residual_g(const G& g, S& s, const IntraFrame& R, const av1g_tu& tu, const int* cf, uint16_t* tp,
-                           int cs, int pw, int ph) {
+__device__ __forceinline__ void residual_store(const G& g, S& s, const IntraFrame& R, const av1g_tu& tu, const int* cf,
+                                               int32_t* out) {
     constexpr int W = kTxW[TX], H = kTxH[TX];
     constexpr int LW = ilog2<W>(), LH = ilog2<H>();
     constexpr int TW = W < 32 ? W : 32, TH = H < 32 ? H : 32, NC = TW * TH, K = (NC + G::N - 1) / G::N;
@@ -315,29 +325,38 @@ __device__ __forceinline__ void residual_g(const G& g, S& s, const IntraFrame& R
         const bool fud = tt == 4 || tt == 8 || tt == 14 || tt == 6;
         const bool flr = tt == 5 || tt == 7 || tt == 15 || tt == 6;
         const int x = flr ? W - 1 - lane : lane;
-        const int maxv = (1 << bd) - 1;
-        if (tu.x + x < pw) {
 #pragma unroll
-            for (int i = 0; i < H; i++) {
-                const int y = fud ? H - 1 - i : i;
-                if (tu.y + y >= ph) continue;
-                const int res = csh ? (t[i] + (1 << (csh - 1))) >> csh : t[i];
-                uint16_t& px = tp[y * cs + x];
-                px = (uint16_t)min(max((int)px + res, 0), maxv);
-            }
+        for (int i = 0; i < H; i++) {
+            const int y = fud ? H - 1 - i : i;
+            out[y * W + x] = csh ? (t[i] + (1 << (csh - 1))) >> csh : t[i];
         }
     }
     g.sync();
+}
+
+// One residual task: its compact levels, then residual_store.
+template <int TX, class G, class S>
+__device__ __forceinline__ void residual_task(const G& g, S& s, const IntraFrame& F, const av1g_tu& tu, int32_t* out) {
+    constexpr int W = kTxW[TX], H = kTxH[TX];
+    constexpr int TW = W < 32 ? W : 32, TH = H < 32 ? H : 32, NC = TW * TH, K = (NC + G::N - 1) / G::N;
+    int cf[K];
+    const int32_t* lv = F.coeffs + tu.coeff_offset;
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+        const int k = g.r + q * G::N;
+        cf[q] = k < NC ? __ldg(lv + k) : 0;
+    }
+    residual_store<TX>(g, s, F, tu, cf, out);
 }
 
 // One TU: prediction (+ inter-intra blend, + CfL), then the residual, all on
 // the shared-memory copy of the superblock.
 template <int TX, class G, class S>
 __device__ void intra_tu(const G& g, S& s, const IntraFrame& F, const SbCtx& c, uint16_t* cache,
-                         const av1g_intra_tu& t) {
+                         const av1g_intra_tu* rec, Pool pool) {
+    const av1g_intra_tu t = *rec;
     constexpr int W = kTxW[TX], H = kTxH[TX];
     constexpr int LW = ilog2<W>(), LH = ilog2<H>();
-    constexpr int TW = W < 32 ? W : 32, TH = H < 32 ? H : 32, NC = TW * TH, K = (NC + G::N - 1) / G::N;
     const int tid = g.r;
     const int pl = t.plane;
     const PlaneDev& P = F.planes[pl];
@@ -346,14 +365,16 @@ __device__ void intra_tu(const G& g, S& s, const IntraFrame& F, const SbCtx& c, 
     const int cs = c.w[pl];
     uint16_t* tp = cache + c.off[pl] + (sy - c.y0[pl]) * cs + (sx - c.x0[pl]);
     const bool has_res = t.flags & AV1G_INTRA_RESIDUAL;
-    // the compact levels, fetched first so that their latency overlaps the prediction
-    int cf[K];
-    {
-        const int32_t* lv = F.coeffs + (has_res ? t.res.coeff_offset : 0);
+    // a warp fetches its residual first, so that the latency overlaps the
+    // prediction (the CTA path reads it at the merge)
+    const int32_t* rp = pool.res + t.res.coeff_offset;
+    constexpr int KP = G::N == 32 ? (W * H + 31) / 32 : 1;
+    int rv[KP];
+    if constexpr (G::N == 32) {
 #pragma unroll
-        for (int q = 0; q < K; q++) {
-            const int k = tid + q * G::N;
-            cf[q] = (has_res && k < NC) ? __ldg(lv + k) : 0;
+        for (int q = 0; q < KP; q++) {
+            const int k = tid + q * 32;
+            rv[q] = (has_res && k < W * H) ? __ldg(rp + k) : 0;
         }
     }
     const int maxv = (1 << bd) - 1;
@@ -515,7 +536,7 @@ __device__ void intra_tu(const G& g, S& s, const IntraFrame& F, const SbCtx& c, 
         const uint8_t* m = F.maps + t.palette_map;
         for (int k = tid; k < W * H; k += G::N) {
             int i = k >> LW, j = k & (W - 1);
-            tp[i * cs + j] = s.tu.palette_colors[m[i * t.palette_stride + j]];
+            tp[i * cs + j] = rec->palette_colors[m[i * t.palette_stride + j]];
         }
         g.sync();
     } else if (t.mode == AV1G_INTRA_MODE_INTRABC) {
@@ -583,37 +604,58 @@ __device__ void intra_tu(const G& g, S& s, const IntraFrame& F, const SbCtx& c, 
         }
         g.sync();
     }
-    if (has_res) residual_g<TX>(g, s, F, t.res, cf, tp, cs, P.w, P.h);
-}
-
-__device__ void run_small(const WarpG& g, WScr& s, const IntraFrame& F, const SbCtx& c, uint16_t* cache) {
-    const av1g_intra_tu t = s.tu;
-    switch (t.tx_size) {
-        case 0: intra_tu<0>(g, s, F, c, cache, t); break;
-        case 1: intra_tu<1>(g, s, F, c, cache, t); break;
-        case 2: intra_tu<2>(g, s, F, c, cache, t); break;
-        case 5: intra_tu<5>(g, s, F, c, cache, t); break;
-        case 6: intra_tu<6>(g, s, F, c, cache, t); break;
-        case 7: intra_tu<7>(g, s, F, c, cache, t); break;
-        case 8: intra_tu<8>(g, s, F, c, cache, t); break;
-        case 13: intra_tu<13>(g, s, F, c, cache, t); break;
-        case 14: intra_tu<14>(g, s, F, c, cache, t); break;
-        case 15: intra_tu<15>(g, s, F, c, cache, t); break;
-        default: intra_tu<16>(g, s, F, c, cache, t); break;
+    if (has_res) {
+        // curr_frame_step3_merge (cdf.rs:17398-17470): Clip1(pred + residual)
+#pragma unroll
+        for (int q = 0; q < (G::N == 32 ? KP : (W * H + G::N - 1) / G::N); q++) {
+            const int k = tid + q * G::N;
+            if (k >= W * H) break;
+            const int i = k >> LW, j = k & (W - 1);
+            if (sy + i >= P.h || sx + j >= P.w) continue;
+            int v;
+            if constexpr (G::N == 32) v = rv[q];
+            else v = __ldg(rp + k);
+            uint16_t& px = tp[i * cs + j];
+            px = (uint16_t)min(max((int)px + v, 0), maxv);
+        }
+        g.sync();
+    }
+    // the TU's final samples to HBM: other superblocks read them once this
+    // level is published
+    for (int k = tid; k < W * H; k += G::N) {
+        const int i = k >> LW, j = k & (W - 1);
+        if (sy + i < P.h && sx + j < P.w) st_px(P, hbd, sy + i, sx + j, tp[i * cs + j]);
     }
 }
 
-__device__ void run_large(const CtaG& g, CScr& s, const IntraFrame& F, const SbCtx& c, uint16_t* cache) {
-    const av1g_intra_tu t = s.tu;
-    switch (t.tx_size) {
-        case 3: intra_tu<3>(g, s, F, c, cache, t); break;
-        case 4: intra_tu<4>(g, s, F, c, cache, t); break;
-        case 9: intra_tu<9>(g, s, F, c, cache, t); break;
-        case 10: intra_tu<10>(g, s, F, c, cache, t); break;
-        case 11: intra_tu<11>(g, s, F, c, cache, t); break;
-        case 12: intra_tu<12>(g, s, F, c, cache, t); break;
-        case 17: intra_tu<17>(g, s, F, c, cache, t); break;
-        default: intra_tu<18>(g, s, F, c, cache, t); break;
+__device__ void run_small(const WarpG& g, WScr& s, const IntraFrame& F, const SbCtx& c, uint16_t* cache,
+                          const av1g_intra_tu* rec, Pool pool) {
+    switch (rec->tx_size) {
+        case 0: intra_tu<0>(g, s, F, c, cache, rec, pool); break;
+        case 1: intra_tu<1>(g, s, F, c, cache, rec, pool); break;
+        case 2: intra_tu<2>(g, s, F, c, cache, rec, pool); break;
+        case 5: intra_tu<5>(g, s, F, c, cache, rec, pool); break;
+        case 6: intra_tu<6>(g, s, F, c, cache, rec, pool); break;
+        case 7: intra_tu<7>(g, s, F, c, cache, rec, pool); break;
+        case 8: intra_tu<8>(g, s, F, c, cache, rec, pool); break;
+        case 13: intra_tu<13>(g, s, F, c, cache, rec, pool); break;
+        case 14: intra_tu<14>(g, s, F, c, cache, rec, pool); break;
+        case 15: intra_tu<15>(g, s, F, c, cache, rec, pool); break;
+        default: intra_tu<16>(g, s, F, c, cache, rec, pool); break;
+    }
+}
+
+__device__ void run_large(const CtaG& g, CScr& s, const IntraFrame& F, const SbCtx& c, uint16_t* cache,
+                          const av1g_intra_tu* rec, Pool pool) {
+    switch (rec->tx_size) {
+        case 3: intra_tu<3>(g, s, F, c, cache, rec, pool); break;
+        case 4: intra_tu<4>(g, s, F, c, cache, rec, pool); break;
+        case 9: intra_tu<9>(g, s, F, c, cache, rec, pool); break;
+        case 10: intra_tu<10>(g, s, F, c, cache, rec, pool); break;
+        case 11: intra_tu<11>(g, s, F, c, cache, rec, pool); break;
+        case 12: intra_tu<12>(g, s, F, c, cache, rec, pool); break;
+        case 17: intra_tu<17>(g, s, F, c, cache, rec, pool); break;
+        default: intra_tu<18>(g, s, F, c, cache, rec, pool); break;
     }
 }
 
@@ -665,14 +707,89 @@ __device__ void move_sb(const IntraFrame& F, const SbCtx& c, uint16_t* cache) {
     }
 }
 
+// One residual block to compute: the TU, its frame, where its block goes.
+struct ResTask {
+    av1g_tu tu;
+    int32_t frame;
+    int32_t out;
+};
+
+// Residual blocks of every intra TU of the batch, ahead of the wavefront:
+// they depend on the coefficients only.  Blocks [0, small_blocks) run the
+// small TUs one per warp; the others run the large TUs with the whole CTA.
+__global__ void __launch_bounds__(kT) intra_res_kernel(const IntraFrame* __restrict__ frames,
+                                                       const ResTask* __restrict__ small, int n_small,
+                                                       const ResTask* __restrict__ large, int n_large,
+                                                       int32_t* __restrict__ res, int small_blocks) {
+    __shared__ union {
+        WScr w[kNW];
+        CScr c;
+    } u;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if ((int)blockIdx.x < small_blocks) {
+        for (int q = blockIdx.x * kNW + warp; q < n_small; q += small_blocks * kNW) {
+            const ResTask tk = small[q];
+            const IntraFrame& F = frames[tk.frame];
+            const WarpG g{lane};
+            int32_t* out = res + tk.out;
+            switch (tk.tu.tx_size) {
+                case 0: residual_task<0>(g, u.w[warp], F, tk.tu, out); break;
+                case 1: residual_task<1>(g, u.w[warp], F, tk.tu, out); break;
+                case 2: residual_task<2>(g, u.w[warp], F, tk.tu, out); break;
+                case 5: residual_task<5>(g, u.w[warp], F, tk.tu, out); break;
+                case 6: residual_task<6>(g, u.w[warp], F, tk.tu, out); break;
+                case 7: residual_task<7>(g, u.w[warp], F, tk.tu, out); break;
+                case 8: residual_task<8>(g, u.w[warp], F, tk.tu, out); break;
+                case 13: residual_task<13>(g, u.w[warp], F, tk.tu, out); break;
+                case 14: residual_task<14>(g, u.w[warp], F, tk.tu, out); break;
+                case 15: residual_task<15>(g, u.w[warp], F, tk.tu, out); break;
+                default: residual_task<16>(g, u.w[warp], F, tk.tu, out); break;
+            }
+        }
+    } else {
+        for (int q = blockIdx.x - small_blocks; q < n_large; q += gridDim.x - small_blocks) {
+            const ResTask tk = large[q];
+            const IntraFrame& F = frames[tk.frame];
+            const CtaG g{tid};
+            int32_t* out = res + tk.out;
+            switch (tk.tu.tx_size) {
+                case 3: residual_task<3>(g, u.c, F, tk.tu, out); break;
+                case 4: residual_task<4>(g, u.c, F, tk.tu, out); break;
+                case 9: residual_task<9>(g, u.c, F, tk.tu, out); break;
+                case 10: residual_task<10>(g, u.c, F, tk.tu, out); break;
+                case 11: residual_task<11>(g, u.c, F, tk.tu, out); break;
+                case 12: residual_task<12>(g, u.c, F, tk.tu, out); break;
+                case 17: residual_task<17>(g, u.c, F, tk.tu, out); break;
+                default: residual_task<18>(g, u.c, F, tk.tu, out); break;
+            }
+        }
+    }
+}
+
+// Stages TU records [b, min(b + kTuWin, end)) into the window and returns
+// the window's end (all threads call; the bounds live in registers, the same
+// in every thread).
+__device__ __forceinline__ int stage_tus(av1g_intra_tu* win, const av1g_intra_tu* __restrict__ tus, int b, int end) {
+    const int e = min(b + kTuWin, end);
+    const uint4* src = reinterpret_cast<const uint4*>(tus + b);
+    uint4* dst = reinterpret_cast<uint4*>(win);
+    for (int q = threadIdx.x; q < (e - b) * 4; q += kT) dst[q] = __ldg(src + q);
+    return e;
+}
+
 __global__ void __launch_bounds__(kT) intra_kernel(const IntraFrame* __restrict__ frames,
                                                    const av1g_intra_tu* __restrict__ tus,
                                                    const SbItem* __restrict__ items, const int2* __restrict__ lvs,
-                                                   const int* __restrict__ deps, int* done, int* ctl, int nitems) {
+                                                   const int4* __restrict__ waits, int* prog, int* ctl, int nitems,
+                                                   const int32_t* __restrict__ res) {
+    // dynamic shared memory: Shared | TU window | superblock copy
     extern __shared__ __align__(16) uint8_t dsm[];
     Shared& S = *reinterpret_cast<Shared*>(dsm);
-    uint16_t* cache = reinterpret_cast<uint16_t*>(dsm + kSharedBytes);
+    av1g_intra_tu* win = reinterpret_cast<av1g_intra_tu*>(dsm + kSharedBytes);
+    uint16_t* cache = reinterpret_cast<uint16_t*>(dsm + kSharedBytes + kTuWin * sizeof(av1g_intra_tu));
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const IntraFrame& F = S.fr;
+    const Pool pool{res};
     for (;;) {
         __syncthreads();
         if (tid == 0) S.idx = atomicAdd(&ctl[0], 1);
@@ -680,7 +797,12 @@ __global__ void __launch_bounds__(kT) intra_kernel(const IntraFrame* __restrict_
         const int idx = S.idx;
         if (idx >= nitems) return;
         const SbItem it = items[idx];
-        const IntraFrame& F = frames[it.frame];
+        {
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(frames + it.frame);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(&S.fr);
+            for (int q = tid; q < (int)(sizeof(IntraFrame) / 4); q += kT) dst[q] = __ldg(src + q);
+        }
+        __syncthreads();
         if (tid == 0) {
             int off = 0;
             for (int p = 0; p < 3; p++) {
@@ -692,64 +814,103 @@ __global__ void __launch_bounds__(kT) intra_kernel(const IntraFrame* __restrict_
                 S.sb.off[p] = off;
                 off += p < F.np ? S.sb.w[p] * S.sb.h[p] : 0;
             }
+            S.abort_seen = 0;
         }
         __syncthreads();
-        // the superblock's own area is written only by its own TUs: stage it
-        // before waiting
+        // the superblock's own area is written only by its own TUs, and its
+        // TU records are inputs: stage both before any wait
         move_sb<true>(F, S.sb, cache);
-        for (int q = tid; q < it.ndep; q += kT) {
-            const int d = __ldg(deps + it.dep_first + q);
-            const long long t0 = gtimer();
-            while (ld_acquire(done + d) == 0) {
-                if (*(volatile int*)(ctl + 1)) break;
-                if (gtimer() - t0 > kWaitNs) {
-                    atomicOr(&g_wave_fault, 1u);
-                    atomicExch(ctl + 1, 1);
-                    break;
-                }
-                __nanosleep(128);
-            }
+        int tw0 = it.tu_first;
+        int tw1 = stage_tus(win, tus, tw0, it.tu_end);
+        // the waits, by level (staged when few; the level of the next one in a register)
+        const int4* wsrc = waits + it.wait_first;
+        if (it.nwait <= kWaitWin) {
+            for (int q = tid; q < it.nwait; q += kT) S.wv[q] = __ldg(wsrc + q);
+            wsrc = S.wv;
         }
+        int wq = 0;
         __syncthreads();
-        if (tid == 0) S.abort_seen = *(volatile int*)(ctl + 1);
-        __syncthreads();
-        if (!S.abort_seen) {
-            for (int L0 = 0; L0 < it.nlv; L0 += kLvChunk) {
-                const int n = min(kLvChunk, it.nlv - L0);
-                for (int q = tid; q <= n; q += kT) S.lv[q] = lvs[it.lv_first + L0 + q];
-                __syncthreads();
-                for (int L = 0; L < n; L++) {
-                    const int b = S.lv[L].x, m = S.lv[L].y, e = S.lv[L + 1].x;
+        int next_wait = it.nwait > 0 ? wsrc[0].x : 0x7fffffff;
+        for (int L0 = 0; L0 < it.nlv; L0 += kLvChunk) {
+            const int n = min(kLvChunk, it.nlv - L0);
+            __syncthreads();
+            for (int q = tid; q <= n; q += kT) S.lv[q] = lvs[it.lv_first + L0 + q];
+            __syncthreads();
+            for (int L = 0; L < n; L++) {
+                const int lg = L0 + L;
+                if (next_wait <= lg) {
+                    // the levels of other superblocks this level reads: poll
+                    // with volatile loads, then an acquire load orders the
+                    // reads after the progress seen
+                    const int w0 = wq;
+                    while (wq < it.nwait && wsrc[wq].x <= lg) wq++;
+                    next_wait = wq < it.nwait ? wsrc[wq].x : 0x7fffffff;
+                    for (int q = w0 + tid; q < wq; q += kT) {
+                        const int4 w = wsrc[q];
+                        const volatile int* f = prog + w.y;
+                        if (*f < w.z) {
+                            const long long t0 = gtimer();
+                            while (*f < w.z) {
+                                if (*(volatile int*)(ctl + 1)) break;
+                                if (gtimer() - t0 > kWaitNs) {
+                                    atomicOr(&g_wave_fault, 1u);
+                                    atomicExch(ctl + 1, 1);
+                                    break;
+                                }
+                                __nanosleep(64);
+                            }
+                        }
+                        ld_acquire(prog + w.y);
+                    }
+                    __syncthreads();
+                    if (tid == 0 && *(volatile int*)(ctl + 1)) S.abort_seen = 1;
+                    __syncthreads();
+                }
+                const bool publish = S.lv[L].y & kLevelPublished;
+                if (!S.abort_seen) {
+                    const int b = S.lv[L].x, m = S.lv[L].y & ~kLevelPublished, e = S.lv[L + 1].x;
+                    if (e > tw1 && b > tw0) {  // slide the window to this level
+                        tw0 = b;
+                        tw1 = stage_tus(win, tus, b, it.tu_end);
+                        __syncthreads();
+                    }
                     for (int k = b + warp; k < m; k += kNW) {
                         WScr& ws = S.s.w[warp];
-                        if (lane < 16)
-                            reinterpret_cast<uint32_t*>(&ws.tu)[lane] =
-                                __ldg(reinterpret_cast<const uint32_t*>(tus + k) + lane);
-                        __syncwarp();
-                        run_small(WarpG{lane}, ws, F, S.sb, cache);
+                        const av1g_intra_tu* rec = win + (k - tw0);
+                        if (k >= tw1) {  // a level wider than the window
+                            if (lane < 16)
+                                reinterpret_cast<uint32_t*>(&ws.tu)[lane] =
+                                    __ldg(reinterpret_cast<const uint32_t*>(tus + k) + lane);
+                            __syncwarp();
+                            rec = &ws.tu;
+                        }
+                        run_small(WarpG{lane}, ws, F, S.sb, cache, rec, pool);
                         __syncwarp();
                     }
                     if (m < e) {
                         __syncthreads();
                         for (int k = m; k < e; k++) {
-                            if (tid < 16)
-                                reinterpret_cast<uint32_t*>(&S.s.c.tu)[tid] =
-                                    __ldg(reinterpret_cast<const uint32_t*>(tus + k) + tid);
-                            __syncthreads();
-                            run_large(CtaG{tid}, S.s.c, F, S.sb, cache);
+                            const av1g_intra_tu* rec = win + (k - tw0);
+                            if (k >= tw1) {
+                                if (tid < 16)
+                                    reinterpret_cast<uint32_t*>(&S.s.c.tu)[tid] =
+                                        __ldg(reinterpret_cast<const uint32_t*>(tus + k) + tid);
+                                __syncthreads();
+                                rec = &S.s.c.tu;
+                            }
+                            run_large(CtaG{tid}, S.s.c, F, S.sb, cache, rec, pool);
                             __syncthreads();
                         }
                     }
-                    __syncthreads();
+                }
+                __syncthreads();
+                // publish "lg + 1 levels done" when another superblock waits
+                // for it, from the last warp (the first warp starts the next level)
+                if (publish && tid == kT - 32) {
+                    __threadfence();
+                    atomicExch(prog + idx, lg + 1);
                 }
             }
-        }
-        __syncthreads();
-        move_sb<false>(F, S.sb, cache);
-        __syncthreads();
-        if (tid == 0) {
-            __threadfence();
-            atomicExch(done + idx, 1);
         }
     }
 }
@@ -784,17 +945,37 @@ av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t st, std::s
     av1g_status rc = intra_plan(jobs, n, plan, err);
     if (rc != AV1G_OK || plan.items.empty()) return rc;
     const int nitems = (int)plan.items.size();
+    // residual tasks; each TU's device record points at its residual block
+    std::vector<ResTask> rs, rl;
+    long long res_ints = 0;
+    for (const SbItem& it : plan.items)
+        for (int k = it.tu_first; k < it.tu_end; k++) {
+            av1g_intra_tu& t = plan.tus[k];
+            if (!(t.flags & AV1G_INTRA_RESIDUAL)) continue;
+            const int px = kTxW[t.tx_size] * kTxH[t.tx_size];
+            (px > kSmallPx ? rl : rs).push_back(ResTask{t.res, it.frame, (int32_t)res_ints});
+            t.res.coeff_offset = (uint32_t)res_ints;
+            res_ints += px;
+        }
+    if (res_ints >= (1LL << 31)) {
+        err = "intra batch: more than 2^31 residual samples";
+        return AV1G_EINVAL;
+    }
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t off_tus = al(sizeof(IntraFrame) * n);
     const size_t off_items = al(off_tus + sizeof(av1g_intra_tu) * plan.tus.size());
     const size_t off_lv = al(off_items + sizeof(SbItem) * plan.items.size());
-    const size_t off_deps = al(off_lv + sizeof(int2) * plan.lvtab.size());
-    const size_t off_done = al(off_deps + sizeof(int) * plan.deps.size());
+    const size_t off_waits = al(off_lv + sizeof(int2) * plan.lvtab.size());
+    const size_t off_done = al(off_waits + sizeof(int4) * plan.waits.size());
     const size_t off_ctl = al(off_done + sizeof(int) * plan.items.size());
-    const size_t off_maps = al(off_ctl + 2 * sizeof(int));
-    const size_t bytes = off_maps + plan.maps.size();
+    const size_t off_rs = al(off_ctl + 2 * sizeof(int));
+    const size_t off_rl = al(off_rs + sizeof(ResTask) * rs.size());
+    const size_t off_maps = al(off_rl + sizeof(ResTask) * rl.size());
+    const size_t bytes = off_maps + plan.maps.size();  // uploaded
+    const size_t off_res = al(bytes);
+    const size_t total = off_res + sizeof(int32_t) * (size_t)res_ints;
     uint8_t* dev_buf = nullptr;
-    cudaError_t e = cudaMallocAsync((void**)&dev_buf, bytes, st);
+    cudaError_t e = cudaMallocAsync((void**)&dev_buf, total, st);
     if (e != cudaSuccess) {
         err = std::string("cudaMallocAsync: ") + cudaGetErrorString(e);
         return AV1G_EDEVICE;
@@ -805,21 +986,34 @@ av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t st, std::s
     memcpy(host.data() + off_tus, plan.tus.data(), sizeof(av1g_intra_tu) * plan.tus.size());
     memcpy(host.data() + off_items, plan.items.data(), sizeof(SbItem) * plan.items.size());
     memcpy(host.data() + off_lv, plan.lvtab.data(), sizeof(int2) * plan.lvtab.size());
-    if (!plan.deps.empty()) memcpy(host.data() + off_deps, plan.deps.data(), sizeof(int) * plan.deps.size());
-    memset(host.data() + off_done, 0, off_maps - off_done);  // done flags, claim counter, abort flag
+    if (!plan.waits.empty()) memcpy(host.data() + off_waits, plan.waits.data(), sizeof(int4) * plan.waits.size());
+    memset(host.data() + off_done, 0, off_rs - off_done);  // progress, claim counter, abort flag
+    if (!rs.empty()) memcpy(host.data() + off_rs, rs.data(), sizeof(ResTask) * rs.size());
+    if (!rl.empty()) memcpy(host.data() + off_rl, rl.data(), sizeof(ResTask) * rl.size());
     if (!plan.maps.empty()) memcpy(host.data() + off_maps, plan.maps.data(), plan.maps.size());
     e = upload(dev_buf, host.data(), bytes, st);
-    const size_t smem = kSharedBytes + plan.cache_bytes;
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(intra_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int per_sm = 0, sms = 0;
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, intra_kernel, kT, smem);
+    const IntraFrame* dframes = (const IntraFrame*)dev_buf;
+    int32_t* dres = (int32_t*)(dev_buf + off_res);
+    int sms = 0;
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess && (!rs.empty() || !rl.empty())) {
+        const int sb_blocks = (int)std::min<long long>(((long long)rs.size() + kNW - 1) / kNW, 16LL * sms);
+        const int lb_blocks = (int)std::min<long long>((long long)rl.size(), 4LL * sms);
+        intra_res_kernel<<<sb_blocks + lb_blocks, kT, 0, st>>>(dframes, (const ResTask*)(dev_buf + off_rs), (int)rs.size(),
+                                                               (const ResTask*)(dev_buf + off_rl), (int)rl.size(), dres,
+                                                               sb_blocks);
+        e = cudaGetLastError();
+    }
+    const size_t smem = kSharedBytes + kTuWin * sizeof(av1g_intra_tu) + plan.cache_bytes;
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(intra_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, intra_kernel, kT, smem);
     if (e == cudaSuccess) {
         const int grid = std::max(1, std::min(nitems, std::max(per_sm, 1) * sms));
         intra_kernel<<<grid, kT, smem, st>>>(
-            (const IntraFrame*)dev_buf, (const av1g_intra_tu*)(dev_buf + off_tus), (const SbItem*)(dev_buf + off_items),
-            (const int2*)(dev_buf + off_lv), (const int*)(dev_buf + off_deps), (int*)(dev_buf + off_done),
-            (int*)(dev_buf + off_ctl), nitems);
+            dframes, (const av1g_intra_tu*)(dev_buf + off_tus), (const SbItem*)(dev_buf + off_items),
+            (const int2*)(dev_buf + off_lv), (const int4*)(dev_buf + off_waits), (int*)(dev_buf + off_done),
+            (int*)(dev_buf + off_ctl), nitems, dres);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess && fault)

@@ -46,14 +46,18 @@ av1g_status intra_plan(const av1g_intra_job* jobs, int n, IntraPlan& plan, std::
     struct SbHost {
         int frame, seq, depth;
         SbItem item;
-        std::vector<int> deps;  // global indices of the superblocks it waits for
+        std::vector<int3> waits;  // {level, global superblock index, progress}
     };
     std::vector<SbHost> sbs_all;
     size_t total_tus = 0;
     for (int i = 0; i < n; i++) total_tus += jobs[i].num_tus > 0 ? (size_t)jobs[i].num_tus : 0;
     plan.tus.reserve(total_tus);
     plan.lvtab.reserve(total_tus + 1024);
-    std::vector<int> lvl, order, bucket, sb_index, hw, hr;
+    std::vector<int> lvl, order, bucket, sb_index, hw, hr, fwl, pend_head;
+    struct Pend {
+        int sb, level, next;
+    };
+    std::vector<Pend> pend;
     std::vector<uint32_t> wedge;
     for (int i = 0; i < n; i++) {
         const av1g_intra_job& j = jobs[i];
@@ -228,7 +232,7 @@ av1g_status intra_plan(const av1g_intra_job* jobs, int n, IntraPlan& plan, std::
             sh.frame = i;
             sh.seq = (int)q;
             sh.depth = 0;
-            sh.item = SbItem{i, 0, 0, 0, 0, sbs[q].sbx << log2sb, sbs[q].sby << log2sb, log2sb};
+            sh.item = SbItem{i, 0, 0, 0, 0, sbs[q].sbx << log2sb, sbs[q].sby << log2sb, log2sb, 0, 0};
             sbs_all.push_back(std::move(sh));
         }
         // 4x4-cell hazard maps of the current superblock: the last writer's
@@ -243,9 +247,23 @@ av1g_status intra_plan(const av1g_intra_job* jobs, int n, IntraPlan& plan, std::
         }
         hw.assign(ncell, -1);
         hr.assign(ncell, -1);
+        // frame-wide, per 4x4 cell inside the plane: the level of its last
+        // writer (within that writer's superblock), and the reads made of it
+        // by superblocks decoded before the one it belongs to
+        int fgw[3] = {}, fgh[3] = {}, fbase[3] = {}, nf = 0;
+        for (int p = 0; p < h.num_planes; p++) {
+            fgw[p] = (pw[p] + 3) >> 2;
+            fgh[p] = (ph[p] + 3) >> 2;
+            fbase[p] = nf;
+            nf += fgw[p] * fgh[p];
+        }
+        fwl.assign(nf, -1);
+        pend_head.assign(nf, -1);
+        pend.clear();
         int epoch = 0;
         for (size_t q = 0; q < sbs.size(); q++) {
             const Sb& b = sbs[q];
+            std::vector<int3>& waits = sbs_all[gbase + q].waits;  // {level, superblock, progress}
             lvl.resize(b.count);
             int nlv = 0;
             int ox[3], oy[3];
@@ -289,24 +307,87 @@ av1g_status intra_plan(const av1g_intra_job* jobs, int n, IntraPlan& plan, std::
                     for (int cx = wc.cx0; cx <= wc.cx1; cx++) hw[wc.base + cy * wc.stride + cx] = epoch + L;
                 lvl[k] = L;
                 nlv = std::max(nlv, L + 1);
-                // a read of another superblock's area orders the two superblocks
+                // reads of other superblocks' areas: wait for the level that
+                // wrote the cell (an earlier superblock), or make the later
+                // superblock's writer wait for this reader
+                int3 tw[8];  // this TU's waits, one per superblock
+                int ntw = 0;
                 for (int u = 0; u < nr; u++) {
                     const Rect& r = rr[u];
-                    const int rsx = r.p ? ssx : 0, rsy = r.p ? ssy : 0;
-                    const int by0 = (r.y0 << rsy) >> log2sb, by1 = (r.y1 << rsy) >> log2sb;
-                    const int bx0 = (r.x0 << rsx) >> log2sb, bx1 = (r.x1 << rsx) >> log2sb;
-                    if (by0 == b.sby && by1 == b.sby && bx0 == b.sbx && bx1 == b.sbx) continue;
-                    for (int by = by0; by <= by1; by++)
-                        for (int bx = bx0; bx <= bx1; bx++) {
-                            const int o = sb_index[(size_t)by * sb_cols + bx];
-                            if (o < 0 || o == (int)q) continue;
-                            std::vector<int>& d = o < (int)q ? sbs_all[gbase + q].deps : sbs_all[gbase + o].deps;
-                            const int v = o < (int)q ? gbase + o : gbase + (int)q;
-                            if (d.empty() || d.back() != v) d.push_back(v);
+                    const int p = r.p, sw = sb >> (p ? ssx : 0), shh = sb >> (p ? ssy : 0);
+                    if (r.x0 >= ox[p] && r.x1 < ox[p] + sw && r.y0 >= oy[p] && r.y1 < oy[p] + shh) continue;
+                    for (int cy = r.y0 >> 2; cy <= r.y1 >> 2; cy++) {
+                        const int py = cy << 2;
+                        const bool row_in = py >= oy[p] && py < oy[p] + shh;
+                        const int by = (py << (p ? ssy : 0)) >> log2sb;
+                        for (int cx = r.x0 >> 2; cx <= r.x1 >> 2; cx++) {
+                            const int px = cx << 2;
+                            if (row_in && px >= ox[p] && px < ox[p] + sw) continue;
+                            const int o = sb_index[(size_t)by * sb_cols + ((px << (p ? ssx : 0)) >> log2sb)];
+                            if (o < 0) continue;
+                            const int fc = fbase[p] + cy * fgw[p] + cx;
+                            if (o < (int)q) {
+                                const int need = fwl[fc] + 1;
+                                if (need <= 0) continue;
+                                int a = 0;
+                                while (a < ntw && tw[a].y != gbase + o) a++;
+                                if (a == ntw) {
+                                    if (ntw == 8) {
+                                        waits.push_back(int3{L, gbase + o, need});
+                                        continue;
+                                    }
+                                    tw[ntw++] = int3{L, gbase + o, need};
+                                } else {
+                                    tw[a].z = std::max(tw[a].z, need);
+                                }
+                            } else {
+                                pend.push_back(Pend{gbase + (int)q, L, pend_head[fc]});
+                                pend_head[fc] = (int)pend.size() - 1;
+                            }
+                        }
+                    }
+                }
+                waits.insert(waits.end(), tw, tw + ntw);
+                // this TU's cells (inside the plane): their writer, and the
+                // reads earlier superblocks made of them before this write
+                {
+                    const int p = t.plane;
+                    const int cx0 = t.x >> 2, cy0 = t.y >> 2;
+                    const int cx1 = std::min((t.x + kW[t.tx_size] - 1) >> 2, fgw[p] - 1);
+                    const int cy1 = std::min((t.y + kH[t.tx_size] - 1) >> 2, fgh[p] - 1);
+                    for (int cy = cy0; cy <= cy1; cy++)
+                        for (int cx = cx0; cx <= cx1; cx++) {
+                            const int fc = fbase[p] + cy * fgw[p] + cx;
+                            fwl[fc] = L;
+                            for (int e = pend_head[fc]; e >= 0; e = pend[e].next)
+                                waits.push_back(int3{L, pend[e].sb, pend[e].level + 1});
+                            pend_head[fc] = -1;
                         }
                 }
             }
             epoch += b.count + 1;
+            // the waits: the strongest per (level, superblock), and only those
+            // a smaller level does not already imply
+            std::sort(waits.begin(), waits.end(), [](const int3& a, const int3& c) {
+                return a.y != c.y ? a.y < c.y : (a.x != c.x ? a.x < c.x : a.z > c.z);
+            });
+            {
+                size_t o = 0;
+                int cur = -1, best = 0;
+                for (size_t u = 0; u < waits.size(); u++) {
+                    const int3 w = waits[u];
+                    if (w.y != cur) {
+                        cur = w.y;
+                        best = 0;
+                    }
+                    if (w.z > best) {
+                        best = w.z;
+                        waits[o++] = w;
+                    }
+                }
+                waits.resize(o);
+                std::sort(waits.begin(), waits.end(), [](const int3& a, const int3& c) { return a.x < c.x; });
+            }
             // the TUs by level, a level's small TUs before its large ones (a
             // counting sort on 2 * level + large, stable in decode order)
             auto large = [&](int k) {
@@ -321,6 +402,8 @@ av1g_status intra_plan(const av1g_intra_job* jobs, int n, IntraPlan& plan, std::
             SbItem& it = sbs_all[gbase + q].item;
             it.lv_first = (int)plan.lvtab.size();
             it.nlv = nlv;
+            it.tu_first = (int)plan.tus.size();
+            it.tu_end = it.tu_first + b.count;
             int cur = -1;
             for (int u = 0; u < b.count; u++) {
                 const int k = order[u];
@@ -335,13 +418,9 @@ av1g_status intra_plan(const av1g_intra_job* jobs, int n, IntraPlan& plan, std::
             }
             const int end = (int)plan.tus.size();
             plan.lvtab.push_back(int2{end, end});
-        }
-        // dependency depth in decode order (every wait points to an earlier superblock)
-        for (size_t q = 0; q < sbs.size(); q++) {
+            // dependency depth (every wait points to a superblock earlier in decode order)
             SbHost& sh = sbs_all[gbase + q];
-            std::sort(sh.deps.begin(), sh.deps.end());
-            sh.deps.erase(std::unique(sh.deps.begin(), sh.deps.end()), sh.deps.end());
-            for (int d : sh.deps) sh.depth = std::max(sh.depth, sbs_all[d].depth + 1);
+            for (const int3& w : sh.waits) sh.depth = std::max(sh.depth, sbs_all[w.y].depth + 1);
         }
     }
     // claim order: depth, then frame, then decode order — a topological order
@@ -357,13 +436,17 @@ av1g_status intra_plan(const av1g_intra_job* jobs, int n, IntraPlan& plan, std::
     });
     std::vector<int> pos(sbs_all.size());
     for (size_t q = 0; q < claim.size(); q++) pos[claim[q]] = (int)q;
+    // the levels some superblock waits for are published (progress z means
+    // z levels done: published after level z - 1)
+    for (const SbHost& sh : sbs_all)
+        for (const int3& w : sh.waits) plan.lvtab[sbs_all[w.y].item.lv_first + w.z - 1].y |= kLevelPublished;
     plan.items.resize(claim.size());
     for (size_t q = 0; q < claim.size(); q++) {
         const SbHost& sh = sbs_all[claim[q]];
         SbItem it = sh.item;
-        it.dep_first = (int)plan.deps.size();
-        it.ndep = (int)sh.deps.size();
-        for (int d : sh.deps) plan.deps.push_back(pos[d]);
+        it.wait_first = (int)plan.waits.size();
+        it.nwait = (int)sh.waits.size();
+        for (const int3& w : sh.waits) plan.waits.push_back(int4{w.x, pos[w.y], w.z, 0});
         plan.items[q] = it;
     }
     return AV1G_OK;

@@ -27,14 +27,17 @@ struct SbItem {
     int32_t frame;
     int32_t lv_first;   // its level table: nlv + 1 entries {first TU, first large TU}
     int32_t nlv;
-    int32_t dep_first;  // claim indices of the superblocks it waits for
-    int32_t ndep;
+    int32_t wait_first; // its waits, by level: {level, claim index, progress, 0}
+    int32_t nwait;
     int32_t x0, y0;     // luma-sample origin
     int32_t log2sb;
+    int32_t tu_first, tu_end;  // its TU records
 };
 
 // TUs of at most this many samples run on one warp; larger ones on the CTA.
 constexpr int kIntraSmallPx = 256;
+// Level-table flag (in .y): other superblocks wait for this level.
+constexpr int kLevelPublished = 1 << 30;
 
 struct IntraPlan {
     std::vector<IntraFrame> frames;     // maps still relative: map_base[frame]
@@ -43,7 +46,7 @@ struct IntraPlan {
     std::vector<av1g_intra_tu> tus;     // per superblock, in level order (small before large)
     std::vector<int2> lvtab;
     std::vector<SbItem> items;          // claim order: a topological order of the waits
-    std::vector<int> deps;
+    std::vector<int4> waits;            // before level x, superblock y has finished z levels
     size_t cache_bytes = 0;             // the largest superblock copy (all planes, u16)
 };
 
