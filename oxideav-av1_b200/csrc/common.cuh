@@ -10,6 +10,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <cuda_runtime.h>
 
 #include "av1g.h"
@@ -72,6 +73,7 @@ __device__ __forceinline__ int floor_log2u(unsigned x) { return x ? 31 - __clz(x
 // Enqueues a host-to-device copy of n bytes through a pinned staging block
 // (returns once enqueued; the host bytes may be reused immediately).
 cudaError_t upload(void* dev, const void* host, size_t n, cudaStream_t s);
+cudaError_t upload_with(void* dev, size_t n, cudaStream_t s, const std::function<void(uint8_t*)>& fill);
 
 __device__ __forceinline__ int ld_px(const PlaneDev& P, int hbd, int y, int x) {
     const uint8_t* row = P.p + (size_t)y * P.stride;

@@ -387,17 +387,20 @@ void enqueue_step(av1g_engine* E, cudaStream_t cs, std::vector<std::shared_ptr<T
             }
             step.work_bytes += w.B.bytes;
             rebase(w.B, w.blob_off, t);
-            std::vector<uint8_t> blob(w.B.host_bytes, 0);
-            for (int g = 0; g < 9; g++)
-                if (!t.grid[g].empty()) memcpy(blob.data() + w.blob_off[g], t.grid[g].data(), t.grid[g].size());
-            if (!t.cdef_idx.empty()) memcpy(blob.data() + w.blob_off[9], t.cdef_idx.data(), t.cdef_idx.size());
-            for (int p = 0; p < 3; p++)
-                if (!t.lr_units[p].empty())
-                    memcpy(blob.data() + w.blob_off[10 + p], t.lr_units[p].data(),
-                           t.lr_units[p].size() * sizeof(av1g_lr_unit));
-            if (!t.coeffs.empty())
-                memcpy(blob.data() + w.blob_off[13], t.coeffs.data(), t.coeffs.size() * sizeof(int32_t));
-            e = upload(w.B.dev, blob.data(), blob.size(), cs);
+            // the frame's grids, CDEF indices, LR units and coefficients,
+            // assembled straight into the pinned staging block
+            e = upload_with(w.B.dev, w.B.host_bytes, cs, [&](uint8_t* blob) {
+                memset(blob, 0, w.B.host_bytes);
+                for (int g = 0; g < 9; g++)
+                    if (!t.grid[g].empty()) memcpy(blob + w.blob_off[g], t.grid[g].data(), t.grid[g].size());
+                if (!t.cdef_idx.empty()) memcpy(blob + w.blob_off[9], t.cdef_idx.data(), t.cdef_idx.size());
+                for (int p = 0; p < 3; p++)
+                    if (!t.lr_units[p].empty())
+                        memcpy(blob + w.blob_off[10 + p], t.lr_units[p].data(),
+                               t.lr_units[p].size() * sizeof(av1g_lr_unit));
+                if (!t.coeffs.empty())
+                    memcpy(blob + w.blob_off[13], t.coeffs.data(), t.coeffs.size() * sizeof(int32_t));
+            });
             // CurrFrame starts at zero, like the walker's fresh planes
             for (int p = 0; e == cudaSuccess && p < t.hdr.num_planes; p++)
                 e = cudaMemsetAsync(w.B.recon[p].data, 0, (size_t)w.B.recon[p].stride * w.B.recon[p].height, cs);

@@ -981,17 +981,17 @@ av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t st, std::s
         return AV1G_EDEVICE;
     }
     for (int i = 0; i < n; i++) plan.frames[i].maps = dev_buf + off_maps + plan.map_base[i];
-    std::vector<uint8_t> host(bytes);
-    memcpy(host.data(), plan.frames.data(), sizeof(IntraFrame) * n);
-    memcpy(host.data() + off_tus, plan.tus.data(), sizeof(av1g_intra_tu) * plan.tus.size());
-    memcpy(host.data() + off_items, plan.items.data(), sizeof(SbItem) * plan.items.size());
-    memcpy(host.data() + off_lv, plan.lvtab.data(), sizeof(int2) * plan.lvtab.size());
-    if (!plan.waits.empty()) memcpy(host.data() + off_waits, plan.waits.data(), sizeof(int4) * plan.waits.size());
-    memset(host.data() + off_done, 0, off_rs - off_done);  // progress, claim counter, abort flag
-    if (!rs.empty()) memcpy(host.data() + off_rs, rs.data(), sizeof(ResTask) * rs.size());
-    if (!rl.empty()) memcpy(host.data() + off_rl, rl.data(), sizeof(ResTask) * rl.size());
-    if (!plan.maps.empty()) memcpy(host.data() + off_maps, plan.maps.data(), plan.maps.size());
-    e = upload(dev_buf, host.data(), bytes, st);
+    e = upload_with(dev_buf, bytes, st, [&](uint8_t* host) {
+        memcpy(host, plan.frames.data(), sizeof(IntraFrame) * n);
+        memcpy(host + off_tus, plan.tus.data(), sizeof(av1g_intra_tu) * plan.tus.size());
+        memcpy(host + off_items, plan.items.data(), sizeof(SbItem) * plan.items.size());
+        memcpy(host + off_lv, plan.lvtab.data(), sizeof(int2) * plan.lvtab.size());
+        if (!plan.waits.empty()) memcpy(host + off_waits, plan.waits.data(), sizeof(int4) * plan.waits.size());
+        memset(host + off_done, 0, off_rs - off_done);  // progress, claim counter, abort flag
+        if (!rs.empty()) memcpy(host + off_rs, rs.data(), sizeof(ResTask) * rs.size());
+        if (!rl.empty()) memcpy(host + off_rl, rl.data(), sizeof(ResTask) * rl.size());
+        if (!plan.maps.empty()) memcpy(host + off_maps, plan.maps.data(), plan.maps.size());
+    });
     const IntraFrame* dframes = (const IntraFrame*)dev_buf;
     int32_t* dres = (int32_t*)(dev_buf + off_res);
     int sms = 0;
@@ -1009,7 +1009,11 @@ av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t st, std::s
     int per_sm = 0;
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, intra_kernel, kT, smem);
     if (e == cudaSuccess) {
-        const int grid = std::max(1, std::min(nitems, std::max(per_sm, 1) * sms));
+        // as many CTAs as the wavefront can keep busy (the superblocks of
+        // one depth, twice over since level-granular waits let the next depth
+        // start early), not the whole GPU: idle CTAs would only poll while
+        // other streams' kernels wait for SMs
+        const int grid = std::max(1, std::min({nitems, std::max(per_sm, 1) * sms, 2 * plan.width + 2}));
         intra_kernel<<<grid, kT, smem, st>>>(
             dframes, (const av1g_intra_tu*)(dev_buf + off_tus), (const SbItem*)(dev_buf + off_items),
             (const int2*)(dev_buf + off_lv), (const int4*)(dev_buf + off_waits), (int*)(dev_buf + off_done),

@@ -436,6 +436,10 @@ av1g_status intra_plan(const av1g_intra_job* jobs, int n, IntraPlan& plan, std::
     });
     std::vector<int> pos(sbs_all.size());
     for (size_t q = 0; q < claim.size(); q++) pos[claim[q]] = (int)q;
+    for (size_t q = 0, run = 0; q < claim.size(); q++) {
+        run = (q > 0 && sbs_all[claim[q]].depth == sbs_all[claim[q - 1]].depth) ? run + 1 : 1;
+        plan.width = std::max(plan.width, (int)run);
+    }
     // the levels some superblock waits for are published (progress z means
     // z levels done: published after level z - 1)
     for (const SbHost& sh : sbs_all)

@@ -48,6 +48,7 @@ struct IntraPlan {
     std::vector<SbItem> items;          // claim order: a topological order of the waits
     std::vector<int4> waits;            // before level x, superblock y has finished z levels
     size_t cache_bytes = 0;             // the largest superblock copy (all planes, u16)
+    int width = 0;                      // most superblocks at one dependency depth
 };
 
 // Validates the jobs and builds the plan.  AV1G_OK with no items when there

@@ -5,8 +5,11 @@
 // waits for the stream to drain before it starts, which would stall every
 // entry point until the GPU caught up and defeat the pipelining of the serving
 // engine.  upload() instead copies the bytes into a pinned block and enqueues
-// the copy from there; a block is reused once the event recorded after its
-// copy has completed.
+// the copy from there (upload_with() lets the caller build the bytes in the
+// block directly); a block is reused once the event recorded after its copy
+// has completed.
+#include <cstring>
+#include <functional>
 #include <mutex>
 #include <vector>
 
@@ -33,7 +36,7 @@ size_t g_pinned = 0;
 
 }  // namespace
 
-cudaError_t upload(void* dev, const void* host, size_t n, cudaStream_t s) {
+cudaError_t upload_with(void* dev, size_t n, cudaStream_t s, const std::function<void(uint8_t*)>& fill) {
     if (n == 0) return cudaSuccess;
     int device = 0;
     cudaError_t e = cudaGetDevice(&device);
@@ -53,7 +56,13 @@ cudaError_t upload(void* dev, const void* host, size_t n, cudaStream_t s) {
         if (!pick) {
             size_t cap = kMinBlock;
             while (cap < n) cap <<= 1;
-            if (g_pinned + cap > kMaxPinned) return cudaMemcpyAsync(dev, host, n, cudaMemcpyHostToDevice, s);
+            if (g_pinned + cap > kMaxPinned) {
+                // beyond the pinned budget: a copy from pageable memory, which
+                // returns once the driver has staged the bytes
+                std::vector<uint8_t> tmp(n);
+                fill(tmp.data());
+                return cudaMemcpyAsync(dev, tmp.data(), n, cudaMemcpyHostToDevice, s);
+            }
             auto* b = new Block();
             b->device = device;
             b->cap = cap;
@@ -74,12 +83,16 @@ cudaError_t upload(void* dev, const void* host, size_t n, cudaStream_t s) {
         }
         pick->busy = true;
     }
-    memcpy(pick->p, host, n);
+    fill(static_cast<uint8_t*>(pick->p));
     e = cudaMemcpyAsync(dev, pick->p, n, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaEventRecord(pick->ev, s);
     std::lock_guard<std::mutex> lk(g_mu);
     pick->busy = false;
     return e;
+}
+
+cudaError_t upload(void* dev, const void* host, size_t n, cudaStream_t s) {
+    return upload_with(dev, n, s, [&](uint8_t* p) { memcpy(p, host, n); });
 }
 
 }  // namespace av1g
