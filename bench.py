@@ -32,6 +32,8 @@ import sys
 import time
 from pathlib import Path
 
+import numpy as np
+
 ROOT = Path(__file__).resolve().parent
 PKG_DIR = ROOT / "oxideav-av1_b200"
 
@@ -340,6 +342,9 @@ def run_gpu(args):
         "gpu_launches": len(stages) * args.steps,
         "clocks": clocks,
     }
+    if rank == 0 and world == 1:
+        line["recon_stages"] = run_recon_stages(args, dev, stream)
+        line["extra_stages"] = run_extra_stages(args, dev, stream)
     if rank == 0 and world == 1 and not args.no_serving:
         line["serving"] = run_serving(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -353,6 +358,128 @@ def run_gpu(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def _device_ms(stream, fn, reps=5):
+    """Device time of the kernels fn() enqueues, and the host time of the call.
+
+    A spin kernel holds the stream while the host prepares the launch (the
+    library validates, plans and stages its records before it launches), so
+    the events around the call bracket only the device work: the descriptor
+    upload and the kernels."""
+    import torch
+    t0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        fn()  # warm-up; also sizes the gate
+    torch.cuda.synchronize()
+    gate_ms = 3 * (time.perf_counter() - t0) * 1e3 + 5
+    dev, host = [], []
+    for _ in range(reps):
+        with torch.cuda.stream(stream):
+            torch.cuda._sleep(int(gate_ms * 2.0e6))  # ~gate_ms at up to 2 GHz
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            h0 = time.perf_counter()
+            fn()
+            host.append((time.perf_counter() - h0) * 1e3)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        dev.append(e0.elapsed_time(e1))
+    return min(dev), min(host)
+
+
+def run_recon_stages(args, dev, stream):
+    """Rows a1-a5 on one 1920x1080 frame each: the residual pass of inter
+    blocks (dequant + inverse transform + merge), the inter prediction pass
+    and the intra wavefront of a key frame (its residual pre-pass included).
+    Device time per frame, the host time of the call beside it, and the
+    algorithmic bytes over the device time."""
+    from oxideav_av1_b200 import postfilter
+    S = 2 if args.bit_depth > 8 else 1
+    peak, _ = measured_peak()
+    out = {}
+    kw = dict(bit_depth=args.bit_depth)
+    tw = np.array([4, 8, 16, 32, 64, 4, 8, 8, 16, 16, 32, 32, 64, 4, 16, 8, 32, 16, 64])
+    th = np.array([4, 8, 16, 32, 64, 8, 4, 16, 8, 32, 16, 64, 32, 16, 4, 32, 8, 64, 16])
+
+    rf = synth.make_recon_frame(9001, WIDTH, HEIGHT, **kw)
+    d = postfilter.DeviceRecon(rf, device=dev)
+    ms, hms = _device_ms(stream, lambda: postfilter.run_recon([d], stream=stream))
+    area = int((tw[rf.tus["tx_size"]] * th[rf.tus["tx_size"]]).sum())
+    nb = rf.coeffs.nbytes + len(rf.tus) * 16 + 2 * area * S
+    out["residual"] = {"kernel": "recon_kernel", "ms_per_frame": ms, "host_ms_per_call": hms, "tus": len(rf.tus),
+                       "algorithmic_bytes": nb, "achieved_gbs": nb / ms / 1e6, "frac_of_hbm": nb / ms / 1e6 / peak,
+                       "bytes_model": "coefficients + TU records + the TU areas read and written"}
+
+    ff = synth.make_inter_frame(9002, WIDTH, HEIGHT, **kw)
+    d = postfilter.DeviceInter(ff, device=dev)
+    ms, hms = _device_ms(stream, lambda: postfilter.run_inter([d], stream=stream))
+    p = ff.preds
+    nref = 1 + (p["kind"] == 1)
+    nb = int(((p["w"].astype(np.int64) + 7) * (p["h"].astype(np.int64) + 7) * nref).sum() * S
+             + (p["w"].astype(np.int64) * p["h"]).sum() * S)
+    out["inter"] = {"kernel": "inter_kernel", "ms_per_frame": ms, "host_ms_per_call": hms, "calls": len(p),
+                    "algorithmic_bytes": nb, "achieved_gbs": nb / ms / 1e6, "frac_of_hbm": nb / ms / 1e6 / peak,
+                    "bytes_model": "sum over calls of (w+7)(h+7) per reference + w*h written"}
+
+    fi = synth.make_intra_frame(9003, WIDTH, HEIGHT, **kw)
+    d = postfilter.DeviceIntra(fi, device=dev)
+    ms, hms = _device_ms(stream, lambda: postfilter.run_intra([d], stream=stream))
+    area = int((tw[fi.tus["tx_size"]] * th[fi.tus["tx_size"]]).sum())
+    out["intra"] = {"kernels": ["intra_res_kernel", "intra_kernel"], "ms_per_frame": ms, "host_ms_per_call": hms,
+                    "tus": len(fi.tus), "tus_per_us": len(fi.tus) / (ms * 1e3),
+                    "bound": "latency: the TU dependency chain of the superblock wavefront",
+                    "algorithmic_bytes": fi.coeffs.nbytes + 2 * area * S}
+    return out
+
+
+def run_extra_stages(args, dev, stream, templates=8, copies=6):
+    """The post-filter stages the main batch leaves off: superres (2x
+    horizontal upscale of the CDEF output and, with LR on, of the deblocked
+    copy) and film grain (seeded parameters), each one launch over
+    templates * copies 1920x1080 frames (more than L2 holds)."""
+    import torch
+    from oxideav_av1_b200 import postfilter
+    S = 2 if args.bit_depth > 8 else 1
+    peak, _ = measured_peak()
+    lib = abi.load()
+    sp = C.c_void_p(stream.cuda_stream)
+    out = {}
+    for name, kw, fn in [("superres", dict(superres_denom=16), lib.av1g_run_superres),
+                         ("film_grain", dict(film_grain=True), lib.av1g_run_film_grain)]:
+        tf = [synth.make_frame(9100 + k, WIDTH, HEIGHT, bit_depth=args.bit_depth, **kw) for k in range(templates)]
+        frames = [tf[k % templates] for k in range(templates * copies)]
+        dfr = [postfilter.DeviceFrame(f, device=dev) for f in frames]
+        jobs = postfilter.jobs_array(dfr)
+        n = len(dfr)
+        for _ in range(3):
+            abi.check(fn(jobs, n, sp))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 10
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(reps):
+                abi.check(fn(jobs, n, sp))
+            e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        h = frames[0].hdr
+        P_up = sum(frames[0].out_dims(p)[0] * frames[0].out_dims(p)[1] for p in range(h.num_planes))
+        if name == "superres":
+            P_down = sum(frames[0].plane_dims(p)[0] * frames[0].plane_dims(p)[1] for p in range(h.num_planes))
+            per = (P_down + P_up) * S * (2 if h.uses_lr else 1)
+            model = "(downscaled + upscaled samples) per pass; two passes (CDEF output and deblocked copy) with LR on"
+        else:
+            per = 2 * P_up * S
+            model = "output planes read and written once (grain templates and LUTs are per frame, negligible)"
+        kern = "superres_kernel" if name == "superres" else "grain_template_kernel + grain_blend_kernel"
+        out[name] = {"kernel": kern, "frames": n, "ms_per_launch": ms, "algorithmic_bytes_per_frame": per,
+                     "achieved_gbs": per * n / ms / 1e6, "frac_of_hbm": per * n / ms / 1e6 / peak,
+                     "bytes_model": model}
+        del dfr, jobs
+        torch.cuda.empty_cache()
+    return out
 
 
 SERVE_SHAPES = [(640, 360, 8, 5), (1280, 720, 8, 5), (1280, 720, 10, 5), (1920, 1080, 8, 4)]
@@ -604,9 +731,20 @@ def main():
     ap.add_argument("--serve-streams", type=int, default=40)
     ap.add_argument("--serve-seconds", type=float, default=6.0)
     ap.add_argument("--serve-lanes", type=int, default=4)
+    ap.add_argument("--section", default="all", choices=["all", "recon", "extra"],
+                    help="recon / extra: only that section (one GPU), printed as its own JSON object; "
+                         "for profiling a row's kernels")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.section != "all":
+        import torch
+        torch.cuda.set_device(0)
+        abi.load()
+        stream = torch.cuda.Stream()
+        fn = run_recon_stages if args.section == "recon" else run_extra_stages
+        print(json.dumps({args.section: fn(args, torch.device("cuda", 0), stream)}), flush=True)
+        return 0
     return run_gpu(args)
 
 

@@ -98,53 +98,63 @@ __device__ void scaling_fill(uint8_t* t, int np, const uint8_t* xv, const uint8_
     for (int v = xv[np - 1]; v < 256; v++) t[v] = yv[np - 1];
 }
 
-// AR filter of one template by one warp: wavefront over t = x + 4y.
+// AR filter of one template by one warp: wavefront over t = x + 4y, the
+// coefficients (minus 128) held in registers.
+template <int LAG>
 __device__ void ar_luma(int16_t* L, const av1g_film_grain& fg, int gmin, int gmax) {
-    int lane = threadIdx.x & 31, lag = fg.ar_coeff_lag;
+    constexpr int NC = 2 * LAG * (LAG + 1);
+    int c[NC > 0 ? NC : 1];
+#pragma unroll
+    for (int i = 0; i < NC; i++) c[i] = fg.ar_coeffs_y_plus_128[i] - 128;
+    const int shift = fg.ar_coeff_shift, lane = threadIdx.x & 31;
     for (int T = 3 + 4 * 3; T <= (LW - 4) + 4 * (LH - 1); T++) {
-        int ylo = max(3, (T - (LW - 4) + 3) >> 2), yhi = min(LH - 1, (T - 3) >> 2);
-        int y = ylo + lane;
+        const int ylo = max(3, (T - (LW - 4) + 3) >> 2), yhi = min(LH - 1, (T - 3) >> 2);
+        const int y = ylo + lane;
         if (y <= yhi) {
-            int x = T - 4 * y;
-            int s = 0, pos = 0;
-            for (int dr = -lag; dr <= 0; dr++)
-                for (int dc = -lag; dc <= lag; dc++) {
-                    if (dr == 0 && dc == 0) goto done;
-                    s += L[(y + dr) * LW + x + dc] * (fg.ar_coeffs_y_plus_128[pos] - 128);
-                    pos++;
+            const int x = T - 4 * y;
+            int s = 0;
+#pragma unroll
+            for (int dr = -LAG; dr <= 0; dr++)
+#pragma unroll
+                for (int dc = -LAG; dc <= LAG; dc++) {
+                    const int pos = (dr + LAG) * (2 * LAG + 1) + dc + LAG;
+                    if (pos < NC) s += L[(y + dr) * LW + x + dc] * c[pos];
                 }
-        done:
-            L[y * LW + x] = (int16_t)clip3(gmin, gmax, L[y * LW + x] + r2(s, fg.ar_coeff_shift));
+            L[y * LW + x] = (int16_t)clip3(gmin, gmax, L[y * LW + x] + r2(s, shift));
         }
         __syncwarp();
     }
 }
 
-__device__ void ar_chroma(int16_t* C, const int16_t* L, const uint8_t* coef, const av1g_film_grain& fg,
-                          int cw, int ch, int ssx, int ssy, int gmin, int gmax) {
-    int lane = threadIdx.x & 31, lag = fg.ar_coeff_lag;
+template <int LAG>
+__device__ void ar_chroma(int16_t* C, const int16_t* L, const uint8_t* coef, const av1g_film_grain& fg, int cw,
+                          int ch, int ssx, int ssy, int gmin, int gmax) {
+    constexpr int NC = 2 * LAG * (LAG + 1);  // the last coefficient weighs the co-located luma
+    int c[NC + 1];
+#pragma unroll
+    for (int i = 0; i <= NC; i++) c[i] = coef[i] - 128;
+    const bool luma = fg.num_y_points > 0;
+    const int shift = fg.ar_coeff_shift, lane = threadIdx.x & 31;
     for (int T = 3 + 4 * 3; T <= (cw - 4) + 4 * (ch - 1); T++) {
-        int ylo = max(3, (T - (cw - 4) + 3) >> 2), yhi = min(ch - 1, (T - 3) >> 2);
+        const int ylo = max(3, (T - (cw - 4) + 3) >> 2), yhi = min(ch - 1, (T - 3) >> 2);
         for (int y = ylo + lane; y <= yhi; y += 32) {
-            int x = T - 4 * y;
-            int s = 0, pos = 0;
-            for (int dr = -lag; dr <= 0; dr++)
-                for (int dc = -lag; dc <= lag; dc++) {
-                    int c = coef[pos] - 128;
-                    if (dr == 0 && dc == 0) {
-                        if (fg.num_y_points > 0) {
-                            int lx = ((x - 3) << ssx) + 3, ly = ((y - 3) << ssy) + 3, l = 0;
-                            for (int i = 0; i <= ssy; i++)
-                                for (int j = 0; j <= ssx; j++) l += L[(ly + i) * LW + lx + j];
-                            s += r2(l, ssx + ssy) * c;
-                        }
-                        goto done;
-                    }
-                    s += C[(y + dr) * cw + x + dc] * c;
-                    pos++;
+            const int x = T - 4 * y;
+            int s = 0;
+#pragma unroll
+            for (int dr = -LAG; dr <= 0; dr++)
+#pragma unroll
+                for (int dc = -LAG; dc <= LAG; dc++) {
+                    const int pos = (dr + LAG) * (2 * LAG + 1) + dc + LAG;
+                    if (pos < NC) s += C[(y + dr) * cw + x + dc] * c[pos];
                 }
-        done:
-            C[y * cw + x] = (int16_t)clip3(gmin, gmax, C[y * cw + x] + r2(s, fg.ar_coeff_shift));
+            if (luma) {
+                const int lx = ((x - 3) << ssx) + 3, ly = ((y - 3) << ssy) + 3;
+                int l = 0;
+                for (int i = 0; i <= ssy; i++)
+                    for (int j = 0; j <= ssx; j++) l += L[(ly + i) * LW + lx + j];
+                s += r2(l, ssx + ssy) * c[NC];
+            }
+            C[y * cw + x] = (int16_t)clip3(gmin, gmax, C[y * cw + x] + r2(s, shift));
         }
         __syncwarp();
     }
@@ -153,6 +163,8 @@ __device__ void ar_chroma(int16_t* C, const int16_t* L, const uint8_t* coef, con
 __global__ void __launch_bounds__(128) grain_template_kernel(const FrameDev* __restrict__ frames,
                                                              const int32_t* __restrict__ starts, int n, int total) {
     __shared__ int16_t T[3][LH * LW];
+    __shared__ int16_t gauss[2048];  // the lanes draw different entries: shared, not constant, memory
+    for (int i = threadIdx.x; i < 2048; i += blockDim.x) gauss[i] = (int16_t)c_gauss[i];
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
         int f = find_frame(starts, n, t);
         const FrameDev& F = frames[f];
@@ -188,18 +200,33 @@ __global__ void __launch_bounds__(128) grain_template_kernel(const FrameDev* __r
                 int g = 0;
                 if (on) {
                     s = lfsr_step(s);
-                    g = c_gauss[(s >> 5) & 2047];
+                    g = gauss[(s >> 5) & 2047];
                 }
                 row[x] = (int16_t)r2(g, shift);
             }
         }
         __syncthreads();
-        if (fg.num_y_points > 0 && threadIdx.x < 32) ar_luma(T[0], fg, gmin, gmax);
+        if (fg.num_y_points > 0 && threadIdx.x < 32) {
+            switch (fg.ar_coeff_lag) {
+                case 0: ar_luma<0>(T[0], fg, gmin, gmax); break;
+                case 1: ar_luma<1>(T[0], fg, gmin, gmax); break;
+                case 2: ar_luma<2>(T[0], fg, gmin, gmax); break;
+                default: ar_luma<3>(T[0], fg, gmin, gmax); break;
+            }
+        }
         __syncthreads();
         if (fg.chroma_scaling_from_luma || fg.num_cb_points > 0 || fg.num_cr_points > 0) {
             int warp = threadIdx.x >> 5;
-            if (warp == 0) ar_chroma(T[1], T[0], fg.ar_coeffs_cb_plus_128, fg, cw, ch, ssx, ssy, gmin, gmax);
-            else if (warp == 1) ar_chroma(T[2], T[0], fg.ar_coeffs_cr_plus_128, fg, cw, ch, ssx, ssy, gmin, gmax);
+            if (warp < 2) {
+                int16_t* C = T[1 + warp];
+                const uint8_t* cf = warp == 0 ? fg.ar_coeffs_cb_plus_128 : fg.ar_coeffs_cr_plus_128;
+                switch (fg.ar_coeff_lag) {
+                    case 0: ar_chroma<0>(C, T[0], cf, fg, cw, ch, ssx, ssy, gmin, gmax); break;
+                    case 1: ar_chroma<1>(C, T[0], cf, fg, cw, ch, ssx, ssy, gmin, gmax); break;
+                    case 2: ar_chroma<2>(C, T[0], cf, fg, cw, ch, ssx, ssy, gmin, gmax); break;
+                    default: ar_chroma<3>(C, T[0], cf, fg, cw, ch, ssx, ssy, gmin, gmax); break;
+                }
+            }
         }
         __syncthreads();
         int16_t* out = F.grain_tmpl;
