@@ -298,6 +298,7 @@ def run_gpu(args):
     torch.cuda.synchronize()
     per_frame_ms = e0.elapsed_time(e1) / args.steps
 
+    graph = run_graphs(lib, jobs, n, stream, args.steps)
     e2e = run_e2e(args, frames, dframes, jobs, stream, dev, world)
     clk.__exit__(None, None, None)
     clocks = clk.summary()
@@ -338,6 +339,7 @@ def run_gpu(args):
         "stages": stage_frac,
         "per_frame_path": {"value": world * n / (per_frame_ms / 1e3), "unit": UNIT, "ms_per_step": per_frame_ms,
                            "launches_per_step": None},
+        "graph": graph,
         "e2e": e2e,
         "gpu_launches": len(stages) * args.steps,
         "clocks": clocks,
@@ -358,6 +360,36 @@ def run_gpu(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def run_graphs(lib, jobs, n, stream, steps):
+    """The same chain (deblock, CDEF, LR) captured once as a CUDA graph
+    (av1g_chain_graph_create) and replayed: batched (one launch per stage)
+    and per-frame (a launch per stage per frame, all inside the graph)."""
+    import torch
+    sp = C.c_void_p(stream.cuda_stream)
+    mask = (1 << 0) | (1 << 1) | (1 << 3)
+    out = {}
+    for name, mode in [("batched", abi.MODE_BATCHED), ("per_frame", abi.MODE_PER_FRAME)]:
+        g = C.c_void_p()
+        abi.check(lib.av1g_chain_graph_create(jobs, n, mask, mode, sp, C.byref(g)))
+        try:
+            for _ in range(3):
+                abi.check(lib.av1g_chain_graph_launch(g, sp))
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+                for _ in range(steps):
+                    abi.check(lib.av1g_chain_graph_launch(g, sp))
+                e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            out[name] = {"value": n / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
+                         "kernels_per_replay": lib.av1g_chain_graph_launches(g)}
+        finally:
+            abi.check(lib.av1g_chain_graph_destroy(g))
+    return out
 
 
 def _device_ms(stream, fn, reps=5):

@@ -676,6 +676,28 @@ av1g_status av1g_run_film_grain(const av1g_frame_job* jobs, int32_t n, void* str
 av1g_status av1g_run_postfilter(const av1g_frame_job* jobs, int32_t n, int32_t mode,
                                 void* stream, int32_t* launches);
 
+/* The §7.4 chain for a fixed set of jobs, captured once as a CUDA graph.
+ * The frame records, tile prefixes and stage scratch live in one device
+ * allocation the graph owns, so each av1g_chain_graph_launch is a single
+ * graph launch on `stream` that replays every stage launch — no record upload
+ * and no allocation per call (frame_driver.rs:830-1096 for the same frames
+ * step after step, e.g. a serving slot set or a benchmark batch).  The jobs'
+ * plane pointers, sizes and headers are baked in; the caller may rewrite the
+ * planes' samples between launches.  stage_mask: bit s runs stage s
+ * (0 deblock, 1 CDEF, 2 superres, 3 loop restoration, 4 film grain) with the
+ * reference's gating; mode: AV1G_MODE_BATCHED (one launch per stage) or
+ * AV1G_MODE_PER_FRAME (a launch per stage per frame, all in the graph).
+ * create runs the chain once, uncaptured, before capturing it. */
+typedef struct av1g_chain_graph av1g_chain_graph;
+av1g_status av1g_chain_graph_create(const av1g_frame_job* jobs, int32_t n, int32_t stage_mask, int32_t mode,
+                                    void* stream, av1g_chain_graph** out);
+av1g_status av1g_chain_graph_launch(av1g_chain_graph* g, void* stream);
+/* Kernel launches one replay performs. */
+int32_t av1g_chain_graph_launches(const av1g_chain_graph* g);
+/* Frees the graph; its device memory is released once the device is idle
+ * (cudaFree synchronizes), so launches still in flight complete first. */
+av1g_status av1g_chain_graph_destroy(av1g_chain_graph* g);
+
 /* Film grain (as av1g_run_film_grain) without any device allocation.  No
  * counterpart in the reference: it exists for callers that may not allocate
  * device memory on the per-frame path, such as a host application that

@@ -227,6 +227,11 @@ _SIGS = {
     "av1g_run_postfilter": (C.c_int, [C.POINTER(FrameJob), C.c_int32, C.c_int32, C.c_void_p,
                                       C.POINTER(C.c_int32)]),
     "av1g_run_film_grain_noalloc": (C.c_int, [C.POINTER(FrameJob), C.c_int32, C.c_void_p]),
+    "av1g_chain_graph_create": (C.c_int, [C.POINTER(FrameJob), C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
+                                          C.POINTER(C.c_void_p)]),
+    "av1g_chain_graph_launch": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "av1g_chain_graph_launches": (C.c_int32, [C.c_void_p]),
+    "av1g_chain_graph_destroy": (C.c_int, [C.c_void_p]),
     "av1g_run_recon": (C.c_int, [C.POINTER(ReconJob), C.c_int32, C.c_void_p]),
     "av1g_run_intra": (C.c_int, [C.POINTER(IntraJob), C.c_int32, C.c_void_p]),
     "av1g_run_inter": (C.c_int, [C.POINTER(InterJob), C.c_int32, C.c_void_p]),

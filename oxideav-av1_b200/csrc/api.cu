@@ -192,88 +192,101 @@ int stage_tiles(const FrameDev& F, int st) {
 }
 
 // Runs `stages` (bit mask over ST_*) for the jobs.
-av1g_status run(const av1g_frame_job* jobs, int n, int stage_mask, int mode, void* stream, int* launches) {
-    g_err.clear();
-    if (launches) *launches = 0;
-    if (n < 0 || (n > 0 && !jobs)) return fail(AV1G_EINVAL, "bad job array");
-    if (n == 0) return AV1G_OK;
-    if (mode != AV1G_MODE_BATCHED && mode != AV1G_MODE_PER_FRAME) return fail(AV1G_EINVAL, "mode %d", mode);
-    cudaStream_t s = (cudaStream_t)stream;
+// A batch's frame records, tile prefixes and scratch layout, built on the
+// host; bind() points the records at a device allocation of total_bytes.
+struct Prepared {
+    static constexpr int NS = ST_COUNT + 1;
     Batch b;
-    b.frames.resize(n);
+    int n = 0, stage_mask = 0, mode = 0, max_cells = 0;
+    size_t off_starts = 0, off_pf = 0, off_scratch = 0, total_bytes = 0;
+    std::vector<size_t> lf_off, grain_off;
+    std::vector<uint8_t> host;  // the uploaded prefix [0, off_scratch)
+    int32_t totals[NS] = {};
+};
+
+av1g_status prepare(const av1g_frame_job* jobs, int n, int stage_mask, int mode, Prepared& P) {
+    if (n < 0 || (n > 0 && !jobs)) return fail(AV1G_EINVAL, "bad job array");
+    if (mode != AV1G_MODE_BATCHED && mode != AV1G_MODE_PER_FRAME) return fail(AV1G_EINVAL, "mode %d", mode);
+    P.n = n;
+    P.stage_mask = stage_mask;
+    P.mode = mode;
+    P.b.frames.resize(n);
     for (int i = 0; i < n; i++) {
-        av1g_status st = prepare_frame(jobs[i], b.frames[i]);
+        av1g_status st = prepare_frame(jobs[i], P.b.frames[i]);
         if (st != AV1G_OK) {
             std::string m = g_err;
             return fail(st, "job %d: %s", i, m.c_str());
         }
     }
-    // layout: frames | starts (batched: NS x (n+1)) | per-frame starts (n x NS x 2) | grain scratch
-    const int NS = ST_COUNT + 1;
-    size_t off_starts = ((sizeof(FrameDev) * n) + 255) & ~(size_t)255;
-    size_t off_pf = off_starts + sizeof(int32_t) * NS * (n + 1);
-    size_t off_scratch = (off_pf + sizeof(int32_t) * n * NS * 2 + 255) & ~(size_t)255;
+    // layout: frames | starts (batched: NS x (n+1)) | per-frame starts (n x NS x 2) | scratch
+    const int NS = Prepared::NS;
+    P.off_starts = ((sizeof(FrameDev) * n) + 255) & ~(size_t)255;
+    P.off_pf = P.off_starts + sizeof(int32_t) * NS * (n + 1);
+    P.off_scratch = (P.off_pf + sizeof(int32_t) * n * NS * 2 + 255) & ~(size_t)255;
     // per-frame scratch: deblock cell codes, film grain templates / LUTs / offsets
     size_t scratch = 0;
-    std::vector<size_t> lf_off(n, 0), grain_off(n, 0);
-    int max_cells = 0;
+    P.lf_off.assign(n, 0);
+    P.grain_off.assign(n, 0);
     for (int i = 0; i < n; i++) {
-        const FrameDev& F = b.frames[i];
+        const FrameDev& F = P.b.frames[i];
         if ((stage_mask & (1 << ST_DEBLOCK)) && F.do_stage[ST_DEBLOCK]) {
             int cells = cells_deblock(F);
-            max_cells = cells > max_cells ? cells : max_cells;
-            lf_off[i] = off_scratch + scratch;
+            P.max_cells = cells > P.max_cells ? cells : P.max_cells;
+            P.lf_off[i] = P.off_scratch + scratch;
             scratch += ((size_t)cells * 2 + 255) & ~(size_t)255;
         }
         if ((stage_mask & (1 << ST_GRAIN)) && F.do_stage[ST_GRAIN]) {
-            grain_off[i] = off_scratch + scratch;
+            P.grain_off[i] = P.off_scratch + scratch;
             scratch += grain_scratch_bytes(F);
         }
     }
-    size_t total_bytes = off_scratch + scratch;
-    uint8_t* dev = nullptr;
-    cudaError_t e = cudaMallocAsync((void**)&dev, total_bytes, s);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
+    P.total_bytes = P.off_scratch + scratch;
+    return AV1G_OK;
+}
+
+// Points the records at dev and builds the uploaded prefix.
+void bind(Prepared& P, uint8_t* dev) {
+    const int n = P.n, NS = Prepared::NS;
     for (int i = 0; i < n; i++) {
-        FrameDev& F = b.frames[i];
-        if (lf_off[i]) {
-            uint16_t* c = (uint16_t*)(dev + lf_off[i]);
+        FrameDev& F = P.b.frames[i];
+        if (P.lf_off[i]) {
+            uint16_t* c = (uint16_t*)(dev + P.lf_off[i]);
             for (int p = 0; p < F.h.num_planes; p++) {
                 F.lf_codes[p] = c;
                 c += (F.recon[p].w >> 2) * (F.recon[p].h >> 2);
             }
         }
-        if (grain_off[i]) {
-            F.grain_tmpl = (int16_t*)(dev + grain_off[i]);
-            F.grain_lut = (uint8_t*)(dev + grain_off[i] + 3 * 73 * 82 * 2);
+        if (P.grain_off[i]) {
+            F.grain_tmpl = (int16_t*)(dev + P.grain_off[i]);
+            F.grain_lut = (uint8_t*)(dev + P.grain_off[i] + 3 * 73 * 82 * 2);
             F.grain_offs = F.grain_lut + 768;
         }
     }
-    std::vector<uint8_t> host(off_scratch, 0);
-    memcpy(host.data(), b.frames.data(), sizeof(FrameDev) * n);
-    int32_t* hs = (int32_t*)(host.data() + off_starts);
-    int32_t* hpf = (int32_t*)(host.data() + off_pf);
-    int32_t totals[ST_COUNT + 1];
+    P.host.assign(P.off_scratch, 0);
+    memcpy(P.host.data(), P.b.frames.data(), sizeof(FrameDev) * n);
+    int32_t* hs = (int32_t*)(P.host.data() + P.off_starts);
+    int32_t* hpf = (int32_t*)(P.host.data() + P.off_pf);
     for (int st = 0; st < NS; st++) {
         int32_t acc = 0;
         for (int i = 0; i < n; i++) {
-            int c = (stage_mask & (1 << (st < ST_COUNT ? st : ST_GRAIN))) ? stage_tiles(b.frames[i], st) : 0;
+            int c = (P.stage_mask & (1 << (st < ST_COUNT ? st : ST_GRAIN))) ? stage_tiles(P.b.frames[i], st) : 0;
             hs[st * (n + 1) + i] = acc;
             hpf[(i * NS + st) * 2 + 0] = 0;
             hpf[(i * NS + st) * 2 + 1] = c;
             acc += c;
         }
         hs[st * (n + 1) + n] = acc;
-        totals[st] = acc;
+        P.totals[st] = acc;
     }
-    e = upload(dev, host.data(), off_scratch, s);
-    if (e != cudaSuccess) {
-        cudaFreeAsync(dev, s);
-        return cuda_fail(e, "cudaMemcpyAsync");
-    }
+}
+
+// The stage launches of a bound batch (records at dev); returns how many.
+int launch_all(const Prepared& P, const uint8_t* dev, cudaStream_t s) {
+    const int n = P.n, NS = Prepared::NS;
     const FrameDev* dframes = (const FrameDev*)dev;
-    const int32_t* ds = (const int32_t*)(dev + off_starts);
-    const int32_t* dpf = (const int32_t*)(dev + off_pf);
+    const int32_t* ds = (const int32_t*)(dev + P.off_starts);
+    const int32_t* dpf = (const int32_t*)(dev + P.off_pf);
+    const int32_t* hpf = (const int32_t*)(P.host.data() + P.off_pf);
     int nl = 0;
     auto launch_stage = [&](int st, const FrameDev* fr, const int32_t* starts, const int32_t* starts_tmpl, int nn,
                             int total, int total_tmpl, int cells) {
@@ -289,16 +302,38 @@ av1g_status run(const av1g_frame_job* jobs, int n, int stage_mask, int mode, voi
         }
     };
     for (int st = 0; st < ST_COUNT; st++) {
-        if (!(stage_mask & (1 << st))) continue;
-        if (mode == AV1G_MODE_BATCHED) {
-            launch_stage(st, dframes, ds + st * (n + 1), ds + ST_COUNT * (n + 1), n, totals[st], totals[ST_COUNT],
-                         max_cells);
+        if (!(P.stage_mask & (1 << st))) continue;
+        if (P.mode == AV1G_MODE_BATCHED) {
+            launch_stage(st, dframes, ds + st * (n + 1), ds + ST_COUNT * (n + 1), n, P.totals[st], P.totals[ST_COUNT],
+                         P.max_cells);
         } else {
             for (int i = 0; i < n; i++)
                 launch_stage(st, dframes + i, dpf + (i * NS + st) * 2, dpf + (i * NS + ST_COUNT) * 2, 1,
-                             hpf[(i * NS + st) * 2 + 1], hpf[(i * NS + ST_COUNT) * 2 + 1], cells_deblock(b.frames[i]));
+                             hpf[(i * NS + st) * 2 + 1], hpf[(i * NS + ST_COUNT) * 2 + 1], cells_deblock(P.b.frames[i]));
         }
     }
+    return nl;
+}
+
+av1g_status run(const av1g_frame_job* jobs, int n, int stage_mask, int mode, void* stream, int* launches) {
+    g_err.clear();
+    if (launches) *launches = 0;
+    if (n < 0 || (n > 0 && !jobs)) return fail(AV1G_EINVAL, "bad job array");
+    if (n == 0) return AV1G_OK;
+    Prepared P;
+    av1g_status st = prepare(jobs, n, stage_mask, mode, P);
+    if (st != AV1G_OK) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    uint8_t* dev = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&dev, P.total_bytes, s);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
+    bind(P, dev);
+    e = upload(dev, P.host.data(), P.off_scratch, s);
+    if (e != cudaSuccess) {
+        cudaFreeAsync(dev, s);
+        return cuda_fail(e, "cudaMemcpyAsync");
+    }
+    int nl = launch_all(P, dev, s);
     e = cudaGetLastError();
     cudaFreeAsync(dev, s);
     if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
@@ -415,6 +450,80 @@ av1g_status av1g_run_inter(const av1g_inter_job* jobs, int32_t n, void* stream) 
 av1g_status av1g_run_postfilter(const av1g_frame_job* jobs, int32_t n, int32_t mode, void* stream,
                                 int32_t* launches) {
     return run(jobs, n, (1 << ST_COUNT) - 1, mode, stream, launches);
+}
+
+struct av1g_chain_graph {
+    uint8_t* dev = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int32_t launches = 0;
+};
+
+av1g_status av1g_chain_graph_create(const av1g_frame_job* jobs, int32_t n, int32_t stage_mask, int32_t mode,
+                                    void* stream, av1g_chain_graph** out) {
+    g_err.clear();
+    if (!out) return fail(AV1G_EINVAL, "no output pointer");
+    *out = nullptr;
+    if (n <= 0 || !jobs) return fail(AV1G_EINVAL, "bad job array");
+    if (stage_mask <= 0 || (stage_mask & ~((1 << ST_COUNT) - 1))) return fail(AV1G_EINVAL, "stage mask %d", stage_mask);
+    Prepared P;
+    av1g_status st = prepare(jobs, n, stage_mask, mode, P);
+    if (st != AV1G_OK) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    auto* G = new av1g_chain_graph;
+    auto bail = [&](cudaError_t e, const char* what) {
+        if (G->exec) cudaGraphExecDestroy(G->exec);
+        if (G->graph) cudaGraphDestroy(G->graph);
+        if (G->dev) cudaFree(G->dev);
+        delete G;
+        return cuda_fail(e, what);
+    };
+    cudaError_t e = cudaMalloc((void**)&G->dev, P.total_bytes);
+    if (e != cudaSuccess) {
+        G->dev = nullptr;
+        return bail(e, "cudaMalloc");
+    }
+    bind(P, G->dev);
+    e = cudaMemcpyAsync(G->dev, P.host.data(), P.off_scratch, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        launch_all(P, G->dev, s);  // once uncaptured: validates the launches
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return bail(e, "chain run");
+    cudaStream_t cs = nullptr;
+    e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bail(e, "cudaStreamCreate");
+    e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        G->launches = launch_all(P, G->dev, cs);
+        cudaError_t e2 = cudaStreamEndCapture(cs, &G->graph);
+        e = e2 != cudaSuccess ? e2 : cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&G->exec, G->graph, 0);
+    cudaStreamDestroy(cs);
+    if (e != cudaSuccess) return bail(e, "graph capture");
+    *out = G;
+    return AV1G_OK;
+}
+
+av1g_status av1g_chain_graph_launch(av1g_chain_graph* g, void* stream) {
+    g_err.clear();
+    if (!g || !g->exec) return fail(AV1G_EINVAL, "no graph");
+    cudaError_t e = cudaGraphLaunch(g->exec, (cudaStream_t)stream);
+    return e == cudaSuccess ? AV1G_OK : cuda_fail(e, "cudaGraphLaunch");
+}
+
+int32_t av1g_chain_graph_launches(const av1g_chain_graph* g) { return g ? g->launches : 0; }
+
+av1g_status av1g_chain_graph_destroy(av1g_chain_graph* g) {
+    g_err.clear();
+    if (!g) return AV1G_OK;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    cudaError_t e = g->dev ? cudaFree(g->dev) : cudaSuccess;
+    delete g;
+    return e == cudaSuccess ? AV1G_OK : cuda_fail(e, "cudaFree");
 }
 
 }  // extern "C"
