@@ -246,6 +246,10 @@ def run_gpu(args):
     n = len(dframes)
     stages = [("deblock", lib.av1g_run_deblock), ("cdef", lib.av1g_run_cdef), ("lr", lib.av1g_run_lr)]
 
+    # launch shapes: the project's autotuner times every candidate grid size
+    # (and superres tile width) on this batch before the warm-up
+    autotune = run_autotune(lib, jobs, n, stream, args.bit_depth > 8)
+
     def step(events=None):
         for i, (_, fn) in enumerate(stages):
             abi.check(fn(jobs, n, sp))
@@ -340,6 +344,7 @@ def run_gpu(args):
         "per_frame_path": {"value": world * n / (per_frame_ms / 1e3), "unit": UNIT, "ms_per_step": per_frame_ms,
                            "launches_per_step": None},
         "graph": graph,
+        "autotune": autotune,
         "e2e": e2e,
         "gpu_launches": len(stages) * args.steps,
         "clocks": clocks,
@@ -360,6 +365,18 @@ def run_gpu(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def run_autotune(lib, jobs, n, stream, hbd):
+    """av1g_autotune_postfilter on the batch; returns the chosen shape per stage."""
+    t0 = time.perf_counter()
+    abi.check(lib.av1g_autotune_postfilter(jobs, n, C.c_void_p(stream.cuda_stream), None))
+    out = {"seconds": time.perf_counter() - t0}
+    for st, name in enumerate(["deblock", "cdef", "superres", "lr", "film_grain"]):
+        c, t = C.c_int32(), C.c_int32()
+        abi.check(lib.av1g_autotune_get(st, int(hbd), C.byref(c), C.byref(t)))
+        out[name] = {"ctas_per_sm": c.value} | ({"tile": t.value} if st == 2 else {})
+    return out
 
 
 def run_graphs(lib, jobs, n, stream, steps):
@@ -484,6 +501,7 @@ def run_extra_stages(args, dev, stream, templates=8, copies=6):
         dfr = [postfilter.DeviceFrame(f, device=dev) for f in frames]
         jobs = postfilter.jobs_array(dfr)
         n = len(dfr)
+        shapes = run_autotune(lib, jobs, n, stream, args.bit_depth > 8)
         for _ in range(3):
             abi.check(fn(jobs, n, sp))
         torch.cuda.synchronize()
@@ -507,6 +525,7 @@ def run_extra_stages(args, dev, stream, templates=8, copies=6):
             model = "output planes read and written once (grain templates and LUTs are per frame, negligible)"
         kern = "superres_kernel" if name == "superres" else "grain_template_kernel + grain_blend_kernel"
         out[name] = {"kernel": kern, "frames": n, "ms_per_launch": ms, "algorithmic_bytes_per_frame": per,
+                     "launch_shape": shapes[name],
                      "achieved_gbs": per * n / ms / 1e6, "frac_of_hbm": per * n / ms / 1e6 / peak,
                      "bytes_model": model}
         del dfr, jobs

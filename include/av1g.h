@@ -513,6 +513,8 @@ typedef struct av1g_config {
                                     0 = 3                                         */
     int32_t lanes;               /* worker threads, each with a CUDA stream; a
                                     stream of frames stays on one lane; 0 = 4     */
+    const char* autotune_cache;  /* NULL, or a file av1g_autotune_postfilter
+                                    wrote: loaded at create                       */
 } av1g_config;
 
 /* What a stream's sequence header fixes: the largest upscaled frame and the
@@ -675,6 +677,23 @@ av1g_status av1g_run_film_grain(const av1g_frame_job* jobs, int32_t n, void* str
  * *launches (optional) receives the number of kernels launched. */
 av1g_status av1g_run_postfilter(const av1g_frame_job* jobs, int32_t n, int32_t mode,
                                 void* stream, int32_t* launches);
+
+/* Launch-shape autotuner for the post-filter stages.  Each stage is a
+ * grid-stride launch over a flattened tile list: its grid size (resident CTAs
+ * per SM) is a free parameter, and so is superres's tile width (256, 512 or
+ * 1024 output samples of a row).  av1g_autotune_postfilter runs the whole
+ * chain on the jobs once per candidate shape of each stage, in chain order
+ * (the stages are idempotent on their inputs), times three launches per
+ * candidate with CUDA events, and keeps the fastest for that stage and the
+ * batch's sample width (8-bit or high bit depth) for every later call in
+ * this process; it synchronizes `stream`.  cache_path (optional) receives
+ * the table as text ("stage hbd ctas_per_sm tile" per line);
+ * av1g_autotune_load reads such a file (av1g_engine_create does when
+ * av1g_config.autotune_cache names one); av1g_autotune_get reads one entry
+ * (stage 0 deblock, 1 CDEF, 2 superres, 3 LR, 4 film grain). */
+av1g_status av1g_autotune_postfilter(const av1g_frame_job* jobs, int32_t n, void* stream, const char* cache_path);
+av1g_status av1g_autotune_load(const char* cache_path);
+av1g_status av1g_autotune_get(int32_t stage, int32_t hbd, int32_t* ctas_per_sm, int32_t* tile);
 
 /* The §7.4 chain for a fixed set of jobs, captured once as a CUDA graph.
  * The frame records, tile prefixes and stage scratch live in one device

@@ -168,7 +168,7 @@ INTER_SINGLE, INTER_COMPOUND, INTER_INTRA = 0, 1, 2
 
 class Config(C.Structure):
     _fields_ = [("device", C.c_int32), ("max_batch", C.c_int32), ("hbm_budget_bytes", C.c_int64),
-                ("max_inflight_steps", C.c_int32), ("lanes", C.c_int32)]
+                ("max_inflight_steps", C.c_int32), ("lanes", C.c_int32), ("autotune_cache", C.c_char_p)]
 
 
 class SeqInfo(C.Structure):
@@ -227,6 +227,9 @@ _SIGS = {
     "av1g_run_postfilter": (C.c_int, [C.POINTER(FrameJob), C.c_int32, C.c_int32, C.c_void_p,
                                       C.POINTER(C.c_int32)]),
     "av1g_run_film_grain_noalloc": (C.c_int, [C.POINTER(FrameJob), C.c_int32, C.c_void_p]),
+    "av1g_autotune_postfilter": (C.c_int, [C.POINTER(FrameJob), C.c_int32, C.c_void_p, C.c_char_p]),
+    "av1g_autotune_load": (C.c_int, [C.c_char_p]),
+    "av1g_autotune_get": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "av1g_chain_graph_create": (C.c_int, [C.POINTER(FrameJob), C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
                                           C.POINTER(C.c_void_p)]),
     "av1g_chain_graph_launch": (C.c_int, [C.c_void_p, C.c_void_p]),

@@ -179,12 +179,12 @@ struct Batch {
     std::vector<int32_t> tiles[ST_COUNT + 1];
 };
 
-int stage_tiles(const FrameDev& F, int st) {
+int stage_tiles(const FrameDev& F, int st, int sr_tile) {
     if (st < ST_COUNT && !F.do_stage[st]) return 0;
     switch (st) {
         case ST_DEBLOCK: return tiles_deblock(F);
         case ST_CDEF: return tiles_cdef(F);
-        case ST_SUPERRES: return tiles_superres(F);
+        case ST_SUPERRES: return tiles_superres(F, sr_tile);
         case ST_LR: return tiles_lr(F);
         case ST_GRAIN: return tiles_grain_blend(F);
         default: return F.do_stage[ST_GRAIN] ? 1 : 0;  // template pass
@@ -202,6 +202,7 @@ struct Prepared {
     std::vector<size_t> lf_off, grain_off;
     std::vector<uint8_t> host;  // the uploaded prefix [0, off_scratch)
     int32_t totals[NS] = {};
+    StageShape shape[ST_COUNT] = {};  // launch shapes (by the first frame's sample width)
 };
 
 av1g_status prepare(const av1g_frame_job* jobs, int n, int stage_mask, int mode, Prepared& P) {
@@ -218,6 +219,7 @@ av1g_status prepare(const av1g_frame_job* jobs, int n, int stage_mask, int mode,
             return fail(st, "job %d: %s", i, m.c_str());
         }
     }
+    for (int st = 0; st < ST_COUNT; st++) P.shape[st] = stage_shape(st, P.b.frames[0].hbd);
     // layout: frames | starts (batched: NS x (n+1)) | per-frame starts (n x NS x 2) | scratch
     const int NS = Prepared::NS;
     P.off_starts = ((sizeof(FrameDev) * n) + 255) & ~(size_t)255;
@@ -269,7 +271,8 @@ void bind(Prepared& P, uint8_t* dev) {
     for (int st = 0; st < NS; st++) {
         int32_t acc = 0;
         for (int i = 0; i < n; i++) {
-            int c = (P.stage_mask & (1 << (st < ST_COUNT ? st : ST_GRAIN))) ? stage_tiles(P.b.frames[i], st) : 0;
+            int c = (P.stage_mask & (1 << (st < ST_COUNT ? st : ST_GRAIN)))
+                        ? stage_tiles(P.b.frames[i], st, P.shape[ST_SUPERRES].tile) : 0;
             hs[st * (n + 1) + i] = acc;
             hpf[(i * NS + st) * 2 + 0] = 0;
             hpf[(i * NS + st) * 2 + 1] = c;
@@ -291,12 +294,12 @@ int launch_all(const Prepared& P, const uint8_t* dev, cudaStream_t s) {
     auto launch_stage = [&](int st, const FrameDev* fr, const int32_t* starts, const int32_t* starts_tmpl, int nn,
                             int total, int total_tmpl, int cells) {
         switch (st) {
-            case ST_DEBLOCK: if (total) { launch_deblock(fr, starts, nn, total, cells, s); nl += 2; } break;
-            case ST_CDEF: if (total) { launch_cdef(fr, starts, nn, total, s); nl++; } break;
-            case ST_SUPERRES: if (total) { launch_superres(fr, starts, nn, total, s); nl++; } break;
-            case ST_LR: if (total) { launch_lr(fr, starts, nn, total, s); nl++; } break;
+            case ST_DEBLOCK: if (total) { launch_deblock(fr, starts, nn, total, cells, P.shape[st], s); nl += 2; } break;
+            case ST_CDEF: if (total) { launch_cdef(fr, starts, nn, total, P.shape[st], s); nl++; } break;
+            case ST_SUPERRES: if (total) { launch_superres(fr, starts, nn, total, P.shape[st], s); nl++; } break;
+            case ST_LR: if (total) { launch_lr(fr, starts, nn, total, P.shape[st], s); nl++; } break;
             case ST_GRAIN:
-                launch_grain(fr, starts_tmpl, starts, nn, total_tmpl, total, s);
+                launch_grain(fr, starts_tmpl, starts, nn, total_tmpl, total, P.shape[st], s);
                 nl += (total_tmpl > 0) + (total > 0);
                 break;
         }
@@ -450,6 +453,116 @@ av1g_status av1g_run_inter(const av1g_inter_job* jobs, int32_t n, void* stream) 
 av1g_status av1g_run_postfilter(const av1g_frame_job* jobs, int32_t n, int32_t mode, void* stream,
                                 int32_t* launches) {
     return run(jobs, n, (1 << ST_COUNT) - 1, mode, stream, launches);
+}
+
+av1g_status av1g_autotune_postfilter(const av1g_frame_job* jobs, int32_t n, void* stream, const char* cache_path) {
+    g_err.clear();
+    if (n <= 0 || !jobs) return fail(AV1G_EINVAL, "bad job array");
+    Prepared P;
+    av1g_status st = prepare(jobs, n, (1 << ST_COUNT) - 1, AV1G_MODE_BATCHED, P);
+    if (st != AV1G_OK) return st;
+    const int hbd = P.b.frames[0].hbd;
+    cudaStream_t s = (cudaStream_t)stream;
+    uint8_t* dev = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&dev, P.total_bytes, s);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
+    bind(P, dev);
+    e = cudaMemcpyAsync(dev, P.host.data(), P.off_scratch, cudaMemcpyHostToDevice, s);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    const FrameDev* fr = (const FrameDev*)dev;
+    int32_t* hs = (int32_t*)(P.host.data() + P.off_starts);
+    const int32_t* ds = (const int32_t*)(dev + P.off_starts);
+    auto starts = [&](int stage) { return ds + stage * (n + 1); };
+    auto launch = [&](int stage, const StageShape& sh, int total) {
+        switch (stage) {
+            case ST_DEBLOCK: launch_deblock(fr, starts(stage), n, total, P.max_cells, sh, s); break;
+            case ST_CDEF: launch_cdef(fr, starts(stage), n, total, sh, s); break;
+            case ST_SUPERRES: launch_superres(fr, starts(stage), n, total, sh, s); break;
+            case ST_LR: launch_lr(fr, starts(stage), n, total, sh, s); break;
+            default:
+                launch_grain(fr, starts(ST_COUNT), starts(ST_GRAIN), n, P.totals[ST_COUNT], total, sh, s);
+                break;
+        }
+    };
+    // superres tile counts depend on the tile width
+    auto sr_total = [&](int tile) {
+        int32_t acc = 0;
+        for (int i = 0; i < n; i++) {
+            hs[ST_SUPERRES * (n + 1) + i] = acc;
+            acc += stage_tiles(P.b.frames[i], ST_SUPERRES, tile);
+        }
+        hs[ST_SUPERRES * (n + 1) + n] = acc;
+        return acc;
+    };
+    // in chain order, so every stage's input is the previous stage's output
+    for (int stage = 0; e == cudaSuccess && stage < ST_COUNT; stage++) {
+        if (P.totals[stage] == 0) continue;
+        std::vector<StageShape> cands;
+        static const int kCtas[ST_COUNT][6] = {{2, 4, 6, 8, 12, 16}, {2, 4, 6, 8, 12, 16}, {4, 8, 16, 32, 0, 0},
+                                               {2, 3, 4, 6, 8, 0}, {4, 8, 16, 32, 0, 0}};
+        for (int c : kCtas[stage]) {
+            if (!c) continue;
+            if (stage == ST_SUPERRES)
+                for (int t : {256, 512, 1024}) cands.push_back(StageShape{c, t});
+            else
+                cands.push_back(StageShape{c, 0});
+        }
+        StageShape best = P.shape[stage];
+        float best_ms = 1e30f;
+        for (const StageShape& sh : cands) {
+            int total = P.totals[stage];
+            if (stage == ST_SUPERRES) {
+                total = sr_total(sh.tile);
+                e = cudaMemcpyAsync(dev + P.off_starts + sizeof(int32_t) * ST_SUPERRES * (n + 1),
+                                    hs + ST_SUPERRES * (n + 1), sizeof(int32_t) * (n + 1), cudaMemcpyHostToDevice, s);
+                if (e != cudaSuccess) break;
+            }
+            launch(stage, sh, total);  // warm
+            e = cudaEventRecord(e0, s);
+            for (int r = 0; r < 3; r++) launch(stage, sh, total);
+            if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+            if (e == cudaSuccess) e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            float ms = 0.f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            if (e != cudaSuccess) break;
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = sh;
+            }
+        }
+        if (e == cudaSuccess) set_stage_shape(stage, hbd, best);
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFreeAsync(dev, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(e, "autotune");
+    if (cache_path) {
+        std::string err;
+        av1g_status sv = save_shapes(cache_path, err);
+        if (sv != AV1G_OK) return fail(sv, "%s", err.c_str());
+    }
+    return AV1G_OK;
+}
+
+av1g_status av1g_autotune_load(const char* cache_path) {
+    g_err.clear();
+    if (!cache_path) return fail(AV1G_EINVAL, "no cache path");
+    std::string err;
+    av1g_status st = load_shapes(cache_path, err);
+    return st == AV1G_OK ? st : fail(st, "%s", err.c_str());
+}
+
+av1g_status av1g_autotune_get(int32_t stage, int32_t hbd, int32_t* ctas_per_sm, int32_t* tile) {
+    g_err.clear();
+    if (stage < 0 || stage >= ST_COUNT || !ctas_per_sm || !tile) return fail(AV1G_EINVAL, "stage %d", stage);
+    const StageShape sh = stage_shape(stage, hbd);
+    *ctas_per_sm = sh.ctas_per_sm;
+    *tile = sh.tile;
+    return AV1G_OK;
 }
 
 struct av1g_chain_graph {
@@ -633,7 +746,7 @@ extern "C" av1g_status av1g_run_film_grain_noalloc(const av1g_frame_job* jobs, i
         e = cudaMemcpyAsync(base + off_starts, hs, sizeof(int32_t) * 2 * (n + 1), cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync");
     const int32_t* ds = (const int32_t*)(base + off_starts);
-    launch_grain((const FrameDev*)base, ds, ds + n + 1, n, tmpl, blend, s);
+    launch_grain((const FrameDev*)base, ds, ds + n + 1, n, tmpl, blend, stage_shape(ST_GRAIN, fr[0].hbd), s);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
     return AV1G_OK;

@@ -323,10 +323,10 @@ __global__ void __launch_bounds__(256, 3) cdef_kernel(const FrameDev* __restrict
 
 int tiles_cdef(const FrameDev& f) { return ((f.h.mi_rows + 15) >> 4) * ((f.h.mi_cols + 15) >> 4); }
 
-void launch_cdef(const FrameDev* frames, const int32_t* starts, int n, int total, cudaStream_t s) {
+void launch_cdef(const FrameDev* frames, const int32_t* starts, int n, int total, const StageShape& sh,
+                 cudaStream_t s) {
     if (total <= 0) return;
-    int grid = total < kSMs * 6 ? total : kSMs * 6;
-    cdef_kernel<<<grid, 256, 0, s>>>(frames, starts, n, total);
+    cdef_kernel<<<shape_grid(sh, total), 256, 0, s>>>(frames, starts, n, total);
 }
 
 }  // namespace av1g

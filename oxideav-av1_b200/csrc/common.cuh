@@ -11,6 +11,7 @@
 
 #include <cstdint>
 #include <functional>
+#include <string>
 #include <cuda_runtime.h>
 
 #include "av1g.h"
@@ -85,22 +86,40 @@ __device__ __forceinline__ void st_px(const PlaneDev& P, int hbd, int y, int x, 
     else row[x] = (uint8_t)v;
 }
 
+// Launch shape of a post-filter stage: resident CTAs per SM of its
+// grid-stride launch and, for superres, the output samples of a row per tile
+// (256, 512 or 1024).  autotune.cu holds the current choice per stage and
+// sample width; av1g_autotune_postfilter measures the candidates.
+struct StageShape {
+    int ctas_per_sm;
+    int tile;
+};
+StageShape stage_shape(int stage, int hbd);
+void set_stage_shape(int stage, int hbd, const StageShape& sh);
+bool shape_valid(int stage, const StageShape& sh);
+int shape_grid(const StageShape& sh, int total);  // min(total, SMs x ctas_per_sm)
+av1g_status save_shapes(const char* path, std::string& err);
+av1g_status load_shapes(const char* path, std::string& err);
+
 // Stage launchers (one per .cu file).  Each takes the batch's device
-// FrameDev array, the stage's tile-start array (n+1 entries, device) and the
-// total tile count.
+// FrameDev array, the stage's tile-start array (n+1 entries, device), the
+// total tile count and the launch shape.
 void launch_deblock(const FrameDev* frames, const int32_t* starts, int n, int total, int max_cells,
-                    cudaStream_t s);
-void launch_cdef(const FrameDev* frames, const int32_t* starts, int n, int total, cudaStream_t s);
-void launch_superres(const FrameDev* frames, const int32_t* starts, int n, int total, cudaStream_t s);
-void launch_lr(const FrameDev* frames, const int32_t* starts, int n, int total, cudaStream_t s);
+                    const StageShape& sh, cudaStream_t s);
+void launch_cdef(const FrameDev* frames, const int32_t* starts, int n, int total, const StageShape& sh,
+                 cudaStream_t s);
+void launch_superres(const FrameDev* frames, const int32_t* starts, int n, int total, const StageShape& sh,
+                     cudaStream_t s);
+void launch_lr(const FrameDev* frames, const int32_t* starts, int n, int total, const StageShape& sh,
+               cudaStream_t s);
 void launch_grain(const FrameDev* frames, const int32_t* starts_tmpl, const int32_t* starts_blend,
-                  int n, int total_tmpl, int total_blend, cudaStream_t s);
+                  int n, int total_tmpl, int total_blend, const StageShape& sh, cudaStream_t s);
 
 // Host-side tile counts (must match the kernels' tile decomposition).
 int tiles_deblock(const FrameDev& f);
 int cells_deblock(const FrameDev& f);  // 4x4 cells over all planes (deblock scratch: 2 bytes each)
 int tiles_cdef(const FrameDev& f);
-int tiles_superres(const FrameDev& f);
+int tiles_superres(const FrameDev& f, int tile);
 int tiles_lr(const FrameDev& f);
 int tiles_grain_blend(const FrameDev& f);
 

@@ -343,11 +343,10 @@ int cells_deblock(const FrameDev& f) {
 }
 
 void launch_deblock(const FrameDev* frames, const int32_t* starts, int n, int total, int max_cells,
-                    cudaStream_t s) {
+                    const StageShape& sh, cudaStream_t s) {
     if (total <= 0) return;
     lf_prep_kernel<<<dim3((max_cells + 255) / 256, n), 256, 0, s>>>(frames);
-    int grid = total < kSMs * 6 ? total : kSMs * 6;
-    deblock_kernel<<<grid, 256, 0, s>>>(frames, starts, n, total);
+    deblock_kernel<<<shape_grid(sh, total), 256, 0, s>>>(frames, starts, n, total);
 }
 
 }  // namespace av1g

@@ -780,6 +780,13 @@ av1g_status av1g_engine_create(const av1g_config* cfg, av1g_engine** out) {
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     E->budget = cfg->hbm_budget_bytes > 0 ? (size_t)cfg->hbm_budget_bytes : free_b / 10 * 8;
+    if (cfg->autotune_cache) {
+        std::string err;
+        if (load_shapes(cfg->autotune_cache, err) != AV1G_OK) {
+            delete E;
+            return AV1G_EINVAL;
+        }
+    }
     for (int i = 0; i < nl; i++) {
         auto L = std::make_unique<Lane>();
         L->idx = i;

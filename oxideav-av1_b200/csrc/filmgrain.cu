@@ -393,12 +393,9 @@ int tiles_grain_blend(const FrameDev& f) {
 }
 
 void launch_grain(const FrameDev* frames, const int32_t* starts_tmpl, const int32_t* starts_blend, int n,
-                  int total_tmpl, int total_blend, cudaStream_t s) {
+                  int total_tmpl, int total_blend, const StageShape& sh, cudaStream_t s) {
     if (total_tmpl > 0) grain_template_kernel<<<total_tmpl, 128, 0, s>>>(frames, starts_tmpl, n, total_tmpl);
-    if (total_blend > 0) {
-        int grid = total_blend < kSMs * 8 ? total_blend : kSMs * 8;
-        grain_blend_kernel<<<grid, 256, 0, s>>>(frames, starts_blend, n, total_blend);
-    }
+    if (total_blend > 0) grain_blend_kernel<<<shape_grid(sh, total_blend), 256, 0, s>>>(frames, starts_blend, n, total_blend);
 }
 
 }  // namespace av1g

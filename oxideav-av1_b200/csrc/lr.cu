@@ -417,12 +417,12 @@ int tiles_lr(const FrameDev& f) {
     return n;
 }
 
-void launch_lr(const FrameDev* frames, const int32_t* starts, int n, int total, cudaStream_t s) {
+void launch_lr(const FrameDev* frames, const int32_t* starts, int n, int total, const StageShape& sh,
+               cudaStream_t s) {
     if (total <= 0) return;
     size_t bytes = lr_smem_bytes();
     cudaFuncSetAttribute(lr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    int grid = total < kSMs * 4 ? total : kSMs * 4;
-    lr_kernel<<<grid, 256, bytes, s>>>(frames, starts, n, total);
+    lr_kernel<<<shape_grid(sh, total), 256, bytes, s>>>(frames, starts, n, total);
 }
 
 }  // namespace av1g

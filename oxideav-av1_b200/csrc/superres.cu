@@ -4,12 +4,13 @@
 // (src/superres.rs:282-445) as called at frame_driver.rs:906-966: both the
 // CDEF output and (when loop restoration is on) the deblocked frame are
 // upscaled from the padded FrameWidth-wide planes to exact UpscaledWidth x
-// FrameHeight planes.  A tile is 512 output samples of one row of one plane
-// of one source set: the CTA stages the source window those outputs read
-// (clamped to the mi-padded width exactly as the reference clamps every tap)
-// and the 64-phase filter table in shared memory, then each thread produces
-// four adjacent outputs with the 8-tap polyphase kernel at the 14-bit
-// fixed-point step and stores them as one vector.
+// FrameHeight planes.  A tile is 256, 512 or 1024 output samples (the launch
+// shape's tile width) of one row of one plane of one source set: the CTA
+// stages the source window those outputs read (clamped to the mi-padded
+// width exactly as the reference clamps every tap) and the 64-phase filter
+// table in shared memory, then each thread produces groups of four adjacent
+// outputs with the 8-tap polyphase kernel at the 14-bit fixed-point step and
+// stores each group as one vector.
 #include "common.cuh"
 #include "av1_spec_tables.h"
 
@@ -21,12 +22,12 @@ namespace {
 
 __device__ __forceinline__ int r2u(int x, int n) { return n ? (x + (1 << (n - 1))) >> n : x; }
 
-constexpr int kSrOut = 512;          // output samples of a row per tile
-constexpr int kSrThreads = 128;      // 4 outputs per thread
-constexpr int kSrWin = 2 * kSrOut + 16;  // source window (step <= 2): 2 * 512 + 8 taps, rounded up
+constexpr int kSrMaxOut = 1024;          // output samples of a row per tile: 256, 512 or 1024 (launch shape)
+constexpr int kSrThreads = 128;          // groups of 4 outputs per thread
+constexpr int kSrWin = kSrMaxOut + 16;   // source window: the step is below 1, plus 8 taps, rounded up
 
 // Output segments of a plane row.
-__device__ __host__ __forceinline__ int sr_segs(int uw) { return (uw + kSrOut - 1) / kSrOut; }
+__device__ __host__ __forceinline__ int sr_segs(int uw, int tile) { return (uw + tile - 1) / tile; }
 
 // A plane of one source set, as a run of tiles: its step, start phase and
 // the clamp bound shared by all its rows.
@@ -35,7 +36,7 @@ struct SrPlane {
     int set, plane, step_x, init, lim, uw, maxv;
 };
 
-__device__ SrPlane sr_plane(const av1g_frame_header& h, int local, int cap_w) {
+__device__ SrPlane sr_plane(const av1g_frame_header& h, int local, int cap_w, int tile) {
     SrPlane P{};
     int first = 0;
     const int nsets = h.uses_lr ? 2 : 1;
@@ -43,7 +44,7 @@ __device__ SrPlane sr_plane(const av1g_frame_header& h, int local, int cap_w) {
         for (int p = 0; p < h.num_planes; p++) {
             const int ssx = p ? h.subsampling_x : 0;
             const int rows = r2u(h.frame_height, p ? h.subsampling_y : 0);
-            const int uw = r2u(h.upscaled_width, ssx), segs = sr_segs(uw);
+            const int uw = r2u(h.upscaled_width, ssx), segs = sr_segs(uw, tile);
             if (local < first + rows * segs || (s == nsets - 1 && p == h.num_planes - 1)) {
                 // upscale_plane's step and start (superres.rs:363-377)
                 const int dw = r2u(h.frame_width, ssx);
@@ -62,7 +63,8 @@ __device__ SrPlane sr_plane(const av1g_frame_header& h, int local, int cap_w) {
 }
 
 __global__ void __launch_bounds__(kSrThreads) superres_kernel(const FrameDev* __restrict__ frames,
-                                                              const int32_t* __restrict__ starts, int n, int total) {
+                                                              const int32_t* __restrict__ starts, int n, int total,
+                                                              int tile) {
     __shared__ __align__(16) int16_t filt[64][8];
     __shared__ uint16_t win[kSrWin];
     for (int i = threadIdx.x; i < 64 * 8; i += kSrThreads) filt[i >> 3][i & 7] = (int16_t)c_upscale[i >> 3][i & 7];
@@ -81,7 +83,7 @@ __global__ void __launch_bounds__(kSrThreads) superres_kernel(const FrameDev* __
                 F = &frames[f];
             }
             const int local = t - starts[f];
-            P = sr_plane(F->h, local, 1 << 30);
+            P = sr_plane(F->h, local, 1 << 30, tile);
             const PlaneDev& S0 = P.set == 0 ? F->cdef[P.plane] : F->deb[P.plane];
             P.lim = min(P.lim, S0.w - 1);
             y = (local - P.first) / P.segs;
@@ -90,7 +92,7 @@ __global__ void __launch_bounds__(kSrThreads) superres_kernel(const FrameDev* __
         const PlaneDev& S = P.set == 0 ? F->cdef[P.plane] : F->deb[P.plane];
         const PlaneDev& D = P.set == 0 ? F->upcdef[P.plane] : F->updeb[P.plane];
         const int hbd = F->hbd;
-        const int x0 = seg * kSrOut, x1 = min(P.uw, x0 + kSrOut);
+        const int x0 = seg * tile, x1 = min(P.uw, x0 + tile);
         const int lo = ((-(1 << 14) + P.init + x0 * P.step_x) >> 14) - 3;
         const int hi = ((-(1 << 14) + P.init + (x1 - 1) * P.step_x) >> 14) + 4;
         __syncthreads();  // the previous tile's window is no longer read
@@ -100,8 +102,7 @@ __global__ void __launch_bounds__(kSrThreads) superres_kernel(const FrameDev* __
             win[i] = hbd ? reinterpret_cast<const uint16_t*>(srow)[sx] : srow[sx];
         }
         __syncthreads();
-        const int xb = x0 + 4 * threadIdx.x;
-        if (xb < x1) {
+        for (int xb = x0 + 4 * threadIdx.x; xb < x1; xb += 4 * kSrThreads) {
             int v[4];
 #pragma unroll
             for (int j = 0; j < 4; j++) {
@@ -137,21 +138,21 @@ __global__ void __launch_bounds__(kSrThreads) superres_kernel(const FrameDev* __
 
 }  // namespace
 
-int tiles_superres(const FrameDev& f) {
+int tiles_superres(const FrameDev& f, int tile) {
     int tiles = 0;
     for (int p = 0; p < f.h.num_planes; p++) {
         const int ssy = p ? f.h.subsampling_y : 0, ssx = p ? f.h.subsampling_x : 0;
         const int rows = ssy ? (f.h.frame_height + 1) >> 1 : f.h.frame_height;
         const int uw = ssx ? (f.h.upscaled_width + 1) >> 1 : f.h.upscaled_width;
-        tiles += rows * sr_segs(uw);
+        tiles += rows * sr_segs(uw, tile);
     }
     return tiles * (f.h.uses_lr ? 2 : 1);
 }
 
-void launch_superres(const FrameDev* frames, const int32_t* starts, int n, int total, cudaStream_t s) {
+void launch_superres(const FrameDev* frames, const int32_t* starts, int n, int total, const StageShape& sh,
+                     cudaStream_t s) {
     if (total <= 0) return;
-    int grid = total < kSMs * 16 ? total : kSMs * 16;
-    superres_kernel<<<grid, kSrThreads, 0, s>>>(frames, starts, n, total);
+    superres_kernel<<<shape_grid(sh, total), kSrThreads, 0, s>>>(frames, starts, n, total, sh.tile);
 }
 
 }  // namespace av1g
