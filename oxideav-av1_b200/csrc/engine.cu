@@ -163,15 +163,18 @@ struct av1g_engine {
     std::multimap<size_t, uint8_t*> pinned_free;
 
     uint8_t* pinned_get(size_t n) {
+        // power-of-two capacities (from 256 KiB), so buffers recycle across
+        // frames of similar size
+        size_t cap = (size_t)256 << 10;
+        while (cap < n) cap <<= 1;
         std::lock_guard<std::mutex> lk(pin_mu);
-        auto it = pinned_free.lower_bound(n);
-        if (it != pinned_free.end() && it->first < 2 * n + (1 << 20)) {
+        auto it = pinned_free.lower_bound(cap);
+        if (it != pinned_free.end() && it->first <= 2 * cap) {
             uint8_t* p = it->second;
             pinned_free.erase(it);
             return p;
         }
         uint8_t* p = nullptr;
-        size_t cap = (n + 4095) & ~(size_t)4095;
         if (cudaHostAlloc((void**)&p, cap + sizeof(size_t), cudaHostAllocPortable) != cudaSuccess) return nullptr;
         *(size_t*)p = cap;
         return p + sizeof(size_t);
@@ -390,7 +393,8 @@ void enqueue_step(av1g_engine* E, cudaStream_t cs, std::vector<std::shared_ptr<T
             // the frame's grids, CDEF indices, LR units and coefficients,
             // assembled straight into the pinned staging block
             e = upload_with(w.B.dev, w.B.host_bytes, cs, [&](uint8_t* blob) {
-                memset(blob, 0, w.B.host_bytes);
+                // the arrays cover the blob but for alignment gaps (and arrays
+                // a frame does not have), which nothing reads
                 for (int g = 0; g < 9; g++)
                     if (!t.grid[g].empty()) memcpy(blob + w.blob_off[g], t.grid[g].data(), t.grid[g].size());
                 if (!t.cdef_idx.empty()) memcpy(blob + w.blob_off[9], t.cdef_idx.data(), t.cdef_idx.size());

@@ -7,8 +7,11 @@
 // engine.  upload() instead copies the bytes into a pinned block and enqueues
 // the copy from there (upload_with() lets the caller build the bytes in the
 // block directly); a block is reused once the event recorded after its copy
-// has completed.
+// has completed.  Idle blocks wait in power-of-two capacity classes; blocks in
+// flight queue in enqueue order and only the oldest few are polled per call,
+// so an upload costs a handful of event queries however large the pool grows.
 #include <cstring>
+#include <deque>
 #include <functional>
 #include <mutex>
 #include <vector>
@@ -21,18 +24,44 @@ namespace {
 
 struct Block {
     void* p = nullptr;
-    size_t cap = 0;
+    size_t cap = 0;  // a power of two
     cudaEvent_t ev = nullptr;
     int device = -1;
-    bool busy = false;  // taken by a caller that has not recorded its event yet
 };
 
 constexpr size_t kMinBlock = 64 << 10;
 constexpr size_t kMaxPinned = (size_t)2 << 30;  // beyond this, copy from pageable memory
+constexpr int kClasses = 40;                    // capacity 2^k
+constexpr int kPollPerCall = 8;                 // in-flight blocks checked per upload
 
 std::mutex g_mu;
-std::vector<Block*> g_blocks;  // stable addresses: callers hold a block outside the lock
+std::vector<Block*> g_free[kClasses];  // idle blocks by capacity class
+std::deque<Block*> g_busy;             // blocks whose copy was enqueued, oldest first
 size_t g_pinned = 0;
+
+int cls(size_t cap) {
+    int k = 0;
+    while (((size_t)1 << k) < cap) k++;
+    return k;
+}
+
+// Moves finished blocks among the oldest kPollPerCall in flight to the free
+// lists (streams finish out of order, so a pending block does not stop the
+// scan); called with g_mu held.
+cudaError_t reap() {
+    for (size_t i = 0, polled = 0; i < g_busy.size() && polled < (size_t)kPollPerCall; polled++) {
+        Block* b = g_busy[i];
+        cudaError_t q = cudaEventQuery(b->ev);
+        if (q == cudaErrorNotReady) {
+            i++;
+            continue;
+        }
+        if (q != cudaSuccess) return q;
+        g_busy.erase(g_busy.begin() + i);
+        g_free[cls(b->cap)].push_back(b);
+    }
+    return cudaSuccess;
+}
 
 }  // namespace
 
@@ -41,21 +70,25 @@ cudaError_t upload_with(void* dev, size_t n, cudaStream_t s, const std::function
     int device = 0;
     cudaError_t e = cudaGetDevice(&device);
     if (e != cudaSuccess) return e;
+    size_t cap = kMinBlock;
+    while (cap < n) cap <<= 1;
     Block* pick = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_mu);
-        for (Block* b : g_blocks) {
-            if (b->busy || b->device != device || b->cap < n) continue;
-            cudaError_t q = cudaEventQuery(b->ev);
-            if (q == cudaSuccess) {
-                if (!pick || b->cap < pick->cap) pick = b;
-            } else if (q != cudaErrorNotReady) {
-                return q;
-            }
+        e = reap();
+        if (e != cudaSuccess) return e;
+        // the smallest idle block of this device that fits (at most 4x larger)
+        for (int k = cls(cap); k < kClasses && k <= cls(cap) + 2 && !pick; k++) {
+            auto& fl = g_free[k];
+            for (size_t i = 0; i < fl.size(); i++)
+                if (fl[i]->device == device) {
+                    pick = fl[i];
+                    fl[i] = fl.back();
+                    fl.pop_back();
+                    break;
+                }
         }
         if (!pick) {
-            size_t cap = kMinBlock;
-            while (cap < n) cap <<= 1;
             if (g_pinned + cap > kMaxPinned) {
                 // beyond the pinned budget: a copy from pageable memory, which
                 // returns once the driver has staged the bytes
@@ -78,16 +111,15 @@ cudaError_t upload_with(void* dev, size_t n, cudaStream_t s, const std::function
                 return e;
             }
             g_pinned += cap;
-            g_blocks.push_back(b);
             pick = b;
         }
-        pick->busy = true;
     }
     fill(static_cast<uint8_t*>(pick->p));
     e = cudaMemcpyAsync(dev, pick->p, n, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaEventRecord(pick->ev, s);
     std::lock_guard<std::mutex> lk(g_mu);
-    pick->busy = false;
+    if (e == cudaSuccess) g_busy.push_back(pick);
+    else g_free[cls(pick->cap)].push_back(pick);  // nothing was enqueued from it
     return e;
 }
 
