@@ -251,50 +251,53 @@ __global__ void __launch_bounds__(128) grain_template_kernel(const FrameDev* __r
     }
 }
 
-// Noise of plane p at (y, x): the materialised noiseImage of the reference.
-struct NoiseCtx {
+// Noise of N adjacent samples of one plane, (y, x0 .. x0 + N - 1): the
+// materialised noiseImage of the reference (film_grain.rs:599-760) in closed
+// form.  x0 is a multiple of N and N divides the 16- or 32-sample noise block,
+// so the group lies in one block: one offset lookup serves all N samples.
+template <int N>
+struct Noise {
     const int16_t* tmpl;
     const uint8_t* offs;
-    int nblocks, tw;  // template row width
+    int nblocks, tw;  // blocks per stripe, template row width
     int psx, psy, overlap, gmin, gmax;
-    __device__ int g(int s, int k, int i, int j) const {
-        int o = offs[s * nblocks + k];
-        int ox = o >> 4, oy = o & 15;
-        int pox = psx ? 6 + ox : 9 + ox * 2, poy = psy ? 6 + oy : 9 + oy * 2;
-        return __ldg(&tmpl[(poy + i) * tw + pox + j]);
+
+    __device__ __forceinline__ const int16_t* block_row(int s, int k, int i) const {
+        const int o = offs[s * nblocks + k];
+        const int ox = o >> 4, oy = o & 15;
+        const int pox = psx ? 6 + ox : 9 + ox * 2, poy = psy ? 6 + oy : 9 + oy * 2;
+        return tmpl + (poy + i) * tw + pox;
     }
-    // value of noise stripe s, row i, column x after the horizontal overlap
-    __device__ int stripe(int s, int i, int x) const {
-        int bs = psx ? 4 : 5;
-        int k = x >> bs, j = x & ((1 << bs) - 1);
-        int v = g(s, k, i, j);
-        if (overlap && k > 0) {
-            if (psx == 0 && j < 2) {
-                int old = g(s, k - 1, i, j + 32);
-                v = j == 0 ? old * 27 + v * 17 : old * 17 + v * 27;
-                v = clip3(gmin, gmax, r2(v, 5));
-            } else if (psx && j == 0) {
-                int old = g(s, k - 1, i, 16);
-                v = clip3(gmin, gmax, r2(old * 23 + v * 22, 5));
+    // noise stripe s, row i, after the horizontal overlap blend
+    __device__ __forceinline__ void stripe(int s, int i, int x0, int (&v)[N]) const {
+        const int bs = psx ? 4 : 5;
+        const int k = x0 >> bs, j0 = x0 & ((1 << bs) - 1);
+        const int16_t* row = block_row(s, k, i) + j0;
+#pragma unroll
+        for (int e = 0; e < N; e++) v[e] = __ldg(row + e);
+        if (overlap && k > 0 && j0 == 0) {
+            const int16_t* old = block_row(s, k - 1, i);
+            if (psx == 0) {  // columns 0 and 1 blend with columns 32 and 33 of the left block
+                v[0] = clip3(gmin, gmax, r2(__ldg(old + 32) * 27 + v[0] * 17, 5));
+                if (N > 1) v[1] = clip3(gmin, gmax, r2(__ldg(old + 33) * 17 + v[1] * 27, 5));
+            } else {  // column 0 blends with column 16 of the left block
+                v[0] = clip3(gmin, gmax, r2(__ldg(old + 16) * 23 + v[0] * 22, 5));
             }
         }
-        return v;
     }
-    __device__ int noise(int y, int x) const {
-        int bs = psy ? 4 : 5;
-        int s = y >> bs, i = y & ((1 << bs) - 1);
-        int v = stripe(s, i, x);
-        if (overlap && s > 0) {
-            if (psy == 0 && i < 2) {
-                int old = stripe(s - 1, i + 32, x);
-                v = i == 0 ? old * 27 + v * 17 : old * 17 + v * 27;
-                v = clip3(gmin, gmax, r2(v, 5));
-            } else if (psy && i == 0) {
-                int old = stripe(s - 1, 16, x);
-                v = clip3(gmin, gmax, r2(old * 23 + v * 22, 5));
+    __device__ __forceinline__ void noise(int y, int x0, int (&v)[N]) const {
+        const int bs = psy ? 4 : 5;
+        const int s = y >> bs, i = y & ((1 << bs) - 1);
+        stripe(s, i, x0, v);
+        if (overlap && s > 0 && (psy ? i == 0 : i < 2)) {
+            int old[N];
+            stripe(s - 1, psy ? 16 : i + 32, x0, old);
+#pragma unroll
+            for (int e = 0; e < N; e++) {
+                const int m = psy ? old[e] * 23 + v[e] * 22 : (i == 0 ? old[e] * 27 + v[e] * 17 : old[e] * 17 + v[e] * 27);
+                v[e] = clip3(gmin, gmax, r2(m, 5));
             }
         }
-        return v;
     }
 };
 
@@ -306,23 +309,169 @@ __device__ __forceinline__ int scale_lut(const uint8_t* lut, int index, int bd) 
     return a + r2((b - a) * rem, shift);
 }
 
-constexpr int BR = 8, BC = 256;
+// N samples of a row at x0: one vector access when the group is whole and the
+// row keeps it aligned, else sample by sample (x < w only).
+template <int N>
+__device__ __forceinline__ void ld_n(const PlaneDev& P, int hbd, int y, int x0, int w, int (&v)[N]) {
+    const uint8_t* row = P.p + (size_t)y * P.stride;
+    if (x0 + N <= w) {
+        if (hbd) {
+            if constexpr (N == 4) {
+                const uint2 u = *reinterpret_cast<const uint2*>(reinterpret_cast<const uint16_t*>(row) + x0);
+                v[0] = u.x & 0xffff; v[1] = u.x >> 16; v[2] = u.y & 0xffff; v[3] = u.y >> 16;
+                return;
+            } else if constexpr (N == 2) {
+                const uint32_t u = *reinterpret_cast<const uint32_t*>(reinterpret_cast<const uint16_t*>(row) + x0);
+                v[0] = u & 0xffff; v[1] = u >> 16;
+                return;
+            }
+        } else {
+            if constexpr (N == 4) {
+                const uint32_t u = *reinterpret_cast<const uint32_t*>(row + x0);
+                v[0] = u & 0xff; v[1] = (u >> 8) & 0xff; v[2] = (u >> 16) & 0xff; v[3] = u >> 24;
+                return;
+            } else if constexpr (N == 2) {
+                const uint16_t u = *reinterpret_cast<const uint16_t*>(row + x0);
+                v[0] = u & 0xff; v[1] = u >> 8;
+                return;
+            }
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < N; e++) v[e] = x0 + e < w ? ld_px(P, hbd, y, x0 + e) : 0;
+}
+template <int N>
+__device__ __forceinline__ void st_n(const PlaneDev& P, int hbd, int y, int x0, int w, const int (&v)[N]) {
+    uint8_t* row = P.p + (size_t)y * P.stride;
+    if (x0 + N <= w) {
+        if (hbd) {
+            if constexpr (N == 4) {
+                *reinterpret_cast<uint2*>(reinterpret_cast<uint16_t*>(row) + x0) =
+                    make_uint2((uint32_t)v[0] | ((uint32_t)v[1] << 16), (uint32_t)v[2] | ((uint32_t)v[3] << 16));
+                return;
+            } else if constexpr (N == 2) {
+                *reinterpret_cast<uint32_t*>(reinterpret_cast<uint16_t*>(row) + x0) =
+                    (uint32_t)v[0] | ((uint32_t)v[1] << 16);
+                return;
+            }
+        } else {
+            if constexpr (N == 4) {
+                *reinterpret_cast<uint32_t*>(row + x0) =
+                    (uint32_t)v[0] | ((uint32_t)v[1] << 8) | ((uint32_t)v[2] << 16) | ((uint32_t)v[3] << 24);
+                return;
+            } else if constexpr (N == 2) {
+                *reinterpret_cast<uint16_t*>(row + x0) = (uint16_t)(v[0] | (v[1] << 8));
+                return;
+            }
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < N; e++)
+        if (x0 + e < w) st_px(P, hbd, y, x0 + e, v[e]);
+}
+
+constexpr int BR = 8;      // chroma-resolution rows per tile
+constexpr int QPT = 256;   // groups of 4 luma columns per tile (one per thread)
+
+// One chroma-resolution row yc of a group: CQ = 4 >> ssx chroma samples of
+// each chroma plane (blended from the un-noised luma first), then the
+// 4 x (1 << ssy) luma samples they cover, as the reference orders it
+// (film_grain.rs:758-828).
+template <int CQ>
+__device__ __forceinline__ void blend_group(const FrameDev& F, const av1g_film_grain& fg, const uint8_t (*lut)[256],
+                                            int q, int yc, int gmin, int gmax, int minv, int maxl, int maxc) {
+    const int bd = F.h.bit_depth, hbd = F.hbd;
+    const int np = F.h.num_planes;
+    const int ssx = np > 1 ? F.h.subsampling_x : 0, ssy = np > 1 ? F.h.subsampling_y : 0;
+    const int w = F.out[0].w, h = F.out[0].h;
+    const int gw = (w + ssx) >> ssx;
+    const int x0 = q * 4, xc0 = q * CQ, ly = yc << ssy;
+    if (np >= 3 && xc0 < gw) {
+        const bool chroma = fg.num_cb_points > 0 || fg.num_cr_points > 0 || fg.chroma_scaling_from_luma;
+        int avg[CQ];
+        if (chroma) {
+            int l[4];
+            ld_n<4>(F.lr[0], hbd, ly, x0, w, l);
+            if (ssx) {
+                // average of the two luma columns, the right one clamped to the plane
+#pragma unroll
+                for (int c = 0; c < CQ; c++) {
+                    const int bx = 2 * c + 1;
+                    avg[c] = r2(l[2 * c] + (x0 + bx < w ? l[bx] : l[min(w - 1 - x0, 3)]), 1);
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < CQ; c++) avg[c] = l[c];
+            }
+        }
+        for (int p = 1; p <= 2; p++) {
+            int orig[CQ];
+            ld_n<CQ>(F.lr[p], hbd, yc, xc0, gw, orig);
+            const int npts = p == 1 ? fg.num_cb_points : fg.num_cr_points;
+            if (!(npts > 0 || fg.chroma_scaling_from_luma)) {
+                st_n<CQ>(F.out[p], hbd, yc, xc0, gw, orig);
+                continue;
+            }
+            const Noise<CQ> nc{F.grain_tmpl + p * LH * LW, F.grain_offs, F.grain_nblocks, F.h.subsampling_x ? 44 : 82,
+                               F.h.subsampling_x, F.h.subsampling_y, fg.overlap_flag, gmin, gmax};
+            int nz[CQ];
+            nc.noise(yc, xc0, nz);
+            const int lm = p == 1 ? fg.cb_luma_mult : fg.cr_luma_mult;
+            const int m = p == 1 ? fg.cb_mult : fg.cr_mult;
+            const int off = p == 1 ? fg.cb_offset : fg.cr_offset;
+            int o[CQ];
+#pragma unroll
+            for (int c = 0; c < CQ; c++) {
+                int merged;
+                if (fg.chroma_scaling_from_luma) {
+                    merged = avg[c];
+                } else {
+                    const int comb = avg[c] * (lm - 128) + orig[c] * (m - 128);
+                    merged = clip3(0, (1 << bd) - 1, (comb >> 6) + (off - 256) * (1 << (bd - 8)));
+                }
+                o[c] = clip3(minv, maxc, orig[c] + r2(scale_lut(lut[p], merged, bd) * nz[c], fg.grain_scaling));
+            }
+            st_n<CQ>(F.out[p], hbd, yc, xc0, gw, o);
+        }
+    }
+    if (x0 >= w) return;
+    const Noise<4> nl{F.grain_tmpl, F.grain_offs, F.grain_nblocks, LW, 0, 0, fg.overlap_flag, gmin, gmax};
+    for (int dy = 0; dy <= ssy; dy++) {
+        const int y = ly + dy;
+        if (y >= h) break;
+        int orig[4];
+        ld_n<4>(F.lr[0], hbd, y, x0, w, orig);
+        if (fg.num_y_points > 0) {
+            int nz[4];
+            nl.noise(y, x0, nz);
+#pragma unroll
+            for (int e = 0; e < 4; e++)
+                orig[e] = clip3(minv, maxl, orig[e] + r2(scale_lut(lut[0], orig[e], bd) * nz[e], fg.grain_scaling));
+        }
+        st_n<4>(F.out[0], hbd, y, x0, w, orig);
+    }
+}
 
 __global__ void __launch_bounds__(256) grain_blend_kernel(const FrameDev* __restrict__ frames,
                                                           const int32_t* __restrict__ starts, int n, int total) {
+    __shared__ uint8_t lut[3][256];
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
-        int f = find_frame(starts, n, t);
+        const int f = find_frame(starts, n, t);
         const FrameDev& F = frames[f];
         const av1g_film_grain& fg = F.h.film_grain;
-        const int bd = F.h.bit_depth, hbd = F.hbd;
-        const int ssx = F.h.num_planes > 1 ? F.h.subsampling_x : 0, ssy = F.h.num_planes > 1 ? F.h.subsampling_y : 0;
+        const int bd = F.h.bit_depth;
+        const int np = F.h.num_planes;
+        const int ssx = np > 1 ? F.h.subsampling_x : 0, ssy = np > 1 ? F.h.subsampling_y : 0;
         const int w = F.out[0].w, h = F.out[0].h;
-        const int gw = (w + ssx) >> ssx, gh = (h + ssy) >> ssy;
-        const int ntc = (gw + BC - 1) / BC;
-        int local = t - starts[f];
-        int tr = local / ntc, tc = local % ntc;
-        int xc = tc * BC + threadIdx.x;
-        if (xc >= gw) continue;
+        const int gh = (h + ssy) >> ssy, nq = (w + 3) >> 2;
+        const int ntc = (nq + QPT - 1) / QPT;
+        const int local = t - starts[f];
+        const int tr = local / ntc, tc = local % ntc;
+        __syncthreads();  // the previous tile's LUTs are no longer read
+        for (int i = threadIdx.x; i < 3 * 256; i += blockDim.x) lut[i >> 8][i & 255] = F.grain_lut[i];
+        __syncthreads();
+        const int q = tc * QPT + threadIdx.x;
+        if (q >= nq) continue;
         const int center = 128 << (bd - 8), gmin = -center, gmax = (256 << (bd - 8)) - 1 - center;
         int minv, maxl, maxc;
         if (fg.clip_to_restricted_range) {
@@ -333,53 +482,9 @@ __global__ void __launch_bounds__(256) grain_blend_kernel(const FrameDev* __rest
             minv = 0;
             maxl = maxc = (256 << (bd - 8)) - 1;
         }
-        const int cw = F.h.subsampling_x ? 44 : 82;
-        NoiseCtx nl{F.grain_tmpl, F.grain_offs, F.grain_nblocks, LW, 0, 0, fg.overlap_flag, gmin, gmax};
-        const bool chroma = F.h.num_planes >= 3 &&
-                            (fg.num_cb_points > 0 || fg.num_cr_points > 0 || fg.chroma_scaling_from_luma);
         for (int yc = tr * BR; yc < min(gh, tr * BR + BR); yc++) {
-            int ly = yc << ssy, lx = xc << ssx;
-            if (chroma) {
-                int lnx = min(lx + 1, w - 1);
-                int y0 = ld_px(F.lr[0], hbd, ly, lx);
-                int avg = ssx ? r2(y0 + ld_px(F.lr[0], hbd, ly, lnx), 1) : y0;
-                for (int p = 1; p <= 2; p++) {
-                    int np_ = p == 1 ? fg.num_cb_points : fg.num_cr_points;
-                    if (!(np_ > 0 || fg.chroma_scaling_from_luma)) {
-                        st_px(F.out[p], hbd, yc, xc, ld_px(F.lr[p], hbd, yc, xc));
-                        continue;
-                    }
-                    int orig = ld_px(F.lr[p], hbd, yc, xc);
-                    int merged;
-                    if (fg.chroma_scaling_from_luma) {
-                        merged = avg;
-                    } else {
-                        int lm = p == 1 ? fg.cb_luma_mult : fg.cr_luma_mult;
-                        int m = p == 1 ? fg.cb_mult : fg.cr_mult;
-                        int off = p == 1 ? fg.cb_offset : fg.cr_offset;
-                        int comb = avg * (lm - 128) + orig * (m - 128);
-                        merged = clip3(0, (1 << bd) - 1, (comb >> 6) + (off - 256) * (1 << (bd - 8)));
-                    }
-                    NoiseCtx nc{F.grain_tmpl + p * LH * LW, F.grain_offs, F.grain_nblocks, cw,
-                                F.h.subsampling_x, F.h.subsampling_y, fg.overlap_flag, gmin, gmax};
-                    int nz = r2(scale_lut(F.grain_lut + p * 256, merged, bd) * nc.noise(yc, xc), fg.grain_scaling);
-                    st_px(F.out[p], hbd, yc, xc, clip3(minv, maxc, orig + nz));
-                }
-            } else if (F.h.num_planes >= 3) {
-                for (int p = 1; p <= 2; p++) st_px(F.out[p], hbd, yc, xc, ld_px(F.lr[p], hbd, yc, xc));
-            }
-            for (int dy = 0; dy <= ssy; dy++)
-                for (int dx = 0; dx <= ssx; dx++) {
-                    int y = ly + dy, x = lx + dx;
-                    if (y >= h || x >= w) continue;
-                    int orig = ld_px(F.lr[0], hbd, y, x);
-                    int o = orig;
-                    if (fg.num_y_points > 0) {
-                        int nz = r2(scale_lut(F.grain_lut, orig, bd) * nl.noise(y, x), fg.grain_scaling);
-                        o = clip3(minv, maxl, orig + nz);
-                    }
-                    st_px(F.out[0], hbd, y, x, o);
-                }
+            if (ssx) blend_group<2>(F, fg, lut, q, yc, gmin, gmax, minv, maxl, maxc);
+            else blend_group<4>(F, fg, lut, q, yc, gmin, gmax, minv, maxl, maxc);
         }
     }
 }
@@ -387,9 +492,9 @@ __global__ void __launch_bounds__(256) grain_blend_kernel(const FrameDev* __rest
 }  // namespace
 
 int tiles_grain_blend(const FrameDev& f) {
-    int ssx = f.h.num_planes > 1 ? f.h.subsampling_x : 0, ssy = f.h.num_planes > 1 ? f.h.subsampling_y : 0;
-    int gw = (f.out[0].w + ssx) >> ssx, gh = (f.out[0].h + ssy) >> ssy;
-    return ((gh + BR - 1) / BR) * ((gw + BC - 1) / BC);
+    int ssy = f.h.num_planes > 1 ? f.h.subsampling_y : 0;
+    int gh = (f.out[0].h + ssy) >> ssy, nq = (f.out[0].w + 3) >> 2;
+    return ((gh + BR - 1) / BR) * ((nq + QPT - 1) / QPT);
 }
 
 void launch_grain(const FrameDev* frames, const int32_t* starts_tmpl, const int32_t* starts_blend, int n,

@@ -30,6 +30,10 @@ CASES = [
     dict(seed=22, width=150, height=98, cdef=False, lr_types=(1, 0, 2)),    # cdef off, per-plane LR types
     dict(seed=23, width=1920, height=1080),                                 # full-size 1080p
     dict(seed=24, width=1920, height=1080, bit_depth=10),                   # full-size 10-bit
+    dict(seed=25, width=130, height=70, ssx=0, ssy=0, film_grain=True),     # 4:4:4 grain, odd width / 4
+    dict(seed=26, width=98, height=66, mono=True, film_grain=True),         # monochrome grain
+    dict(seed=27, width=177, height=143, film_grain=True),                  # odd sizes, grain
+    dict(seed=28, width=322, height=182, bit_depth=10, ssx=1, ssy=0, film_grain=True),  # 4:2:2 10-bit grain
 ]
 
 
