@@ -393,17 +393,22 @@ bool setup_shear(const int32_t p[6], bool* valid, int32_t abcd[4]) {
 }
 
 // motion_vector_scaling (inter_pred.rs:318).
-bool mv_scale(int ssx, int ssy, long long fw, long long fh, long long ruw, long long rh, int x, int y,
-              const int16_t mv[2], RefCall& rc) {
+// xScale / yScale of motion_vector_scaling (inter_pred.rs:318-330); false
+// for a zero frame or reference extent.
+bool ref_scale(long long fw, long long fh, long long ruw, long long rh, long long& xs, long long& ys) {
     if (fw <= 0 || fh <= 0 || ruw <= 0 || rh <= 0) return false;
-    long long xs = ((ruw << 14) + fw / 2) / fw, ys = ((rh << 14) + fh / 2) / fh;
+    xs = ((ruw << 14) + fw / 2) / fw;
+    ys = ((rh << 14) + fh / 2) / fh;
+    return true;
+}
+
+void mv_scale(int ssx, int ssy, long long xs, long long ys, int x, int y, const int16_t mv[2], RefCall& rc) {
     long long ox = ((long long)x << 4) + ((2 * (long long)mv[1]) >> ssx) + 8;
     long long oy = ((long long)y << 4) + ((2 * (long long)mv[0]) >> ssy) + 8;
     rc.sx = (int32_t)(rnd2s(ox * xs - (8LL << 14), 8) + 32);
     rc.sy = (int32_t)(rnd2s(oy * ys - (8LL << 14), 8) + 32);
     rc.stx = (int32_t)rnd2s(xs, 4);
     rc.sty = (int32_t)rnd2s(ys, 4);
-    return true;
 }
 
 int small_filter(int f, int n) {
@@ -422,6 +427,18 @@ struct Builder {
     std::vector<Seg>& segs;
     std::string& err;
     bool any_diff = false;
+    // per reference, computed once: its scale factors and whether each plane is usable
+    long long xs[7] = {}, ys[7] = {};
+    int8_t scale_ok[7] = {}, plane_ok[7][3] = {};
+
+    void init() {
+        const av1g_frame_header& hd = *job.hdr;
+        for (int r = 0; r < 7; r++) {
+            scale_ok[r] = ref_scale(hd.frame_width, hd.frame_height, job.refs[r].upscaled_width,
+                                    job.refs[r].frame_height, xs[r], ys[r]);
+            for (int p = 0; p < 3; p++) plane_ok[r][p] = p < hd.num_planes && ref_ok(r, p);
+        }
+    }
 
     bool bad(int k, const char* what) {
         err = "inter job " + std::to_string(fi) + ": call " + std::to_string(k) + ": " + what;
@@ -441,12 +458,10 @@ struct Builder {
 
     bool trans(int k, int plane, int ref, const int16_t mv[2], int x, int y, int w, int h, int fx, int fy,
                RefCall& rc) {
-        const av1g_frame_header& hd = *job.hdr;
         int sx = plane ? ssx_frame : 0, sy = plane ? ssy_frame : 0;
-        if (!mv_scale(sx, sy, hd.frame_width, hd.frame_height, job.refs[ref].upscaled_width,
-                      job.refs[ref].frame_height, x, y, mv, rc))
-            return bad(k, "zero frame or reference extent");
-        if (!ref_ok(ref, plane)) return bad(k, "reference plane smaller than its extent");
+        if (!scale_ok[ref]) return bad(k, "zero frame or reference extent");
+        mv_scale(sx, sy, xs[ref], ys[ref], x, y, mv, rc);
+        if (!plane_ok[ref][plane]) return bad(k, "reference plane smaller than its extent");
         if (fx >= 6 || fy >= 6) return bad(k, "interpolation filter");
         // The kernel's int32 position arithmetic covers references up to 16x
         // larger than the frame; conformant streams stay within 2x.
@@ -663,6 +678,11 @@ av1g_status inter_run(const av1g_inter_job* jobs, int n, cudaStream_t st, std::s
     std::vector<WarpRec> warps;
     std::vector<Seg> segs;
     std::vector<int> diff_frames;
+    {
+        size_t np = 0;
+        for (int i = 0; i < n; i++) np += jobs[i].num_preds > 0 ? (size_t)jobs[i].num_preds : 0;
+        a.reserve(np);
+    }
     for (int i = 0; i < n; i++) {
         const av1g_inter_job& j = jobs[i];
         if (!j.hdr || !j.refs || j.num_preds < 0 || (j.num_preds > 0 && !j.preds) || j.num_neighbours < 0 ||
@@ -706,6 +726,7 @@ av1g_status inter_run(const av1g_inter_job* jobs, int n, cudaStream_t st, std::s
             }
         }
         Builder B{j, i, h.subsampling_x, h.subsampling_y, F.hbd, a, b, warps, segs, err};
+        B.init();
         for (int k = 0; k < j.num_preds; k++)
             if (!B.add(k)) return AV1G_EINVAL;
         if (B.any_diff) {
@@ -742,15 +763,15 @@ av1g_status inter_run(const av1g_inter_job* jobs, int n, cudaStream_t st, std::s
         return AV1G_EDEVICE;
     }
     for (int i : diff_frames) frames[i].mask = dev + mask_off[i];
-    std::vector<uint8_t> host(host_bytes);
-    memcpy(host.data() + o_frames, frames.data(), sizeof(InterFrame) * n);
-    if (!a.empty()) memcpy(host.data() + o_a, a.data(), sizeof(Call) * a.size());
-    if (!b.empty()) memcpy(host.data() + o_b, b.data(), sizeof(Call) * b.size());
-    memcpy(host.data() + o_sa, sa.data(), sizeof(uint32_t) * sa.size());
-    memcpy(host.data() + o_sb, sb.data(), sizeof(uint32_t) * sb.size());
-    if (!warps.empty()) memcpy(host.data() + o_w, warps.data(), sizeof(WarpRec) * warps.size());
-    if (!segs.empty()) memcpy(host.data() + o_s, segs.data(), sizeof(Seg) * segs.size());
-    e = upload(dev, host.data(), host_bytes, st);
+    e = upload_with(dev, host_bytes, st, [&](uint8_t* host) {
+        memcpy(host + o_frames, frames.data(), sizeof(InterFrame) * n);
+        if (!a.empty()) memcpy(host + o_a, a.data(), sizeof(Call) * a.size());
+        if (!b.empty()) memcpy(host + o_b, b.data(), sizeof(Call) * b.size());
+        memcpy(host + o_sa, sa.data(), sizeof(uint32_t) * sa.size());
+        memcpy(host + o_sb, sb.data(), sizeof(uint32_t) * sb.size());
+        if (!warps.empty()) memcpy(host + o_w, warps.data(), sizeof(WarpRec) * warps.size());
+        if (!segs.empty()) memcpy(host + o_s, segs.data(), sizeof(Seg) * segs.size());
+    });
     if (e == cudaSuccess && bytes > host_bytes) e = cudaMemsetAsync(dev + host_bytes, 0, bytes - host_bytes, st);
     const InterFrame* df = (const InterFrame*)(dev + o_frames);
     const WarpRec* dw = (const WarpRec*)(dev + o_w);

@@ -97,7 +97,10 @@ av1g_status recon_run(const av1g_recon_job* jobs, int n, cudaStream_t s, std::st
     std::vector<TuDev> all;
     size_t total = 0;
     for (int i = 0; i < n; i++) total += jobs[i].num_tus > 0 ? jobs[i].num_tus : 0;
-    all.reserve(total);
+    // TUs bucketed by (size, type) so the threads of a warp run one butterfly
+    // network: a counting sort, stable in (job, decode order)
+    constexpr int kKeys = 19 * 16;
+    std::vector<uint32_t> count(kKeys + 1, 0);
     for (int i = 0; i < n; i++) {
         const av1g_recon_job& j = jobs[i];
         if (!j.hdr || !j.quant || (j.num_tus > 0 && (!j.tus || !j.coeffs)) || j.num_tus < 0) {
@@ -131,14 +134,17 @@ av1g_status recon_run(const av1g_recon_job* jobs, int n, cudaStream_t s, std::st
                 err = "recon job " + std::to_string(i) + ": TU " + std::to_string(k) + " has an invalid size/type/plane";
                 return AV1G_EINVAL;
             }
-            all.push_back(TuDev{t, i});
+            count[t.tx_size * 16 + t.tx_type + 1]++;
         }
     }
-    if (all.empty()) return AV1G_OK;
-    // bucket by (size, type) so the threads of a warp run one butterfly network
-    std::stable_sort(all.begin(), all.end(), [](const TuDev& a, const TuDev& b) {
-        return a.tu.tx_size != b.tu.tx_size ? a.tu.tx_size < b.tu.tx_size : a.tu.tx_type < b.tu.tx_type;
-    });
+    if (total == 0) return AV1G_OK;
+    for (int k = 1; k <= kKeys; k++) count[k] += count[k - 1];
+    all.resize(total);
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < jobs[i].num_tus; k++) {
+            const av1g_tu& t = jobs[i].tus[k];
+            all[count[t.tx_size * 16 + t.tx_type]++] = TuDev{t, i};
+        }
     std::vector<Task> tasks;
     for (size_t k = 0; k < all.size();) {
         int tx = all[k].tu.tx_size, cap = slots_for(tx);
@@ -150,17 +156,17 @@ av1g_status recon_run(const av1g_recon_job* jobs, int n, cudaStream_t s, std::st
     size_t off_tus = (sizeof(ReconFrame) * n + 255) & ~(size_t)255;
     size_t off_tasks = (off_tus + sizeof(TuDev) * all.size() + 255) & ~(size_t)255;
     size_t bytes = off_tasks + sizeof(Task) * tasks.size();
-    std::vector<uint8_t> host(bytes);
-    memcpy(host.data(), frames.data(), sizeof(ReconFrame) * n);
-    memcpy(host.data() + off_tus, all.data(), sizeof(TuDev) * all.size());
-    memcpy(host.data() + off_tasks, tasks.data(), sizeof(Task) * tasks.size());
     uint8_t* dev = nullptr;
     cudaError_t e = cudaMallocAsync((void**)&dev, bytes, s);
     if (e != cudaSuccess) {
         err = std::string("cudaMallocAsync: ") + cudaGetErrorString(e);
         return AV1G_EDEVICE;
     }
-    e = upload(dev, host.data(), bytes, s);
+    e = upload_with(dev, bytes, s, [&](uint8_t* host) {
+        memcpy(host, frames.data(), sizeof(ReconFrame) * n);
+        memcpy(host + off_tus, all.data(), sizeof(TuDev) * all.size());
+        memcpy(host + off_tasks, tasks.data(), sizeof(Task) * tasks.size());
+    });
     if (e == cudaSuccess) {
         int nt = (int)tasks.size();
         int grid = nt < kSMs * 16 ? nt : kSMs * 16;
