@@ -48,9 +48,9 @@ using namespace itx;
 constexpr int kT = 128;             // threads per CTA
 constexpr int kNW = kT / 32;        // warps per CTA
 constexpr int kSmallPx = kIntraSmallPx;
-constexpr int kLvChunk = 256;       // level-table entries staged at a time
+constexpr int kLvChunk = 64;        // level-table entries staged at a time
 constexpr int kTuWin = 128;         // TU records staged at a time
-constexpr int kWaitWin = 64;        // waits staged per superblock
+constexpr int kWaitWin = 32;        // waits staged per superblock (more: read from HBM)
 constexpr long long kWaitNs = 2000000000LL;
 
 __constant__ AV1T_MODE_TO_ANGLE_TYPE c_mode_angle AV1T_MODE_TO_ANGLE_DIMS = AV1T_MODE_TO_ANGLE_INIT;

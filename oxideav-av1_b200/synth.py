@@ -438,15 +438,16 @@ class IntraFrame(ReconFrame):
         self.sb_size = 64
 
 
-def _blocks(rng, x0, y0, n, pw, ph, out):
-    """Recursive square/rect partition of an n x n area (samples) into blocks, in decode order."""
+def _blocks(rng, x0, y0, n, pw, ph, out, split=0.55):
+    """Recursive square/rect partition of an n x n area (samples) into blocks,
+    in decode order; `split` is the probability of a quad split."""
     if x0 >= pw or y0 >= ph:
         return
-    if n > 4 and (rng.random() < 0.55 or x0 + n > pw or y0 + n > ph):
+    if n > 4 and (rng.random() < split or x0 + n > pw or y0 + n > ph):
         h = n // 2
         for dy in (0, h):
             for dx in (0, h):
-                _blocks(rng, x0 + dx, y0 + dy, h, pw, ph, out)
+                _blocks(rng, x0 + dx, y0 + dy, h, pw, ph, out, split)
         return
     r = rng.random()
     if n >= 8 and r < 0.2:
@@ -460,9 +461,10 @@ def _blocks(rng, x0, y0, n, pw, ph, out):
 
 
 def make_intra_frame(seed, width=176, height=144, bit_depth=8, ssx=1, ssy=1, mono=False, sb_size=64,
-                     edge_filter=True, palette=0.0, intrabc=0.0, intrabc_order="wavefront"):
+                     edge_filter=True, palette=0.0, intrabc=0.0, intrabc_order="wavefront", split=0.55):
     """Intra TUs in decode order.  palette / intrabc: probability that a block
-    is a palette block / an intra-block-copy block.  intrabc_order picks where
+    is a palette block / an intra-block-copy block; split: probability of a
+    quad split in the block partition.  intrabc_order picks where
     copies read from: "wavefront" (the superblock row above, within reach of
     the level-2 wavefront), "steep" (further right in the row above, which
     needs a steeper wavefront) or "raster" (the row below, not yet decoded,
@@ -486,7 +488,7 @@ def make_intra_frame(seed, width=176, height=144, bit_depth=8, ssx=1, ssy=1, mon
                 sx_, sy_ = (h.subsampling_x, h.subsampling_y) if p else (0, 0)
                 ph, pw = f.plane_dims(p)
                 blocks = []
-                _blocks(rng, sbx >> sx_, sby >> sy_, sb_size >> max(sx_, sy_), pw, ph, blocks)
+                _blocks(rng, sbx >> sx_, sby >> sy_, sb_size >> max(sx_, sy_), pw, ph, blocks, split)
                 for (bx, by, bw, bh) in blocks:
                     # a legal TU size for the block (Max_Tx_Size_Rect, optionally split once)
                     bw_, bh_ = min(bw, 64), min(bh, 64)

@@ -31,6 +31,10 @@ CASES = [
     dict(seed=92, width=640, height=360, intrabc=0.4, intrabc_order="steep"),
     dict(seed=93, width=1280, height=128, intrabc=0.5, intrabc_order="raster"),
     dict(seed=94, width=352, height=288, bit_depth=10, palette=0.2, intrabc=0.2, ssx=0, ssy=0),
+    # 128x128 superblocks of 4:4:4 4x4 TUs (thousands per superblock: the TU window slides)
+    dict(seed=96, width=256, height=192, sb_size=128, ssx=0, ssy=0, split=0.97),
+    # palette blocks read no neighbours: a superblock's tiny TUs share one level wider than the TU window
+    dict(seed=97, width=256, height=128, palette=1.0, split=0.95),
 ]
 
 
