@@ -352,6 +352,7 @@ def run_gpu(args):
     if rank == 0 and world == 1:
         line["recon_stages"] = run_recon_stages(args, dev, stream)
         line["extra_stages"] = run_extra_stages(args, dev, stream)
+        line["motion_field"] = run_motion_field(args, dev, stream)
     if rank == 0 and world == 1 and not args.no_serving:
         line["serving"] = run_serving(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -531,6 +532,64 @@ def run_extra_stages(args, dev, stream, templates=8, copies=6):
         del dfr, jobs
         torch.cuda.empty_cache()
     return out
+
+
+def run_motion_field(args, dev, stream, frames=16):
+    """Row f2 on 1920x1080 frames (mi 270 x 480): §7.19 storage of `frames`
+    decoded frames in one launch, then the §7.9 projection of `frames`
+    current frames (each from four stored slots, up to four passes) in one
+    call.  Device time per frame beside the oracle's single-thread time per
+    frame on the same inputs."""
+    import torch
+    from oxideav_av1_b200 import mfmv
+    import oracle
+    rows, cols = 270, 480
+    cells, pos = rows * cols, (rows >> 1) * (cols >> 1)
+    peak, _ = measured_peak()
+    ins = [synth.make_mf_store_inputs(9200 + k, rows, cols) for k in range(frames)]
+    store_jobs, store_keep = [], []
+    for s in ins:
+        rf, mv = torch.from_numpy(s["ref_frames"]).to(dev), torch.from_numpy(s["mvs"]).to(dev)
+        j, r, m = mfmv.store_job(rows, cols, True, s["order_hint"], s["hint_bits"], s["ref_order_hint"], rf, mv)
+        store_jobs.append(j)
+        store_keep.append((rf, mv, r, m))
+    ms_s, hms_s = _device_ms(stream, lambda: mfmv.run_store(store_jobs, stream=stream))
+    scenes = [synth.make_mf_scene(9300 + k, rows, cols) for k in range(frames)]
+    keep, pjobs = [], []
+    for sc in scenes:
+        slots = [None if sl is None else dict(sl, mf_mvs=torch.from_numpy(sl["mf_mvs"]).to(dev),
+                                              mf_ref_frames=torch.from_numpy(sl["mf_ref_frames"]).to(dev))
+                 for sl in sc["slots"]]
+        j, out = mfmv.project_job(slots, sc["ref_frame_idx"], sc["order_hints"], sc["order_hint"], sc["hint_bits"],
+                                  rows, cols, device=dev)
+        keep.append((slots, out))
+        pjobs.append(j)
+    ms_p, hms_p = _device_ms(stream, lambda: mfmv.run_project(pjobs, stream=stream))
+    t0 = time.perf_counter()
+    for s in ins[:4]:
+        oracle.mf_store(rows, cols, True, s["order_hint"], s["hint_bits"], s["ref_order_hint"], s["ref_frames"],
+                        s["mvs"])
+    cpu_s = (time.perf_counter() - t0) * 1e3 / 4
+    t0 = time.perf_counter()
+    for sc in scenes[:4]:
+        oracle.mf_project(sc["slots"], sc["ref_frame_idx"], sc["order_hints"], sc["order_hint"], sc["hint_bits"],
+                          rows, cols)
+    cpu_p = (time.perf_counter() - t0) * 1e3 / 4
+    nb_s = 15 * cells
+    nb_p = 28 * pos + 8 * pos
+    return {"frames_per_launch": frames,
+            "store": {"kernel": "mf_store_kernel", "ms_per_frame": ms_s / frames, "host_ms_per_call": hms_s,
+                      "algorithmic_bytes_per_frame": nb_s, "achieved_gbs": nb_s * frames / ms_s / 1e6,
+                      "frac_of_hbm": nb_s * frames / ms_s / 1e6 / peak,
+                      "cpu_baseline": {"kind": "port", "cores": 1, "ms_per_frame": cpu_s},
+                      "bytes_model": "per 4x4 cell: RefFrames[2] + Mvs[2][2] read, MfRefFrames + MfMvs written"},
+            "project": {"kernels": ["mf_claim_kernel", "mf_write_kernel"], "ms_per_frame": ms_p / frames,
+                        "host_ms_per_call": hms_p, "algorithmic_bytes_per_frame": nb_p,
+                        "achieved_gbs": nb_p * frames / ms_p / 1e6,
+                        "frac_of_hbm": nb_p * frames / ms_p / 1e6 / peak,
+                        "cpu_baseline": {"kind": "port", "cores": 1, "ms_per_frame": cpu_p},
+                        "bytes_model": "per 8x8 position: 7 projected MVs written + one 8-byte claim word "
+                                       "(stored candidates read per pass are L2-resident)"}}
 
 
 SERVE_SHAPES = [(640, 360, 8, 5), (1280, 720, 8, 5), (1280, 720, 10, 5), (1920, 1080, 8, 4)]
@@ -841,7 +900,7 @@ def main():
     ap.add_argument("--serve-streams", type=int, default=40)
     ap.add_argument("--serve-seconds", type=float, default=6.0)
     ap.add_argument("--serve-lanes", type=int, default=8)
-    ap.add_argument("--section", default="all", choices=["all", "recon", "extra"],
+    ap.add_argument("--section", default="all", choices=["all", "recon", "extra", "motion_field"],
                     help="recon / extra: only that section (one GPU), printed as its own JSON object; "
                          "for profiling a row's kernels")
     args = ap.parse_args()
@@ -852,7 +911,7 @@ def main():
         torch.cuda.set_device(0)
         abi.load()
         stream = torch.cuda.Stream()
-        fn = run_recon_stages if args.section == "recon" else run_extra_stages
+        fn = {"recon": run_recon_stages, "extra": run_extra_stages, "motion_field": run_motion_field}[args.section]
         print(json.dumps({args.section: fn(args, torch.device("cuda", 0), stream)}), flush=True)
         return 0
     return run_gpu(args)

@@ -499,6 +499,80 @@ av1g_status av1g_warp_estimation(const av1g_warp_sample* cands, int32_t n, int32
 av1g_status av1g_run_inter(const av1g_inter_job* jobs, int32_t n, void* stream);
 
 /* ---------------------------------------------------------------------
+ * Motion-field motion vectors: §7.19 storage and §7.9 projection
+ * ------------------------------------------------------------------- */
+
+/* MotionFieldMvs entry of a position no projection reached (MFMV_INVALID,
+ * src/cdf.rs:515). */
+#define AV1G_MFMV_INVALID (-32768)
+
+/* One decoded frame's §7.19 motion field motion vector storage: filters the
+ * block walker's per-4x4-cell RefFrames[2] / Mvs[2][2] down to the one
+ * candidate per cell that a later frame's §7.9 projection reads.  Per cell,
+ * the last list whose reference (1..7) lies in the past
+ * (get_relative_dist(ref_order_hint[r - 1], order_hint) < 0) and whose MV
+ * components are within +-(1 << 12) - 1; -1 / {0, 0} otherwise, and for every
+ * cell of a frame that is not an inter frame.  Cell values outside 1..7 are no
+ * reference.  Arrays are device memory, row-major over mi_rows x mi_cols
+ * cells; ref_frames 2-byte, mvs 8-byte and mf_mvs 4-byte aligned. */
+typedef struct av1g_mf_store_job {
+    int32_t mi_rows, mi_cols;
+    int32_t is_inter_frame;
+    int32_t order_hint;          /* OrderHint of the frame */
+    int32_t hint_bits;           /* OrderHintBits, 0 when enable_order_hint is 0 */
+    int32_t ref_order_hint[7];   /* RefOrderHint[ref_frame_idx[i]], LAST..ALTREF */
+    const int8_t* ref_frames;    /* device: [cell][list] */
+    const int16_t* mvs;          /* device: [cell][list][row, col] */
+    int8_t* mf_ref_frames;       /* device out: [cell] */
+    int16_t* mf_mvs;             /* device out: [cell][row, col] */
+} av1g_mf_store_job;
+
+/* Replaces the §7.19 loop of decode_frame_spec_tiles
+ * (src/decoder/frame_driver.rs:1119-1160) for `n` frames in one launch. */
+av1g_status av1g_run_mf_store(const av1g_mf_store_job* jobs, int32_t n, void* stream);
+
+/* One §7.20 reference slot as the projection reads it (MotionFieldSlot,
+ * src/inter_pred.rs:7567-7586): the stored frame's av1g_mf_store_job outputs
+ * (device, 4-byte aligned mf_mvs), SavedOrderHints[0..8], mi extent and
+ * FrameIsIntra.  mf_ref_frames == NULL marks an empty slot; stored
+ * reference values outside 1..7 are no candidate. */
+typedef struct av1g_mf_slot {
+    const int16_t* mf_mvs;
+    const int8_t* mf_ref_frames;
+    int32_t saved_order_hints[8];
+    int32_t mi_rows, mi_cols;
+    int32_t frame_is_intra;
+    int32_t pad;
+} av1g_mf_slot;
+
+/* The current frame's §7.9 motion_field_estimation inputs
+ * (motion_field_estimation_core, src/inter_pred.rs:7592): the eight slots,
+ * ref_frame_idx[0..7], OrderHints[0..8] (index LAST_FRAME + i holds the
+ * order hint of reference i), OrderHint, OrderHintBits (0 when order hints
+ * are off) and the frame's mi extent.  out is a device array of
+ * 7 x (mi_rows >> 1) x (mi_cols >> 1) x 2 int16, MotionFieldMvs layout
+ * [ref - LAST_FRAME][y8][x8][row, col] (src/cdf.rs:34989), 4-byte aligned;
+ * every entry is written (AV1G_MFMV_INVALID where no projection lands). */
+typedef struct av1g_mf_project_job {
+    av1g_mf_slot slots[8];
+    int32_t ref_frame_idx[7];
+    int32_t pad;
+    int32_t order_hints[8];
+    int32_t order_hint;
+    int32_t hint_bits;
+    int32_t mi_rows, mi_cols;
+    int16_t* out;
+} av1g_mf_project_job;
+
+/* §7.9.1-§7.9.4 for `n` frames: the projection passes (LAST, BWDREF,
+ * ALTREF2, ALTREF, LAST2 with the reference's selection and stamp rules,
+ * src/inter_pred.rs:7716-7741) over every stored cell at once.  Where several
+ * cells land on one position the reference's sequential order decides — the
+ * last pass, then the last cell in raster order, wins — so the result equals
+ * the reference's grid entry for entry. */
+av1g_status av1g_run_mf_project(const av1g_mf_project_job* jobs, int32_t n, void* stream);
+
+/* ---------------------------------------------------------------------
  * Serving engine: streams, device-resident reference slots, tickets
  * ------------------------------------------------------------------- */
 

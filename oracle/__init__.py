@@ -394,3 +394,71 @@ def decode_stream(frames):
                     slots[i] = sl
         outs.append(out if fr.show else None)
     return outs
+
+
+def relative_dist(a, b, bits):
+    """get_relative_dist (inter_pred.rs:3383)."""
+    return load().ora_relative_dist(int(a), int(b), int(bits))
+
+
+def mv_projection(mv, numerator, denominator):
+    """§7.9.3 get_mv_projection (cdf.rs:35101) of mv = (row, col)."""
+    lib = load()
+    src = (C.c_int * 2)(int(mv[0]), int(mv[1]))
+    out = (C.c_int * 2)()
+    lib.ora_mv_projection(src, int(numerator), int(denominator), out)
+    return [out[0], out[1]]
+
+
+def block_position(x8, y8, sign, proj_mv, mi_rows, mi_cols):
+    """§7.9.4 get_block_position (cdf.rs:35141): (pos_y8, pos_x8) or None."""
+    py, px = C.c_int(), C.c_int()
+    ok = load().ora_block_position(x8, y8, sign, int(proj_mv[0]), int(proj_mv[1]), mi_rows, mi_cols, C.byref(py),
+                                   C.byref(px))
+    return (py.value, px.value) if ok else None
+
+
+def mf_store(mi_rows, mi_cols, is_inter, order_hint, hint_bits, ref_order_hint, ref_frames, mvs):
+    """§7.19 storage of one frame (frame_driver.rs:1119-1160).
+
+    ref_frames: int8 [cells, 2]; mvs: int16 [cells, 2, 2].  Returns
+    (mf_ref_frames int8 [cells], mf_mvs int16 [cells, 2])."""
+    abi = _abi_module()
+    cells = mi_rows * mi_cols
+    rf = np.ascontiguousarray(ref_frames, dtype=np.int8).reshape(-1)
+    mv = np.ascontiguousarray(mvs, dtype=np.int16).reshape(-1)
+    assert rf.size == 2 * cells and mv.size == 4 * cells
+    out_r = np.empty(cells, np.int8)
+    out_m = np.empty((cells, 2), np.int16)
+    j = abi.MfStoreJob(mi_rows, mi_cols, int(is_inter), order_hint, hint_bits, (C.c_int32 * 7)(*ref_order_hint),
+                       rf.ctypes.data, mv.ctypes.data, out_r.ctypes.data, out_m.ctypes.data)
+    load().ora_mf_store(C.byref(j))
+    return out_r, out_m
+
+
+def mf_project(slots, ref_frame_idx, order_hints, order_hint, hint_bits, mi_rows, mi_cols):
+    """§7.9 motion_field_estimation_core (inter_pred.rs:7592) for one frame.
+
+    slots: 8 entries, None or dict(mf_mvs int16 [cells, 2], mf_ref_frames
+    int8 [cells], saved_order_hints (8), mi_rows, mi_cols, frame_is_intra).
+    Returns the MotionFieldMvs grid, int16 [7, mi_rows >> 1, mi_cols >> 1, 2]."""
+    abi = _abi_module()
+    j = abi.MfProjectJob()
+    keep = []
+    for i, sl in enumerate(slots):
+        if sl is None:
+            continue
+        m = np.ascontiguousarray(sl["mf_mvs"], dtype=np.int16)
+        r = np.ascontiguousarray(sl["mf_ref_frames"], dtype=np.int8)
+        keep += [m, r]
+        j.slots[i] = abi.MfSlot(m.ctypes.data, r.ctypes.data, (C.c_int32 * 8)(*sl["saved_order_hints"]),
+                                sl["mi_rows"], sl["mi_cols"], int(sl["frame_is_intra"]), 0)
+    for k in range(7):
+        j.ref_frame_idx[k] = ref_frame_idx[k]
+    for k in range(8):
+        j.order_hints[k] = order_hints[k]
+    j.order_hint, j.hint_bits, j.mi_rows, j.mi_cols = order_hint, hint_bits, mi_rows, mi_cols
+    out = np.empty((7, mi_rows >> 1, mi_cols >> 1, 2), np.int16)
+    j.out = out.ctypes.data
+    load().ora_mf_project(C.byref(j))
+    return out

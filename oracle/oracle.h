@@ -130,6 +130,18 @@ int ora_warp_estimation(const av1g_warp_sample* cand, int n, int mi_row, int mi_
 /* wedge_mask (inter_pred.rs:2844) into a block_width x block_height mask. */
 int ora_wedge_mask(int mi_size, int idx, int sign, uint8_t* mask);
 
+/* get_relative_dist (inter_pred.rs:3383). */
+int ora_relative_dist(int a, int b, int bits);
+/* §7.9.3 get_mv_projection (cdf.rs:35101). */
+void ora_mv_projection(const int mv[2], int numerator, int denominator, int out[2]);
+/* get_block_position (cdf.rs:35141): 1 and (*py, *px) when valid, else 0. */
+int ora_block_position(int x8, int y8, int sign, int pr, int pc, int mi_rows, int mi_cols, int* py, int* px);
+/* §7.19 storage (frame_driver.rs:1119-1160) for one job, host pointers. */
+void ora_mf_store(const av1g_mf_store_job* job);
+/* §7.9 motion_field_estimation_core (inter_pred.rs:7592) for one job, host
+ * pointers; fills all of job->out. */
+void ora_mf_project(const av1g_mf_project_job* job);
+
 #ifdef __cplusplus
 }
 #endif

@@ -200,6 +200,26 @@ class EngineStats(C.Structure):
                 ("pad", C.c_int32), ("host_ms", C.c_double), ("device_ms", C.c_double),
                 ("host_stage_ms", C.c_double * 6)]
 
+class MfStoreJob(C.Structure):
+    _fields_ = [("mi_rows", C.c_int32), ("mi_cols", C.c_int32), ("is_inter_frame", C.c_int32),
+                ("order_hint", C.c_int32), ("hint_bits", C.c_int32), ("ref_order_hint", C.c_int32 * 7),
+                ("ref_frames", C.c_void_p), ("mvs", C.c_void_p), ("mf_ref_frames", C.c_void_p),
+                ("mf_mvs", C.c_void_p)]
+
+
+class MfSlot(C.Structure):
+    _fields_ = [("mf_mvs", C.c_void_p), ("mf_ref_frames", C.c_void_p), ("saved_order_hints", C.c_int32 * 8),
+                ("mi_rows", C.c_int32), ("mi_cols", C.c_int32), ("frame_is_intra", C.c_int32), ("pad", C.c_int32)]
+
+
+class MfProjectJob(C.Structure):
+    _fields_ = [("slots", MfSlot * 8), ("ref_frame_idx", C.c_int32 * 7), ("pad", C.c_int32),
+                ("order_hints", C.c_int32 * 8), ("order_hint", C.c_int32), ("hint_bits", C.c_int32),
+                ("mi_rows", C.c_int32), ("mi_cols", C.c_int32), ("out", C.c_void_p)]
+
+
+MFMV_INVALID = -32768
+
 INTRA_HAVE_ABOVE, INTRA_HAVE_LEFT, INTRA_HAVE_ABOVE_RIGHT, INTRA_HAVE_BELOW_LEFT = 1, 2, 4, 8
 INTRA_EDGE_FILTER, INTRA_FILTER_TYPE, INTRA_RESIDUAL, INTRA_CFL = 16, 32, 64, 128
 INTRA_MODE_PALETTE, INTRA_MODE_INTRABC, INTRA_MODE_NONE = 64, 65, 255
@@ -211,7 +231,8 @@ _STRUCTS = {"av1g_film_grain": FilmGrain, "av1g_frame_header": FrameHeader, "av1
             "av1g_warp_ctx": WarpCtx, "av1g_obmc_neighbour": ObmcNeighbour, "av1g_inter_pred": InterPred,
             "av1g_inter_job": InterJob, "av1g_warp_sample": WarpSample, "av1g_config": Config,
             "av1g_seq_info": SeqInfo, "av1g_frame_desc": FrameDesc, "av1g_frame_out": FrameOut,
-            "av1g_engine_stats": EngineStats}
+            "av1g_engine_stats": EngineStats, "av1g_mf_store_job": MfStoreJob, "av1g_mf_slot": MfSlot,
+            "av1g_mf_project_job": MfProjectJob}
 
 # exported entry points and their ctypes signatures
 _SIGS = {
@@ -238,6 +259,8 @@ _SIGS = {
     "av1g_run_recon": (C.c_int, [C.POINTER(ReconJob), C.c_int32, C.c_void_p]),
     "av1g_run_intra": (C.c_int, [C.POINTER(IntraJob), C.c_int32, C.c_void_p]),
     "av1g_run_inter": (C.c_int, [C.POINTER(InterJob), C.c_int32, C.c_void_p]),
+    "av1g_run_mf_store": (C.c_int, [C.POINTER(MfStoreJob), C.c_int32, C.c_void_p]),
+    "av1g_run_mf_project": (C.c_int, [C.POINTER(MfProjectJob), C.c_int32, C.c_void_p]),
     "av1g_engine_create": (C.c_int, [C.POINTER(Config), C.POINTER(C.c_void_p)]),
     "av1g_engine_destroy": (None, [C.c_void_p]),
     "av1g_engine_get_stats": (C.c_int, [C.c_void_p, C.POINTER(EngineStats)]),

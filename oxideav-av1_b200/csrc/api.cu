@@ -25,6 +25,8 @@ size_t lr_smem_bytes();
 av1g_status recon_run(const av1g_recon_job* jobs, int n, cudaStream_t s, std::string& err);
 av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t s, std::string& err);
 av1g_status inter_run(const av1g_inter_job* jobs, int n, cudaStream_t s, std::string& err);
+av1g_status mf_store_run(const av1g_mf_store_job* jobs, int n, cudaStream_t s, std::string& err);
+av1g_status mf_project_run(const av1g_mf_project_job* jobs, int n, cudaStream_t s, std::string& err);
 }
 
 using namespace av1g;
@@ -401,6 +403,9 @@ int32_t av1g_struct_size(const char* name) {
     if (!strcmp(name, "av1g_frame_desc")) return (int32_t)sizeof(av1g_frame_desc);
     if (!strcmp(name, "av1g_frame_out")) return (int32_t)sizeof(av1g_frame_out);
     if (!strcmp(name, "av1g_engine_stats")) return (int32_t)sizeof(av1g_engine_stats);
+    if (!strcmp(name, "av1g_mf_store_job")) return (int32_t)sizeof(av1g_mf_store_job);
+    if (!strcmp(name, "av1g_mf_slot")) return (int32_t)sizeof(av1g_mf_slot);
+    if (!strcmp(name, "av1g_mf_project_job")) return (int32_t)sizeof(av1g_mf_project_job);
     return -1;
 }
 
@@ -447,6 +452,24 @@ av1g_status av1g_run_inter(const av1g_inter_job* jobs, int32_t n, void* stream) 
     if (n == 0) return AV1G_OK;
     std::string err;
     av1g_status st = inter_run(jobs, n, (cudaStream_t)stream, err);
+    if (st != AV1G_OK) g_err = err;
+    return st;
+}
+av1g_status av1g_run_mf_store(const av1g_mf_store_job* jobs, int32_t n, void* stream) {
+    g_err.clear();
+    if (n < 0 || (n > 0 && !jobs)) return fail(AV1G_EINVAL, "bad job array");
+    if (n == 0) return AV1G_OK;
+    std::string err;
+    av1g_status st = mf_store_run(jobs, n, (cudaStream_t)stream, err);
+    if (st != AV1G_OK) g_err = err;
+    return st;
+}
+av1g_status av1g_run_mf_project(const av1g_mf_project_job* jobs, int32_t n, void* stream) {
+    g_err.clear();
+    if (n < 0 || (n > 0 && !jobs)) return fail(AV1G_EINVAL, "bad job array");
+    if (n == 0) return AV1G_OK;
+    std::string err;
+    av1g_status st = mf_project_run(jobs, n, (cudaStream_t)stream, err);
     if (st != AV1G_OK) g_err = err;
     return st;
 }

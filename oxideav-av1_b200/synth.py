@@ -1008,3 +1008,60 @@ def interintra_tus(f, seed, quant=None, coeff_base=0, calls=None, rng=None):
                         0, 0, 0, [0] * 8, 0, 0, 0, 0))
     arr = np.array(tus, dtype=INTRA_TU_DTYPE) if tus else np.zeros(0, INTRA_TU_DTYPE)
     return arr, coeffs
+
+
+def _mf_mvs(rng, shape, far=0.25):
+    """MV components: mostly short (they project inside the §7.9.4 window),
+    a share long enough to leave it, a few beyond the storage limit."""
+    near = rng.integers(-160, 161, shape)
+    long_ = rng.integers(-4095, 4096, shape)
+    huge = rng.integers(-16384, 16385, shape)
+    pick = rng.random(shape)
+    return np.where(pick < 1 - far, near, np.where(pick < 1 - far / 8, long_, huge)).astype(np.int16)
+
+
+def make_mf_store_inputs(seed, mi_rows, mi_cols, hint_bits=7, is_inter=True):
+    """One frame's §7.19 storage inputs: per-cell RefFrames[2] in -1..7 and
+    Mvs[2][2], with the order hints of the frame and of its seven references
+    (some past, some future).  Returns a dict of the av1g_mf_store_job fields
+    with host arrays."""
+    rng = np.random.default_rng(seed)
+    cells = mi_rows * mi_cols
+    period = 1 << hint_bits if hint_bits else 256
+    cur = int(rng.integers(0, period))
+    ref_hints = [int((cur + d) % period) for d in rng.integers(-8, 9, 7)]
+    refs = rng.choice(np.array([-1, 0, 1, 2, 3, 4, 5, 6, 7]), size=(cells, 2)).astype(np.int8)
+    return dict(mi_rows=mi_rows, mi_cols=mi_cols, is_inter=is_inter, order_hint=cur, hint_bits=hint_bits,
+                ref_order_hint=ref_hints, ref_frames=refs, mvs=_mf_mvs(rng, (cells, 2, 2)))
+
+
+def make_mf_scene(seed, mi_rows, mi_cols, hint_bits=7, empty=(), intra=(), mismatched=(), fill=0.7):
+    """The §7.9 projection inputs of one frame: eight stored slots (MfMvs,
+    MfRefFrames, SavedOrderHints, extent, FrameIsIntra), ref_frame_idx,
+    OrderHints, OrderHint and OrderHintBits.  Slots in `empty` are absent,
+    those in `intra` are intra frames, those in `mismatched` have another mi
+    extent.  Stored frames lie up to 7 order hints before or after the
+    current frame and their own references up to 8 before them (a few after,
+    which the projection rejects)."""
+    rng = np.random.default_rng(seed)
+    period = 1 << hint_bits if hint_bits else 256
+    cur = int(rng.integers(0, period))
+    slot_hints = [int((cur + d) % period) for d in rng.choice([-7, -5, -3, -2, -1, 1, 2, 3, 4, 6], 8)]
+    slots = []
+    for s in range(8):
+        if s in empty:
+            slots.append(None)
+            continue
+        rows, cols = (mi_rows + 2, mi_cols) if s in mismatched else (mi_rows, mi_cols)
+        cells = rows * cols
+        h = slot_hints[s]
+        saved = [h] + [int((h - d) % period) for d in rng.choice([1, 2, 3, 4, 5, 8, -2], 7)]
+        refs = np.where(rng.random(cells) < fill, rng.integers(1, 8, cells), -1).astype(np.int8)
+        mvs = _mf_mvs(rng, (cells, 2), far=0.15)
+        mvs[refs < 0] = 0
+        slots.append(dict(mf_mvs=mvs, mf_ref_frames=refs, saved_order_hints=saved, mi_rows=rows, mi_cols=cols,
+                          frame_is_intra=s in intra))
+    ref_frame_idx = [int(v) for v in rng.integers(0, 8, 7)]
+    order_hints = [0] + [slot_hints[ref_frame_idx[i]] for i in range(7)]
+    return dict(slots=slots, ref_frame_idx=ref_frame_idx, order_hints=order_hints, order_hint=cur,
+                hint_bits=hint_bits, mi_rows=mi_rows, mi_cols=mi_cols)
