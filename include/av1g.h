@@ -700,6 +700,178 @@ av1g_status av1g_release_output(av1g_stream* s, uint64_t ticket);
 #define AV1G_MODE_PER_FRAME 1   /* one launch per stage per frame          */
 
 /* ---------------------------------------------------------------------
+ * Framing (host functions, no device work): IVF files, §5.3 OBUs,
+ * Annex B length-delimited streams, §5.5 sequence headers, the §7.5
+ * temporal-unit OBU walk and the leading fields of §5.9.2 frame headers.
+ * A malformed input returns AV1G_EINVAL; av1g_framing_error() then names
+ * the reference's error variant and av1g_last_error() gives the text.
+ * ------------------------------------------------------------------- */
+
+#define AV1G_FE_NONE 0
+#define AV1G_FE_UNEXPECTED_END 1          /* Error::UnexpectedEnd, IvfReadError::UnexpectedEnd */
+#define AV1G_FE_FORBIDDEN_BIT_SET 2       /* Error::ForbiddenBitSet                            */
+#define AV1G_FE_MISSING_SIZE_FIELD 3      /* Error::MissingSizeField                           */
+#define AV1G_FE_LEB128_OVERFLOW 4         /* Error::Leb128Overflow (value > 2^32 - 1)          */
+#define AV1G_FE_LEB128_TOO_LONG 5         /* Error::Leb128TooLong (8 continuation bytes)       */
+#define AV1G_FE_SIZE_OVERFLOW 6           /* Error::SizeOverflow                               */
+#define AV1G_FE_ANNEXB_INVALID 7          /* Error::AnnexBInvalid                              */
+#define AV1G_FE_IVF_BAD_MAGIC 8           /* IvfReadError::BadMagic                            */
+#define AV1G_FE_IVF_UNSUPPORTED_VERSION 9 /* IvfReadError::UnsupportedVersion                  */
+#define AV1G_FE_IVF_UNSUPPORTED_HEADER_LENGTH 10 /* IvfReadError::UnsupportedHeaderLength      */
+#define AV1G_FE_RESERVED_PROFILE 11       /* Error::ReservedProfile (seq_profile > 2)          */
+#define AV1G_FE_REDUCED_STILL_REQUIRES_STILL 12 /* Error::ReducedStillRequiresStill            */
+#define AV1G_FE_OPERATING_POINT_OUT_OF_RANGE 13 /* Error::OperatingPointOutOfRange             */
+#define AV1G_FE_OUTPUT_TOO_SMALL 14       /* the caller's output buffer (no reference variant) */
+#define AV1G_FE_UNSUPPORTED_OBU 15        /* a reserved OBU type in a temporal unit (the
+                                             reference's walk rejects it as well)             */
+#define AV1G_FE_TEMPORAL_POINT_INFO_UNSUPPORTED 16 /* Error::TemporalPointInfoUnsupported      */
+int32_t av1g_framing_error(void);
+
+/* OBU type values (§6.2.2, ObuType, src/obu.rs). */
+#define AV1G_OBU_SEQUENCE_HEADER 1
+#define AV1G_OBU_TEMPORAL_DELIMITER 2
+#define AV1G_OBU_FRAME_HEADER 3
+#define AV1G_OBU_TILE_GROUP 4
+#define AV1G_OBU_METADATA 5
+#define AV1G_OBU_FRAME 6
+#define AV1G_OBU_REDUNDANT_FRAME_HEADER 7
+#define AV1G_OBU_TILE_LIST 8
+#define AV1G_OBU_PADDING 15
+
+/* One OBU (ObuDescriptor, src/obu.rs): the raw 4-bit type, the header
+ * flags, temporal / spatial id (0 without an extension), header_len (header +
+ * extension + obu_size bytes), and where its payload lies: payload_offset
+ * bytes from the start of the buffer the call parsed. */
+typedef struct av1g_obu {
+    int32_t obu_type;
+    int32_t extension_flag;
+    int32_t has_size_field;
+    int32_t temporal_id;
+    int32_t spatial_id;
+    int32_t header_len;
+    uint64_t payload_offset;
+    uint64_t payload_len;
+} av1g_obu;
+
+/* §4.10.5 leb128 (parse_leb128, src/obu.rs): value and bytes used. */
+av1g_status av1g_leb128(const uint8_t* p, size_t n, uint64_t* value, int32_t* len);
+/* §5.3.1-§5.3.3 one OBU at p (parse_obu, src/obu.rs): the low-overhead
+ * format, so obu_has_size_field must be 1.  *consumed = header + payload. */
+av1g_status av1g_parse_obu(const uint8_t* p, size_t n, av1g_obu* out, uint64_t* consumed);
+
+/* IVF file header (IvfFileHeader, src/encoder/ivf.rs:205). */
+typedef struct av1g_ivf_header {
+    uint16_t version;
+    uint16_t header_length;
+    uint8_t fourcc[4];
+    uint16_t width;
+    uint16_t height;
+    uint32_t fps_num;
+    uint32_t fps_den;
+    uint32_t frame_count;
+} av1g_ivf_header;
+/* One IVF frame record: its timestamp and the payload's place in the file. */
+typedef struct av1g_ivf_frame {
+    uint64_t pts;
+    uint64_t offset;
+    uint64_t size;
+} av1g_ivf_frame;
+/* parse_file_header (ivf.rs:242): DKIF magic, version 0, 32-byte header. */
+av1g_status av1g_ivf_parse_header(const uint8_t* p, size_t n, av1g_ivf_header* out);
+/* IvfReader::read_next_frame (ivf.rs:309): *cursor starts at 32; on return
+ * *got = 1 with the frame and *cursor past it, or *got = 0 at the end. */
+av1g_status av1g_ivf_next_frame(const uint8_t* p, size_t n, uint64_t* cursor, av1g_ivf_frame* out, int32_t* got);
+
+/* Annex B -> §7.5 low-overhead temporal units (split_temporal_units,
+ * src/annexb.rs:66): every OBU gains an obu_size field where it had none, a
+ * temporal unit must open with its temporal delimiter and sizes must nest
+ * exactly.  The units are written back to back into out (never longer than
+ * the input, so cap >= n always suffices); tu_end[i] is the end offset of
+ * unit i in out; at most tu_cap units. */
+av1g_status av1g_annexb_split(const uint8_t* p, size_t n, uint8_t* out, size_t cap, uint64_t* tu_end,
+                              int32_t tu_cap, int32_t* n_tu, uint64_t* out_len);
+/* Low-overhead temporal units -> Annex B (build_from_temporal_units,
+ * annexb.rs:185): unit i is tus[tu_end[i-1] .. tu_end[i]).  out == NULL
+ * only measures: *out_len receives the size the stream needs. */
+av1g_status av1g_annexb_build(const uint8_t* tus, const uint64_t* tu_end, int32_t n_tu, uint8_t* out, size_t cap,
+                              uint64_t* out_len);
+
+/* §5.5 sequence header (SequenceHeader, src/sequence_header.rs), flattened:
+ * one entry per operating point (at most 32). */
+typedef struct av1g_operating_point {
+    uint16_t idc;                  /* operating_point_idc                     */
+    uint8_t seq_level_idx;
+    uint8_t seq_tier;
+    uint8_t decoder_model_present;
+    uint8_t initial_display_delay_present;
+    uint8_t initial_display_delay_minus_1;
+    uint8_t low_delay_mode_flag;
+    uint64_t decoder_buffer_delay;
+    uint64_t encoder_buffer_delay;
+} av1g_operating_point;
+
+typedef struct av1g_sequence_header {
+    uint8_t seq_profile, still_picture, reduced_still_picture_header;
+    uint8_t timing_info_present_flag, equal_picture_interval;
+    uint8_t decoder_model_info_present_flag, initial_display_delay_present_flag;
+    uint8_t operating_points_cnt_minus_1;
+    uint32_t num_units_in_display_tick, time_scale, num_ticks_per_picture_minus_1;
+    uint8_t buffer_delay_length_minus_1, buffer_removal_time_length_minus_1;
+    uint8_t frame_presentation_time_length_minus_1, pad0;
+    uint32_t num_units_in_decoding_tick;
+    av1g_operating_point operating_points[32];
+    uint8_t frame_width_bits_minus_1, frame_height_bits_minus_1;
+    uint8_t frame_id_numbers_present_flag, delta_frame_id_length_minus_2, additional_frame_id_length_minus_1;
+    uint8_t use_128x128_superblock, enable_filter_intra, enable_intra_edge_filter;
+    uint32_t max_frame_width_minus_1, max_frame_height_minus_1;
+    uint8_t enable_interintra_compound, enable_masked_compound, enable_warped_motion, enable_dual_filter;
+    uint8_t enable_order_hint, enable_jnt_comp, enable_ref_frame_mvs;
+    uint8_t seq_force_screen_content_tools, seq_force_integer_mv, order_hint_bits;
+    uint8_t enable_superres, enable_cdef, enable_restoration;
+    /* §5.5.2 color config */
+    uint8_t high_bitdepth, twelve_bit, bit_depth, mono_chrome, num_planes;
+    uint8_t color_description_present_flag, color_primaries, transfer_characteristics, matrix_coefficients;
+    uint8_t color_range, subsampling_x, subsampling_y, chroma_sample_position, separate_uv_delta_q;
+    uint8_t film_grain_params_present;
+    uint8_t pad1[3];
+    uint32_t bits_consumed;
+} av1g_sequence_header;
+
+/* parse_sequence_header (src/sequence_header.rs) of an OBU payload. */
+av1g_status av1g_parse_sequence_header(const uint8_t* payload, size_t n, av1g_sequence_header* out);
+/* The engine's stream parameters from a sequence header: the largest frame,
+ * sample format and superblock size (what av1g_stream_open needs). */
+av1g_status av1g_seq_info_from_header(const av1g_sequence_header* sh, av1g_seq_info* out);
+
+/* The OBU walk of one temporal unit (decode_temporal_unit_spec,
+ * src/decoder/frame_driver.rs:1590-1650): OBUs outside the chosen operating
+ * point are dropped (an extension header whose temporal / spatial id is not
+ * in *op_idc), a sequence header is parsed into *seq (*have_seq = 1) and
+ * selects *op_idc = operating_points[chosen_op].idc, and the OBUs the frame
+ * decode acts on — sequence header, frame header, redundant frame header,
+ * tile group, frame — are listed in order (temporal delimiters, padding,
+ * metadata and tile lists are passed over).  *op_idc, *seq and *have_seq
+ * carry from one unit of a stream to the next. */
+av1g_status av1g_temporal_unit_obus(const uint8_t* tu, size_t n, int32_t chosen_op, uint16_t* op_idc,
+                                    av1g_sequence_header* seq, int32_t* have_seq, av1g_obu* obus, int32_t cap,
+                                    int32_t* count);
+
+/* The leading fields of a §5.9.2 uncompressed header (frame header OBU or
+ * frame OBU payload) under sequence header sh: show_existing_frame and
+ * frame_to_show_map_idx, or frame_type, show_frame, showable_frame and
+ * error_resilient_mode.  Enough to know which frames a stream shows. */
+typedef struct av1g_frame_prefix {
+    int32_t show_existing_frame;
+    int32_t frame_to_show_map_idx;
+    int32_t frame_type;            /* 0 KEY, 1 INTER, 2 INTRA_ONLY, 3 SWITCH */
+    int32_t show_frame;
+    int32_t showable_frame;
+    int32_t error_resilient_mode;
+} av1g_frame_prefix;
+av1g_status av1g_frame_header_prefix(const uint8_t* payload, size_t n, const av1g_sequence_header* sh,
+                                     av1g_frame_prefix* out);
+
+/* ---------------------------------------------------------------------
  * Library
  * ------------------------------------------------------------------- */
 

@@ -220,6 +220,71 @@ class MfProjectJob(C.Structure):
 
 MFMV_INVALID = -32768
 
+
+class Obu(C.Structure):
+    _fields_ = [("obu_type", C.c_int32), ("extension_flag", C.c_int32), ("has_size_field", C.c_int32),
+                ("temporal_id", C.c_int32), ("spatial_id", C.c_int32), ("header_len", C.c_int32),
+                ("payload_offset", C.c_uint64), ("payload_len", C.c_uint64)]
+
+
+class IvfHeader(C.Structure):
+    _fields_ = [("version", C.c_uint16), ("header_length", C.c_uint16), ("fourcc", C.c_uint8 * 4),
+                ("width", C.c_uint16), ("height", C.c_uint16), ("fps_num", C.c_uint32), ("fps_den", C.c_uint32),
+                ("frame_count", C.c_uint32)]
+
+
+class IvfFrame(C.Structure):
+    _fields_ = [("pts", C.c_uint64), ("offset", C.c_uint64), ("size", C.c_uint64)]
+
+
+class OperatingPoint(C.Structure):
+    _fields_ = [("idc", C.c_uint16), ("seq_level_idx", C.c_uint8), ("seq_tier", C.c_uint8),
+                ("decoder_model_present", C.c_uint8), ("initial_display_delay_present", C.c_uint8),
+                ("initial_display_delay_minus_1", C.c_uint8), ("low_delay_mode_flag", C.c_uint8),
+                ("decoder_buffer_delay", C.c_uint64), ("encoder_buffer_delay", C.c_uint64)]
+
+
+_U8 = C.c_uint8
+
+
+class SequenceHeader(C.Structure):
+    _fields_ = [(n, _U8) for n in ("seq_profile", "still_picture", "reduced_still_picture_header",
+                                   "timing_info_present_flag", "equal_picture_interval",
+                                   "decoder_model_info_present_flag", "initial_display_delay_present_flag",
+                                   "operating_points_cnt_minus_1")] + \
+              [(n, C.c_uint32) for n in ("num_units_in_display_tick", "time_scale",
+                                         "num_ticks_per_picture_minus_1")] + \
+              [(n, _U8) for n in ("buffer_delay_length_minus_1", "buffer_removal_time_length_minus_1",
+                                  "frame_presentation_time_length_minus_1", "pad0")] + \
+              [("num_units_in_decoding_tick", C.c_uint32), ("operating_points", OperatingPoint * 32)] + \
+              [(n, _U8) for n in ("frame_width_bits_minus_1", "frame_height_bits_minus_1",
+                                  "frame_id_numbers_present_flag", "delta_frame_id_length_minus_2",
+                                  "additional_frame_id_length_minus_1", "use_128x128_superblock",
+                                  "enable_filter_intra", "enable_intra_edge_filter")] + \
+              [("max_frame_width_minus_1", C.c_uint32), ("max_frame_height_minus_1", C.c_uint32)] + \
+              [(n, _U8) for n in ("enable_interintra_compound", "enable_masked_compound", "enable_warped_motion",
+                                  "enable_dual_filter", "enable_order_hint", "enable_jnt_comp",
+                                  "enable_ref_frame_mvs", "seq_force_screen_content_tools",
+                                  "seq_force_integer_mv", "order_hint_bits", "enable_superres", "enable_cdef",
+                                  "enable_restoration", "high_bitdepth", "twelve_bit", "bit_depth", "mono_chrome",
+                                  "num_planes", "color_description_present_flag", "color_primaries",
+                                  "transfer_characteristics", "matrix_coefficients", "color_range",
+                                  "subsampling_x", "subsampling_y", "chroma_sample_position",
+                                  "separate_uv_delta_q", "film_grain_params_present")] + \
+              [("pad1", _U8 * 3), ("bits_consumed", C.c_uint32)]
+
+
+class FramePrefix(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("show_existing_frame", "frame_to_show_map_idx", "frame_type", "show_frame",
+                                         "showable_frame", "error_resilient_mode")]
+
+
+FE_NONE, FE_UNEXPECTED_END, FE_FORBIDDEN_BIT_SET, FE_MISSING_SIZE_FIELD = 0, 1, 2, 3
+FE_LEB128_OVERFLOW, FE_LEB128_TOO_LONG, FE_SIZE_OVERFLOW, FE_ANNEXB_INVALID = 4, 5, 6, 7
+FE_IVF_BAD_MAGIC, FE_IVF_UNSUPPORTED_VERSION, FE_IVF_UNSUPPORTED_HEADER_LENGTH = 8, 9, 10
+FE_RESERVED_PROFILE, FE_REDUCED_STILL_REQUIRES_STILL, FE_OPERATING_POINT_OUT_OF_RANGE = 11, 12, 13
+FE_OUTPUT_TOO_SMALL, FE_UNSUPPORTED_OBU, FE_TEMPORAL_POINT_INFO_UNSUPPORTED = 14, 15, 16
+
 INTRA_HAVE_ABOVE, INTRA_HAVE_LEFT, INTRA_HAVE_ABOVE_RIGHT, INTRA_HAVE_BELOW_LEFT = 1, 2, 4, 8
 INTRA_EDGE_FILTER, INTRA_FILTER_TYPE, INTRA_RESIDUAL, INTRA_CFL = 16, 32, 64, 128
 INTRA_MODE_PALETTE, INTRA_MODE_INTRABC, INTRA_MODE_NONE = 64, 65, 255
@@ -232,7 +297,9 @@ _STRUCTS = {"av1g_film_grain": FilmGrain, "av1g_frame_header": FrameHeader, "av1
             "av1g_inter_job": InterJob, "av1g_warp_sample": WarpSample, "av1g_config": Config,
             "av1g_seq_info": SeqInfo, "av1g_frame_desc": FrameDesc, "av1g_frame_out": FrameOut,
             "av1g_engine_stats": EngineStats, "av1g_mf_store_job": MfStoreJob, "av1g_mf_slot": MfSlot,
-            "av1g_mf_project_job": MfProjectJob}
+            "av1g_mf_project_job": MfProjectJob, "av1g_obu": Obu, "av1g_ivf_header": IvfHeader,
+            "av1g_ivf_frame": IvfFrame, "av1g_operating_point": OperatingPoint,
+            "av1g_sequence_header": SequenceHeader, "av1g_frame_prefix": FramePrefix}
 
 # exported entry points and their ctypes signatures
 _SIGS = {
@@ -261,6 +328,23 @@ _SIGS = {
     "av1g_run_inter": (C.c_int, [C.POINTER(InterJob), C.c_int32, C.c_void_p]),
     "av1g_run_mf_store": (C.c_int, [C.POINTER(MfStoreJob), C.c_int32, C.c_void_p]),
     "av1g_run_mf_project": (C.c_int, [C.POINTER(MfProjectJob), C.c_int32, C.c_void_p]),
+    "av1g_framing_error": (C.c_int32, []),
+    "av1g_leb128": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(C.c_uint64), C.POINTER(C.c_int32)]),
+    "av1g_parse_obu": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(Obu), C.POINTER(C.c_uint64)]),
+    "av1g_ivf_parse_header": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(IvfHeader)]),
+    "av1g_ivf_next_frame": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(C.c_uint64), C.POINTER(IvfFrame),
+                                      C.POINTER(C.c_int32)]),
+    "av1g_annexb_split": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint64), C.c_int32,
+                                    C.POINTER(C.c_int32), C.POINTER(C.c_uint64)]),
+    "av1g_annexb_build": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.c_int32, C.c_void_p, C.c_size_t,
+                                    C.POINTER(C.c_uint64)]),
+    "av1g_parse_sequence_header": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(SequenceHeader)]),
+    "av1g_seq_info_from_header": (C.c_int, [C.POINTER(SequenceHeader), C.POINTER(SeqInfo)]),
+    "av1g_temporal_unit_obus": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int32, C.POINTER(C.c_uint16),
+                                          C.POINTER(SequenceHeader), C.POINTER(C.c_int32), C.POINTER(Obu), C.c_int32,
+                                          C.POINTER(C.c_int32)]),
+    "av1g_frame_header_prefix": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(SequenceHeader),
+                                           C.POINTER(FramePrefix)]),
     "av1g_engine_create": (C.c_int, [C.POINTER(Config), C.POINTER(C.c_void_p)]),
     "av1g_engine_destroy": (None, [C.c_void_p]),
     "av1g_engine_get_stats": (C.c_int, [C.c_void_p, C.POINTER(EngineStats)]),

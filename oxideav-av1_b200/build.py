@@ -1,6 +1,7 @@
 """Build the engine's CUDA library in-tree for sm_100a.
 
-``build_library()`` compiles every ``csrc/*.cu`` with nvcc into
+``build_library()`` compiles every ``csrc/*.cu`` (and the host-only
+``csrc/*.cpp``) with nvcc into
 ``liboxav1_b200.so`` next to this file (objects in ``_build/``), rebuilding only
 what changed.  The library is the product: the Python host layer loads it with
 ctypes and has no fallback when it is missing.
@@ -34,7 +35,7 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
     headers = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list((REPO / "include").glob("*.h"))
     hdr_mtime = max(p.stat().st_mtime for p in headers)
     objs = []
-    for cu in sorted(CSRC.glob("*.cu")):
+    for cu in sorted(list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cpp"))):
         obj = BUILD / (cu.stem + ".o")
         objs.append(obj)
         if force or not obj.exists() or obj.stat().st_mtime < max(cu.stat().st_mtime, hdr_mtime):

@@ -375,6 +375,11 @@ av1g_status postfilter_result_planes(const av1g_frame_job& j, PlaneDev pre[3], P
 
 }  // namespace av1g
 
+namespace av1g {
+// The framing functions (framing.cpp) report through the same error text.
+void set_last_error_text(const std::string& s) { g_err = s; }
+}  // namespace av1g
+
 extern "C" {
 
 int32_t av1g_abi_version(void) { return AV1G_ABI_VERSION; }
@@ -406,6 +411,12 @@ int32_t av1g_struct_size(const char* name) {
     if (!strcmp(name, "av1g_mf_store_job")) return (int32_t)sizeof(av1g_mf_store_job);
     if (!strcmp(name, "av1g_mf_slot")) return (int32_t)sizeof(av1g_mf_slot);
     if (!strcmp(name, "av1g_mf_project_job")) return (int32_t)sizeof(av1g_mf_project_job);
+    if (!strcmp(name, "av1g_obu")) return (int32_t)sizeof(av1g_obu);
+    if (!strcmp(name, "av1g_ivf_header")) return (int32_t)sizeof(av1g_ivf_header);
+    if (!strcmp(name, "av1g_ivf_frame")) return (int32_t)sizeof(av1g_ivf_frame);
+    if (!strcmp(name, "av1g_operating_point")) return (int32_t)sizeof(av1g_operating_point);
+    if (!strcmp(name, "av1g_sequence_header")) return (int32_t)sizeof(av1g_sequence_header);
+    if (!strcmp(name, "av1g_frame_prefix")) return (int32_t)sizeof(av1g_frame_prefix);
     return -1;
 }
 

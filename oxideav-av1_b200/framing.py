@@ -1,0 +1,224 @@
+"""Stream framing through the C ABI: IVF, OBUs, Annex B, sequence headers.
+
+Names and behaviour mirror the reference's framing layer — ``parse_leb128`` /
+``parse_obu`` / ``ObuIter`` (src/obu.rs), ``IvfReader`` (src/encoder/ivf.rs),
+``split_temporal_units`` / ``build_from_temporal_units`` (src/annexb.rs),
+``parse_sequence_header`` (src/sequence_header.rs) — and the OBU walk of a
+temporal unit (decode_temporal_unit_spec, src/decoder/frame_driver.rs:1590).
+Errors raise ``FramingError`` whose ``variant`` is the reference's error
+variant name.  The work happens in the library's host code (framing.cpp).
+"""
+import ctypes as C
+from dataclasses import dataclass
+
+from . import abi
+
+VARIANTS = {abi.FE_UNEXPECTED_END: "UnexpectedEnd", abi.FE_FORBIDDEN_BIT_SET: "ForbiddenBitSet",
+            abi.FE_MISSING_SIZE_FIELD: "MissingSizeField", abi.FE_LEB128_OVERFLOW: "Leb128Overflow",
+            abi.FE_LEB128_TOO_LONG: "Leb128TooLong", abi.FE_SIZE_OVERFLOW: "SizeOverflow",
+            abi.FE_ANNEXB_INVALID: "AnnexBInvalid", abi.FE_IVF_BAD_MAGIC: "BadMagic",
+            abi.FE_IVF_UNSUPPORTED_VERSION: "UnsupportedVersion",
+            abi.FE_IVF_UNSUPPORTED_HEADER_LENGTH: "UnsupportedHeaderLength",
+            abi.FE_RESERVED_PROFILE: "ReservedProfile",
+            abi.FE_REDUCED_STILL_REQUIRES_STILL: "ReducedStillRequiresStill",
+            abi.FE_OPERATING_POINT_OUT_OF_RANGE: "OperatingPointOutOfRange",
+            abi.FE_OUTPUT_TOO_SMALL: "OutputTooSmall", abi.FE_UNSUPPORTED_OBU: "UnsupportedObu",
+            abi.FE_TEMPORAL_POINT_INFO_UNSUPPORTED: "TemporalPointInfoUnsupported"}
+
+OBU_NAMES = {1: "SequenceHeader", 2: "TemporalDelimiter", 3: "FrameHeader", 4: "TileGroup", 5: "Metadata",
+             6: "Frame", 7: "RedundantFrameHeader", 8: "TileList", 15: "Padding"}
+
+
+class FramingError(ValueError):
+    def __init__(self, code, text):
+        self.code = code
+        self.variant = VARIANTS.get(code, str(code))
+        super().__init__(f"{self.variant}: {text}")
+
+
+def _check(lib, status):
+    if status != abi.AV1G_OK:
+        raise FramingError(lib.av1g_framing_error(), lib.av1g_last_error().decode(errors="replace"))
+
+
+def _buf(data):
+    data = bytes(data)
+    return data, C.cast(C.c_char_p(data), C.c_void_p) if data else None
+
+
+def parse_leb128(data):
+    """(value, bytes used)."""
+    lib = abi.load()
+    data, p = _buf(data)
+    v, n = C.c_uint64(), C.c_int32()
+    _check(lib, lib.av1g_leb128(p, len(data), C.byref(v), C.byref(n)))
+    return v.value, n.value
+
+
+@dataclass
+class ObuDescriptor:
+    obu_type: int
+    extension_flag: bool
+    has_size_field: bool
+    temporal_id: int
+    spatial_id: int
+    payload_len: int
+    header_len: int
+    payload: bytes
+
+    @property
+    def type_name(self):
+        return OBU_NAMES.get(self.obu_type, f"Reserved({self.obu_type})")
+
+
+def _desc(o, data, base=0):
+    off = o.payload_offset - base
+    return ObuDescriptor(o.obu_type, bool(o.extension_flag), bool(o.has_size_field), o.temporal_id, o.spatial_id,
+                         o.payload_len, o.header_len, bytes(data[off: off + o.payload_len]))
+
+
+def parse_obu(data):
+    """(ObuDescriptor, bytes consumed) of the OBU at the start of data."""
+    lib = abi.load()
+    data, p = _buf(data)
+    o, used = abi.Obu(), C.c_uint64()
+    _check(lib, lib.av1g_parse_obu(p, len(data), C.byref(o), C.byref(used)))
+    return _desc(o, data), used.value
+
+
+def obu_iter(data):
+    """Yields the OBUs of a low-overhead byte stream; a malformed OBU raises."""
+    pos = 0
+    data = bytes(data)
+    while pos < len(data):
+        d, used = parse_obu(data[pos:])
+        pos += used
+        yield d
+
+
+@dataclass
+class IvfFrame:
+    pts: int
+    payload: bytes
+
+
+class IvfReader:
+    """IvfReader (src/encoder/ivf.rs:284): header, read_next_frame, read_all."""
+
+    def __init__(self, data):
+        self._lib = abi.load()
+        self._data, self._p = _buf(data)
+        self.header = abi.IvfHeader()
+        _check(self._lib, self._lib.av1g_ivf_parse_header(self._p, len(self._data), C.byref(self.header)))
+        self._cursor = C.c_uint64(32)
+
+    def read_next_frame(self):
+        f, got = abi.IvfFrame(), C.c_int32()
+        _check(self._lib, self._lib.av1g_ivf_next_frame(self._p, len(self._data), C.byref(self._cursor), C.byref(f),
+                                                        C.byref(got)))
+        if not got.value:
+            return None
+        return IvfFrame(f.pts, self._data[f.offset: f.offset + f.size])
+
+    def read_all(self):
+        out = []
+        while (f := self.read_next_frame()) is not None:
+            out.append(f)
+        return out
+
+
+def split_temporal_units(data):
+    """Annex B stream -> list of low-overhead temporal units (bytes)."""
+    lib = abi.load()
+    data, p = _buf(data)
+    cap_units = max(1, len(data))
+    out = (C.c_uint8 * max(1, len(data)))()
+    ends = (C.c_uint64 * cap_units)()
+    n_tu, out_len = C.c_int32(), C.c_uint64()
+    _check(lib, lib.av1g_annexb_split(p, len(data), out, len(data), ends, cap_units, C.byref(n_tu),
+                                      C.byref(out_len)))
+    raw = bytes(out)[: out_len.value]
+    units, start = [], 0
+    for i in range(n_tu.value):
+        units.append(raw[start: ends[i]])
+        start = ends[i]
+    return units
+
+
+def build_from_temporal_units(units):
+    """Low-overhead temporal units -> one Annex B stream."""
+    lib = abi.load()
+    joined = b"".join(bytes(u) for u in units)
+    ends, acc = (C.c_uint64 * max(1, len(units)))(), 0
+    for i, u in enumerate(units):
+        acc += len(u)
+        ends[i] = acc
+    joined, p = _buf(joined)
+    need = C.c_uint64()
+    _check(lib, lib.av1g_annexb_build(p, ends, len(units), None, 0, C.byref(need)))
+    out = (C.c_uint8 * max(1, need.value))()
+    _check(lib, lib.av1g_annexb_build(p, ends, len(units), out, need.value, C.byref(need)))
+    return bytes(out)[: need.value]
+
+
+def parse_sequence_header(payload):
+    """The §5.5 sequence header of an OBU payload (av1g_sequence_header)."""
+    lib = abi.load()
+    data, p = _buf(payload)
+    sh = abi.SequenceHeader()
+    _check(lib, lib.av1g_parse_sequence_header(p, len(data), C.byref(sh)))
+    return sh
+
+
+def seq_info(sh):
+    """The engine's stream parameters (av1g_seq_info) of a sequence header."""
+    lib = abi.load()
+    out = abi.SeqInfo()
+    _check(lib, lib.av1g_seq_info_from_header(C.byref(sh), C.byref(out)))
+    return out
+
+
+def frame_header_prefix(payload, sh):
+    lib = abi.load()
+    data, p = _buf(payload)
+    out = abi.FramePrefix()
+    _check(lib, lib.av1g_frame_header_prefix(p, len(data), C.byref(sh), C.byref(out)))
+    return out
+
+
+class TemporalUnitWalker:
+    """The per-stream state of the §7.5 OBU walk: the chosen operating point,
+    its idc and the latest sequence header, carried from unit to unit."""
+
+    def __init__(self, chosen_op=0):
+        self._lib = abi.load()
+        self.chosen_op = chosen_op
+        self.op_idc = C.c_uint16(0)
+        self.seq = abi.SequenceHeader()
+        self.have_seq = C.c_int32(0)
+
+    def walk(self, tu):
+        """The OBUs of one temporal unit that the frame decode acts on."""
+        data, p = _buf(tu)
+        cap = max(1, len(data) // 2 + 1)
+        obus, count = (abi.Obu * cap)(), C.c_int32()
+        _check(self._lib, self._lib.av1g_temporal_unit_obus(p, len(data), self.chosen_op, C.byref(self.op_idc),
+                                                            C.byref(self.seq), C.byref(self.have_seq), obus, cap,
+                                                            C.byref(count)))
+        return [_desc(obus[i], data) for i in range(count.value)]
+
+    def shown_frames(self, tu):
+        """Frames this temporal unit outputs: every frame header that shows an
+        existing frame and every frame whose show_frame is set."""
+        n = 0
+        for d in self.walk(tu):
+            if d.obu_type in (3, 6):
+                pre = frame_header_prefix(d.payload, self.seq)
+                n += 1 if (pre.show_existing_frame or pre.show_frame) else 0
+        return n
+
+
+def ivf_shown_frames(data, chosen_op=0):
+    """Frames a whole IVF stream outputs under operating point chosen_op."""
+    w = TemporalUnitWalker(chosen_op)
+    return sum(w.shown_frames(f.payload) for f in IvfReader(data).read_all())
