@@ -116,11 +116,16 @@ __device__ void box_coeffs(Smem& s, int th, int tw, int bd, int r, int eps, bool
         }
     }
     __syncthreads();
-    // row sums and coefficients: one thread per (grid row, run of 8 columns)
+    // row sums and coefficients: one thread per (grid row, run of 8 columns);
+    // with odd_only the work list holds only the odd-plane-row grid rows, so
+    // no lane of a warp idles on a skipped row
     constexpr int SEGS = (TW + 2 + RUN - 1) / RUN;
-    for (int k = threadIdx.x; k < rows * SEGS; k += blockDim.x) {
-        const int row = k / SEGS, sg = k - row * SEGS;
-        if (odd_only && !((y0 + row - 1) & 1)) continue;
+    const int first = odd_only ? ((y0 & 1) ? 1 : 0) : 0;  // grid row r holds plane row y0 + r - 1
+    const int step = odd_only ? 2 : 1;
+    const int nrows = (rows - first + step - 1) / step;
+    for (int k = threadIdx.x; k < nrows * SEGS; k += blockDim.x) {
+        const int rk = k / SEGS, sg = k - rk * SEGS;
+        const int row = first + rk * step;
         const int ja = sg * RUN - 1, jb = min(tw + 1, ja + RUN);  // j in [ja, jb)
         if (ja >= jb) continue;
         const int* c1 = s.v1 + row * VW;
@@ -365,8 +370,13 @@ __global__ void __launch_bounds__(256) lr_kernel(const FrameDev* __restrict__ fr
         constexpr int Q = TW / 4;
         if (r0) {
             box_coeffs(s, th, tw, bd, r0, e0, true, y0);
+            // rows of one parity run together (the odd-row and even-row
+            // weightings differ), so a warp's two rows share a code path
+            const int n_odd = (th + ((y0 & 1) ? 1 : 0)) >> 1;      // rows i with (y0 + i) odd
+            const int odd0 = (y0 & 1) ? 0 : 1;
             for (int k = threadIdx.x; k < th * Q; k += blockDim.x) {
-                int i = k / Q, j0 = (k - i * Q) * 4;
+                const int rk = k / Q, j0 = (k - rk * Q) * 4;
+                const int i = rk < n_odd ? odd0 + 2 * rk : (1 - odd0) + 2 * (rk - n_odd);
                 if (j0 >= tw) continue;
                 int u[4], f[4];
 #pragma unroll
@@ -385,13 +395,24 @@ __global__ void __launch_bounds__(256) lr_kernel(const FrameDev* __restrict__ fr
 #pragma unroll
             for (int e = 0; e < 4; e++) u[e] = s.src[(i + H3) * SP + j0 + e + H3];
             if (r1) box_weight4(s, i, j0, u, 1, y0, f1);
+            int o[4];
 #pragma unroll
             for (int e = 0; e < 4; e++) {
-                if (j0 + e >= tw) break;
                 int uu = u[e] << 4;
                 int f0 = r0 ? s.F0[i * TW + j0 + e] : uu;
                 int v = w1 * uu + w0 * f0 + w2 * (r1 ? f1[e] : uu);
-                st_px(O, hbd, y0 + i, x0 + j0 + e, clip3(0, maxv, (v + (1 << 10)) >> 11));
+                o[e] = clip3(0, maxv, (v + (1 << 10)) >> 11);
+            }
+            if (j0 + 4 <= tw && !((x0 + j0) & 3)) {  // one aligned vector store
+                uint8_t* row = O.p + (size_t)(y0 + i) * O.stride;
+                if (hbd)
+                    *reinterpret_cast<uint2*>(row + 2 * (x0 + j0)) =
+                        make_uint2((uint32_t)o[0] | (uint32_t)o[1] << 16, (uint32_t)o[2] | (uint32_t)o[3] << 16);
+                else
+                    *reinterpret_cast<uint32_t*>(row + x0 + j0) =
+                        (uint32_t)o[0] | (uint32_t)o[1] << 8 | (uint32_t)o[2] << 16 | (uint32_t)o[3] << 24;
+            } else {
+                for (int e = 0; e < 4 && j0 + e < tw; e++) st_px(O, hbd, y0 + i, x0 + j0 + e, o[e]);
             }
         }
     }
