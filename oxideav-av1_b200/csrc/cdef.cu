@@ -137,7 +137,7 @@ __device__ __forceinline__ int filter_px(const int16_t* c, int xv, const Taps& T
 
 __global__ void __launch_bounds__(256, 3) cdef_kernel(const FrameDev* __restrict__ frames,
                                                       const int32_t* __restrict__ starts, int n, int total) {
-    __shared__ int16_t win[3][WMAX * WP];
+    __shared__ __align__(16) int16_t win[3][WMAX * WP];
     __shared__ BlockParams bp[64];
     __shared__ int costs[64][8];
     // luma of the 64 8x8 blocks, block-major with a 136-byte block stride so
@@ -312,8 +312,13 @@ __global__ void __launch_bounds__(256, 3) cdef_kernel(const FrameDev* __restrict
                         out1 = filter_px<false>(cp + 1, xv1, T, pri, sec, padj, sadj, pt0, pt1);
                     }
                 }
-                st_px(D, hbd, gy, gx, out0);
-                if (gx + 1 < dw) st_px(D, hbd, gy, gx + 1, out1);
+                if (gx + 1 < dw) {  // gx is even: one aligned 2- or 4-byte store
+                    uint8_t* row = D.p + (size_t)gy * D.stride;
+                    if (hbd) *reinterpret_cast<uint32_t*>(row + 2 * gx) = (uint32_t)out0 | (uint32_t)out1 << 16;
+                    else *reinterpret_cast<uint16_t*>(row + gx) = (uint16_t)(out0 | out1 << 8);
+                } else {
+                    st_px(D, hbd, gy, gx, out0);
+                }
             }
         }
     }
