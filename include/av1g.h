@@ -573,6 +573,42 @@ typedef struct av1g_mf_project_job {
 av1g_status av1g_run_mf_project(const av1g_mf_project_job* jobs, int32_t n, void* stream);
 
 /* ---------------------------------------------------------------------
+ * Large-scale tile (§7.3): output assembly of decoded camera tiles
+ * ------------------------------------------------------------------- */
+
+/* Where one decoded camera tile lies: the CurrFrame planes its §7.3.2
+ * decode wrote (device, the camera frame's extent) and the tile's luma
+ * origin in them (MiColStart * 4, MiRowStart * 4). */
+typedef struct av1g_tile_list_entry {
+    av1g_plane src[3];
+    int32_t x0, y0;
+} av1g_tile_list_entry;
+
+/* One tile list's output frame (decode_tile_list, src/tile_list.rs:651-740):
+ * tile_width x tile_height luma samples per tile (TileWidth, TileHeight),
+ * an output of width_in_tiles x height_in_tiles tiles
+ * (output_frame_*_in_tiles_minus_1 + 1), num_entries decoded tiles (host
+ * array) placed in raster order; output tile positions no entry covers are
+ * zero, as the reference's output buffer starts.  out: device planes of
+ * width_in_tiles * tile_width x height_in_tiles * tile_height luma samples
+ * (chroma >> subsampling), u8 for 8-bit content, u16 otherwise. */
+typedef struct av1g_tile_list_job {
+    int32_t tile_width, tile_height;
+    int32_t width_in_tiles, height_in_tiles;
+    int32_t num_planes, subsampling_x, subsampling_y, bit_depth;
+    int32_t num_entries;
+    int32_t pad;
+    const av1g_tile_list_entry* entries;
+    av1g_plane out[3];
+} av1g_tile_list_job;
+
+/* The §7.3.1 output placement for `n` tile lists in one launch; the camera
+ * tiles themselves are decoded by the batched reconstruction entry points
+ * (each tile an independent job with its anchor frame as reference), not one
+ * after the other as the reference does. */
+av1g_status av1g_run_tile_list_output(const av1g_tile_list_job* jobs, int32_t n, void* stream);
+
+/* ---------------------------------------------------------------------
  * Serving engine: streams, device-resident reference slots, tickets
  * ------------------------------------------------------------------- */
 
@@ -870,6 +906,35 @@ typedef struct av1g_frame_prefix {
 } av1g_frame_prefix;
 av1g_status av1g_frame_header_prefix(const uint8_t* payload, size_t n, const av1g_sequence_header* sh,
                                      av1g_frame_prefix* out);
+
+/* §5.12 tile list OBU (TileListObu / TileListEntry, src/tile_list.rs): the
+ * output size in tiles and, per entry, the anchor and tile it names and
+ * where its coded tile data lies in the payload. */
+typedef struct av1g_tile_list_header {
+    int32_t output_frame_width_in_tiles_minus_1;
+    int32_t output_frame_height_in_tiles_minus_1;
+    int32_t tile_count_minus_1;
+    int32_t pad;
+} av1g_tile_list_header;
+typedef struct av1g_tile_list_obu_entry {
+    int32_t anchor_frame_idx;
+    int32_t anchor_tile_row;
+    int32_t anchor_tile_col;
+    int32_t pad;
+    uint64_t data_offset;
+    uint64_t data_size;
+} av1g_tile_list_obu_entry;
+#define AV1G_FE_TILE_LIST_INVALID 17      /* Error::TileListInvalid                            */
+/* parse_tile_list_obu (tile_list.rs:102): at most cap entries are written;
+ * the conformance bounds tile_count_minus_1 <= 511 and anchor_frame_idx <=
+ * 127 are enforced and the payload must end with the last entry. */
+av1g_status av1g_parse_tile_list(const uint8_t* payload, size_t n, av1g_tile_list_header* hdr,
+                                 av1g_tile_list_obu_entry* entries, int32_t cap);
+/* write_tile_list_obu (tile_list.rs:156): 1..512 entries, anchor_frame_idx <=
+ * 127, 1..65536 bytes of tile data each (entries[i].data_offset indexes
+ * `data`).  out == NULL only measures. */
+av1g_status av1g_write_tile_list(const av1g_tile_list_header* hdr, const av1g_tile_list_obu_entry* entries,
+                                 int32_t count, const uint8_t* data, uint8_t* out, size_t cap, uint64_t* out_len);
 
 /* ---------------------------------------------------------------------
  * Library

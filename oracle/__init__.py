@@ -462,3 +462,23 @@ def mf_project(slots, ref_frame_idx, order_hints, order_hint, hint_bits, mi_rows
     j.out = out.ctypes.data
     load().ora_mf_project(C.byref(j))
     return out
+
+
+def tile_list_output(tile_w, tile_h, width_in_tiles, height_in_tiles, ssx, ssy, bit_depth, tiles):
+    """The §7.3.1 placement of decode_tile_list (src/tile_list.rs:665-740):
+    tiles = list of (camera frame planes, x0, y0) in list order; tile k goes
+    to (tile_w * (k % width_in_tiles), tile_h * (k // width_in_tiles)), chroma
+    shifted by the subsampling; the rest of the output stays 0; samples are
+    clamped to the bit depth."""
+    np_ = len(tiles[0][0])
+    ow, oh = width_in_tiles * tile_w, height_in_tiles * tile_h
+    dims = [(oh, ow) if p == 0 else (oh >> ssy, ow >> ssx) for p in range(np_)]
+    out = [np.zeros(d, np.int32) for d in dims]
+    for k, (planes, x0, y0) in enumerate(tiles):
+        dx, dy = tile_w * (k % width_in_tiles), tile_h * (k // width_in_tiles)
+        for p in range(np_):
+            sx, sy = (ssx, ssy) if p else (0, 0)
+            tw, th = (tile_w + sx) >> sx, (tile_h + sy) >> sy
+            src = np.asarray(planes[p], np.int32)[y0 >> sy: (y0 >> sy) + th, x0 >> sx: (x0 >> sx) + tw]
+            out[p][dy >> sy: (dy >> sy) + th, dx >> sx: (dx >> sx) + tw] = src
+    return [np.clip(o, 0, (1 << bit_depth) - 1) for o in out]

@@ -279,6 +279,27 @@ class FramePrefix(C.Structure):
                                          "showable_frame", "error_resilient_mode")]
 
 
+class TileListEntry(C.Structure):
+    _fields_ = [("src", Plane * 3), ("x0", C.c_int32), ("y0", C.c_int32)]
+
+
+class TileListJob(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("tile_width", "tile_height", "width_in_tiles", "height_in_tiles",
+                                         "num_planes", "subsampling_x", "subsampling_y", "bit_depth", "num_entries",
+                                         "pad")] + [("entries", C.POINTER(TileListEntry)), ("out", Plane * 3)]
+
+
+class TileListHeader(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("output_frame_width_in_tiles_minus_1",
+                                         "output_frame_height_in_tiles_minus_1", "tile_count_minus_1", "pad")]
+
+
+class TileListObuEntry(C.Structure):
+    _fields_ = [("anchor_frame_idx", C.c_int32), ("anchor_tile_row", C.c_int32), ("anchor_tile_col", C.c_int32),
+                ("pad", C.c_int32), ("data_offset", C.c_uint64), ("data_size", C.c_uint64)]
+
+
+FE_TILE_LIST_INVALID = 17
 FE_NONE, FE_UNEXPECTED_END, FE_FORBIDDEN_BIT_SET, FE_MISSING_SIZE_FIELD = 0, 1, 2, 3
 FE_LEB128_OVERFLOW, FE_LEB128_TOO_LONG, FE_SIZE_OVERFLOW, FE_ANNEXB_INVALID = 4, 5, 6, 7
 FE_IVF_BAD_MAGIC, FE_IVF_UNSUPPORTED_VERSION, FE_IVF_UNSUPPORTED_HEADER_LENGTH = 8, 9, 10
@@ -299,7 +320,9 @@ _STRUCTS = {"av1g_film_grain": FilmGrain, "av1g_frame_header": FrameHeader, "av1
             "av1g_engine_stats": EngineStats, "av1g_mf_store_job": MfStoreJob, "av1g_mf_slot": MfSlot,
             "av1g_mf_project_job": MfProjectJob, "av1g_obu": Obu, "av1g_ivf_header": IvfHeader,
             "av1g_ivf_frame": IvfFrame, "av1g_operating_point": OperatingPoint,
-            "av1g_sequence_header": SequenceHeader, "av1g_frame_prefix": FramePrefix}
+            "av1g_sequence_header": SequenceHeader, "av1g_frame_prefix": FramePrefix,
+            "av1g_tile_list_entry": TileListEntry, "av1g_tile_list_job": TileListJob,
+            "av1g_tile_list_header": TileListHeader, "av1g_tile_list_obu_entry": TileListObuEntry}
 
 # exported entry points and their ctypes signatures
 _SIGS = {
@@ -345,6 +368,11 @@ _SIGS = {
                                           C.POINTER(C.c_int32)]),
     "av1g_frame_header_prefix": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(SequenceHeader),
                                            C.POINTER(FramePrefix)]),
+    "av1g_run_tile_list_output": (C.c_int, [C.POINTER(TileListJob), C.c_int32, C.c_void_p]),
+    "av1g_parse_tile_list": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(TileListHeader),
+                                       C.POINTER(TileListObuEntry), C.c_int32]),
+    "av1g_write_tile_list": (C.c_int, [C.POINTER(TileListHeader), C.POINTER(TileListObuEntry), C.c_int32,
+                                       C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint64)]),
     "av1g_engine_create": (C.c_int, [C.POINTER(Config), C.POINTER(C.c_void_p)]),
     "av1g_engine_destroy": (None, [C.c_void_p]),
     "av1g_engine_get_stats": (C.c_int, [C.c_void_p, C.POINTER(EngineStats)]),

@@ -27,6 +27,7 @@ av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t s, std::st
 av1g_status inter_run(const av1g_inter_job* jobs, int n, cudaStream_t s, std::string& err);
 av1g_status mf_store_run(const av1g_mf_store_job* jobs, int n, cudaStream_t s, std::string& err);
 av1g_status mf_project_run(const av1g_mf_project_job* jobs, int n, cudaStream_t s, std::string& err);
+av1g_status tile_list_run(const av1g_tile_list_job* jobs, int n, cudaStream_t s, std::string& err);
 }
 
 using namespace av1g;
@@ -417,6 +418,10 @@ int32_t av1g_struct_size(const char* name) {
     if (!strcmp(name, "av1g_operating_point")) return (int32_t)sizeof(av1g_operating_point);
     if (!strcmp(name, "av1g_sequence_header")) return (int32_t)sizeof(av1g_sequence_header);
     if (!strcmp(name, "av1g_frame_prefix")) return (int32_t)sizeof(av1g_frame_prefix);
+    if (!strcmp(name, "av1g_tile_list_entry")) return (int32_t)sizeof(av1g_tile_list_entry);
+    if (!strcmp(name, "av1g_tile_list_job")) return (int32_t)sizeof(av1g_tile_list_job);
+    if (!strcmp(name, "av1g_tile_list_header")) return (int32_t)sizeof(av1g_tile_list_header);
+    if (!strcmp(name, "av1g_tile_list_obu_entry")) return (int32_t)sizeof(av1g_tile_list_obu_entry);
     return -1;
 }
 
@@ -481,6 +486,15 @@ av1g_status av1g_run_mf_project(const av1g_mf_project_job* jobs, int32_t n, void
     if (n == 0) return AV1G_OK;
     std::string err;
     av1g_status st = mf_project_run(jobs, n, (cudaStream_t)stream, err);
+    if (st != AV1G_OK) g_err = err;
+    return st;
+}
+av1g_status av1g_run_tile_list_output(const av1g_tile_list_job* jobs, int32_t n, void* stream) {
+    g_err.clear();
+    if (n < 0 || (n > 0 && !jobs)) return fail(AV1G_EINVAL, "bad job array");
+    if (n == 0) return AV1G_OK;
+    std::string err;
+    av1g_status st = tile_list_run(jobs, n, (cudaStream_t)stream, err);
     if (st != AV1G_OK) g_err = err;
     return st;
 }

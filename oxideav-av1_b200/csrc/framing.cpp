@@ -100,6 +100,7 @@ const char* fe_text(int code) {
         case AV1G_FE_OUTPUT_TOO_SMALL: return "output buffer too small";
         case AV1G_FE_UNSUPPORTED_OBU: return "reserved OBU type in a temporal unit";
         case AV1G_FE_TEMPORAL_POINT_INFO_UNSUPPORTED: return "temporal_point_info is not supported";
+        case AV1G_FE_TILE_LIST_INVALID: return "tile list outside the conformance bounds";
         default: return "framing error";
     }
 }
@@ -612,6 +613,68 @@ av1g_status av1g_frame_header_prefix(const uint8_t* payload, size_t n, const av1
     const int c = parse_prefix(payload, n, *sh, o);
     if (c) return done(c);
     *out = o;
+    return AV1G_OK;
+}
+
+av1g_status av1g_parse_tile_list(const uint8_t* payload, size_t n, av1g_tile_list_header* hdr,
+                                 av1g_tile_list_obu_entry* entries, int32_t cap) {
+    g_code = AV1G_FE_NONE;
+    if (!hdr || (!payload && n) || cap < 0 || (cap > 0 && !entries)) return fe(AV1G_FE_UNEXPECTED_END, "null argument");
+    if (n < 4) return done(AV1G_FE_UNEXPECTED_END);
+    av1g_tile_list_header h;
+    memset(&h, 0, sizeof h);
+    h.output_frame_width_in_tiles_minus_1 = payload[0];
+    h.output_frame_height_in_tiles_minus_1 = payload[1];
+    h.tile_count_minus_1 = payload[2] << 8 | payload[3];
+    if (h.tile_count_minus_1 > 511) return done(AV1G_FE_TILE_LIST_INVALID);
+    size_t at = 4;
+    for (int k = 0; k <= h.tile_count_minus_1; k++) {
+        if (n - at < 5) return done(AV1G_FE_UNEXPECTED_END);
+        av1g_tile_list_obu_entry e;
+        memset(&e, 0, sizeof e);
+        e.anchor_frame_idx = payload[at];
+        if (e.anchor_frame_idx > 127) return done(AV1G_FE_TILE_LIST_INVALID);
+        e.anchor_tile_row = payload[at + 1];
+        e.anchor_tile_col = payload[at + 2];
+        e.data_size = (uint64_t)(payload[at + 3] << 8 | payload[at + 4]) + 1;
+        at += 5;
+        if (e.data_size > n - at) return done(AV1G_FE_UNEXPECTED_END);
+        e.data_offset = at;
+        at += e.data_size;
+        if (k < cap) entries[k] = e;
+    }
+    if (at != n) return done(AV1G_FE_TILE_LIST_INVALID);
+    if (h.tile_count_minus_1 + 1 > cap) return done(AV1G_FE_OUTPUT_TOO_SMALL);
+    *hdr = h;
+    return AV1G_OK;
+}
+
+av1g_status av1g_write_tile_list(const av1g_tile_list_header* hdr, const av1g_tile_list_obu_entry* entries,
+                                 int32_t count, const uint8_t* data, uint8_t* out, size_t cap, uint64_t* out_len) {
+    g_code = AV1G_FE_NONE;
+    if (!hdr || !out_len || count < 0 || (count > 0 && (!entries || !data)))
+        return fe(AV1G_FE_UNEXPECTED_END, "null argument");
+    if (count < 1 || count > 512) return done(AV1G_FE_TILE_LIST_INVALID);
+    std::vector<uint8_t> b;
+    b.push_back((uint8_t)hdr->output_frame_width_in_tiles_minus_1);
+    b.push_back((uint8_t)hdr->output_frame_height_in_tiles_minus_1);
+    b.push_back((uint8_t)((count - 1) >> 8));
+    b.push_back((uint8_t)(count - 1));
+    for (int k = 0; k < count; k++) {
+        const av1g_tile_list_obu_entry& e = entries[k];
+        if (e.anchor_frame_idx < 0 || e.anchor_frame_idx > 127 || e.data_size < 1 || e.data_size > 65536)
+            return done(AV1G_FE_TILE_LIST_INVALID);
+        b.push_back((uint8_t)e.anchor_frame_idx);
+        b.push_back((uint8_t)e.anchor_tile_row);
+        b.push_back((uint8_t)e.anchor_tile_col);
+        b.push_back((uint8_t)((e.data_size - 1) >> 8));
+        b.push_back((uint8_t)(e.data_size - 1));
+        b.insert(b.end(), data + e.data_offset, data + e.data_offset + e.data_size);
+    }
+    *out_len = b.size();
+    if (!out) return AV1G_OK;
+    if (b.size() > cap) return done(AV1G_FE_OUTPUT_TOO_SMALL);
+    memcpy(out, b.data(), b.size());
     return AV1G_OK;
 }
 

@@ -3,7 +3,8 @@
 Names and behaviour mirror the reference's framing layer — ``parse_leb128`` /
 ``parse_obu`` / ``ObuIter`` (src/obu.rs), ``IvfReader`` (src/encoder/ivf.rs),
 ``split_temporal_units`` / ``build_from_temporal_units`` (src/annexb.rs),
-``parse_sequence_header`` (src/sequence_header.rs) — and the OBU walk of a
+``parse_sequence_header`` (src/sequence_header.rs), ``parse_tile_list_obu`` /
+``write_tile_list_obu`` (src/tile_list.rs) — and the OBU walk of a
 temporal unit (decode_temporal_unit_spec, src/decoder/frame_driver.rs:1590).
 Errors raise ``FramingError`` whose ``variant`` is the reference's error
 variant name.  The work happens in the library's host code (framing.cpp).
@@ -23,7 +24,8 @@ VARIANTS = {abi.FE_UNEXPECTED_END: "UnexpectedEnd", abi.FE_FORBIDDEN_BIT_SET: "F
             abi.FE_REDUCED_STILL_REQUIRES_STILL: "ReducedStillRequiresStill",
             abi.FE_OPERATING_POINT_OUT_OF_RANGE: "OperatingPointOutOfRange",
             abi.FE_OUTPUT_TOO_SMALL: "OutputTooSmall", abi.FE_UNSUPPORTED_OBU: "UnsupportedObu",
-            abi.FE_TEMPORAL_POINT_INFO_UNSUPPORTED: "TemporalPointInfoUnsupported"}
+            abi.FE_TEMPORAL_POINT_INFO_UNSUPPORTED: "TemporalPointInfoUnsupported",
+            abi.FE_TILE_LIST_INVALID: "TileListInvalid"}
 
 OBU_NAMES = {1: "SequenceHeader", 2: "TemporalDelimiter", 3: "FrameHeader", 4: "TileGroup", 5: "Metadata",
              6: "Frame", 7: "RedundantFrameHeader", 8: "TileList", 15: "Padding"}
@@ -222,3 +224,51 @@ def ivf_shown_frames(data, chosen_op=0):
     """Frames a whole IVF stream outputs under operating point chosen_op."""
     w = TemporalUnitWalker(chosen_op)
     return sum(w.shown_frames(f.payload) for f in IvfReader(data).read_all())
+
+
+@dataclass
+class TileListEntry:
+    anchor_frame_idx: int
+    anchor_tile_row: int
+    anchor_tile_col: int
+    coded_tile_data: bytes
+
+
+@dataclass
+class TileListObu:
+    output_frame_width_in_tiles_minus_1: int
+    output_frame_height_in_tiles_minus_1: int
+    entries: list
+
+
+def parse_tile_list_obu(payload):
+    """parse_tile_list_obu (src/tile_list.rs:102)."""
+    lib = abi.load()
+    data, p = _buf(payload)
+    hdr = abi.TileListHeader()
+    ents = (abi.TileListObuEntry * 512)()
+    _check(lib, lib.av1g_parse_tile_list(p, len(data), C.byref(hdr), ents, 512))
+    out = [TileListEntry(e.anchor_frame_idx, e.anchor_tile_row, e.anchor_tile_col,
+                         data[e.data_offset: e.data_offset + e.data_size])
+           for e in ents[: hdr.tile_count_minus_1 + 1]]
+    return TileListObu(hdr.output_frame_width_in_tiles_minus_1, hdr.output_frame_height_in_tiles_minus_1, out)
+
+
+def write_tile_list_obu(tl):
+    """write_tile_list_obu (src/tile_list.rs:156)."""
+    lib = abi.load()
+    hdr = abi.TileListHeader(tl.output_frame_width_in_tiles_minus_1, tl.output_frame_height_in_tiles_minus_1,
+                             max(len(tl.entries) - 1, 0), 0)
+    data = b"".join(bytes(e.coded_tile_data) for e in tl.entries)
+    ents = (abi.TileListObuEntry * max(1, len(tl.entries)))()
+    off = 0
+    for i, e in enumerate(tl.entries):
+        ents[i] = abi.TileListObuEntry(e.anchor_frame_idx, e.anchor_tile_row, e.anchor_tile_col, 0, off,
+                                       len(e.coded_tile_data))
+        off += len(e.coded_tile_data)
+    data, p = _buf(data if data else b"\0")
+    need = C.c_uint64()
+    _check(lib, lib.av1g_write_tile_list(C.byref(hdr), ents, len(tl.entries), p, None, 0, C.byref(need)))
+    out = (C.c_uint8 * max(1, need.value))()
+    _check(lib, lib.av1g_write_tile_list(C.byref(hdr), ents, len(tl.entries), p, out, need.value, C.byref(need)))
+    return bytes(out)[: need.value]

@@ -293,3 +293,40 @@ def test_operating_point_selection_drops_other_layers():
     assert [d.type_name for d in full.walk(tus[1])] == ["Frame"]
     assert _variant(framing.TemporalUnitWalker(2).walk, tus[0]) == "OperatingPointOutOfRange"
     assert _variant(framing.TemporalUnitWalker(0).walk, obu(2, b"") + obu(9, b"\x00")) == "UnsupportedObu"
+
+
+# --- src/tile_list.rs unit tests (§5.12 tile list OBU) ---
+
+def _sample_tl():
+    E = framing.TileListEntry
+    return framing.TileListObu(1, 0, [E(0, 0, 0, bytes([0xAA, 0xBB, 0xCC])), E(3, 0, 1, bytes([0x11]))])
+
+
+def test_tile_list_round_trips_byte_exact():
+    tl = _sample_tl()
+    b = framing.write_tile_list_obu(tl)
+    assert len(b) == 4 + 5 + 3 + 5 + 1
+    assert b[:4] == bytes([1, 0, 0x00, 0x01])
+    assert framing.parse_tile_list_obu(b) == tl
+
+
+def test_tile_list_rejects_truncated_and_overlong_payloads():
+    b = framing.write_tile_list_obu(_sample_tl())
+    assert _variant(framing.parse_tile_list_obu, b[:-1]) == "UnexpectedEnd"
+    assert _variant(framing.parse_tile_list_obu, b + b"\x00") == "TileListInvalid"
+    assert _variant(framing.parse_tile_list_obu, b[:3]) == "UnexpectedEnd"
+
+
+def test_tile_list_conformance_bounds():
+    assert _variant(framing.parse_tile_list_obu, bytes([0, 0, 0x02, 0x00])) == "TileListInvalid"
+    assert _variant(framing.parse_tile_list_obu, bytes([0, 0, 0, 0, 128, 0, 0, 0, 0, 0xAA])) == "TileListInvalid"
+    tl = _sample_tl()
+    tl.entries[0].anchor_frame_idx = 128
+    assert _variant(framing.write_tile_list_obu, tl) == "TileListInvalid"
+    tl = _sample_tl()
+    tl.entries[0].coded_tile_data = b""
+    assert _variant(framing.write_tile_list_obu, tl) == "TileListInvalid"
+    assert _variant(framing.write_tile_list_obu, framing.TileListObu(0, 0, [])) == "TileListInvalid"
+    big = framing.TileListObu(31, 15, [framing.TileListEntry(k % 128, k % 4, k % 8, bytes([k & 255]) * (1 + k % 3))
+                                       for k in range(512)])
+    assert framing.parse_tile_list_obu(framing.write_tile_list_obu(big)) == big
