@@ -907,6 +907,40 @@ typedef struct av1g_frame_prefix {
 av1g_status av1g_frame_header_prefix(const uint8_t* payload, size_t n, const av1g_sequence_header* sh,
                                      av1g_frame_prefix* out);
 
+/* §8.2 symbol decoder (SymbolDecoder, src/symbol_decoder.rs), the first
+ * piece of the host parse layer: the arithmetic decoder the tile walker reads
+ * every symbol with.  The state is caller-owned and plain; `data` must stay
+ * valid while it is in use.  A CDF of an n-symbol alphabet is n + 1 uint16
+ * values: the n cumulative values (the last 32768) and the adaptation
+ * counter. */
+typedef struct av1g_symbol_decoder {
+    const uint8_t* data;
+    uint64_t size;               /* sz: the tile's byte count                 */
+    uint64_t pos;                /* bits consumed from data                   */
+    int64_t max_bits;            /* SymbolMaxBits                             */
+    uint32_t value;              /* SymbolValue                               */
+    uint32_t range;              /* SymbolRange                               */
+    int32_t disable_cdf_update;
+    int32_t pad;
+} av1g_symbol_decoder;
+#define AV1G_FE_SYMBOL_STATE_INVARIANT 18 /* Error::SymbolStateInvariantBroken                */
+#define AV1G_FE_SYMBOL_EXIT_UNDERFLOW 19  /* Error::SymbolExitUnderflow                       */
+/* init_symbol(sz) (§8.2.2, symbol_decoder.rs init_symbol). */
+av1g_status av1g_symbol_init(av1g_symbol_decoder* d, const uint8_t* data, size_t sz, int32_t disable_cdf_update);
+/* read_symbol (§8.2.6) with the §8.3 CDF update unless disabled. */
+av1g_status av1g_symbol_read(av1g_symbol_decoder* d, uint16_t* cdf, int32_t n, uint32_t* symbol);
+av1g_status av1g_symbol_read_bool(av1g_symbol_decoder* d, uint32_t* bit);
+av1g_status av1g_symbol_read_literal(av1g_symbol_decoder* d, int32_t n, uint32_t* value);
+av1g_status av1g_symbol_read_ns(av1g_symbol_decoder* d, uint32_t n, uint32_t* value);
+/* decode_signed_subexp_with_ref_bool (low, high, k, r) (§5.9.26-§5.9.28 with
+ * bools from the symbol decoder). */
+av1g_status av1g_symbol_read_signed_subexp(av1g_symbol_decoder* d, int64_t low, int64_t high, uint32_t k, int64_t r,
+                                           int64_t* value);
+/* exit_symbol (§8.2.4): the trailing-bit position and the padding end. */
+av1g_status av1g_symbol_exit(av1g_symbol_decoder* d, uint64_t* trailing_bit_position, uint64_t* padding_end);
+/* The §8.3 CDF adaptation after decoding `symbol` of an n-symbol CDF. */
+void av1g_update_cdf(uint16_t* cdf, uint32_t symbol, int32_t n);
+
 /* §5.12 tile list OBU (TileListObu / TileListEntry, src/tile_list.rs): the
  * output size in tiles and, per entry, the anchor and tile it names and
  * where its coded tile data lies in the payload. */

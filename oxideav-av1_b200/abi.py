@@ -300,6 +300,13 @@ class TileListObuEntry(C.Structure):
 
 
 FE_TILE_LIST_INVALID = 17
+FE_SYMBOL_STATE_INVARIANT, FE_SYMBOL_EXIT_UNDERFLOW = 18, 19
+
+
+class SymbolDecoder(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("size", C.c_uint64), ("pos", C.c_uint64), ("max_bits", C.c_int64),
+                ("value", C.c_uint32), ("range", C.c_uint32), ("disable_cdf_update", C.c_int32),
+                ("pad", C.c_int32)]
 FE_NONE, FE_UNEXPECTED_END, FE_FORBIDDEN_BIT_SET, FE_MISSING_SIZE_FIELD = 0, 1, 2, 3
 FE_LEB128_OVERFLOW, FE_LEB128_TOO_LONG, FE_SIZE_OVERFLOW, FE_ANNEXB_INVALID = 4, 5, 6, 7
 FE_IVF_BAD_MAGIC, FE_IVF_UNSUPPORTED_VERSION, FE_IVF_UNSUPPORTED_HEADER_LENGTH = 8, 9, 10
@@ -322,7 +329,8 @@ _STRUCTS = {"av1g_film_grain": FilmGrain, "av1g_frame_header": FrameHeader, "av1
             "av1g_ivf_frame": IvfFrame, "av1g_operating_point": OperatingPoint,
             "av1g_sequence_header": SequenceHeader, "av1g_frame_prefix": FramePrefix,
             "av1g_tile_list_entry": TileListEntry, "av1g_tile_list_job": TileListJob,
-            "av1g_tile_list_header": TileListHeader, "av1g_tile_list_obu_entry": TileListObuEntry}
+            "av1g_tile_list_header": TileListHeader, "av1g_tile_list_obu_entry": TileListObuEntry,
+            "av1g_symbol_decoder": SymbolDecoder}
 
 # exported entry points and their ctypes signatures
 _SIGS = {
@@ -373,6 +381,16 @@ _SIGS = {
                                        C.POINTER(TileListObuEntry), C.c_int32]),
     "av1g_write_tile_list": (C.c_int, [C.POINTER(TileListHeader), C.POINTER(TileListObuEntry), C.c_int32,
                                        C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint64)]),
+    "av1g_symbol_init": (C.c_int, [C.POINTER(SymbolDecoder), C.c_void_p, C.c_size_t, C.c_int32]),
+    "av1g_symbol_read": (C.c_int, [C.POINTER(SymbolDecoder), C.POINTER(C.c_uint16), C.c_int32,
+                                   C.POINTER(C.c_uint32)]),
+    "av1g_symbol_read_bool": (C.c_int, [C.POINTER(SymbolDecoder), C.POINTER(C.c_uint32)]),
+    "av1g_symbol_read_literal": (C.c_int, [C.POINTER(SymbolDecoder), C.c_int32, C.POINTER(C.c_uint32)]),
+    "av1g_symbol_read_ns": (C.c_int, [C.POINTER(SymbolDecoder), C.c_uint32, C.POINTER(C.c_uint32)]),
+    "av1g_symbol_read_signed_subexp": (C.c_int, [C.POINTER(SymbolDecoder), C.c_int64, C.c_int64, C.c_uint32,
+                                                 C.c_int64, C.POINTER(C.c_int64)]),
+    "av1g_symbol_exit": (C.c_int, [C.POINTER(SymbolDecoder), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "av1g_update_cdf": (None, [C.POINTER(C.c_uint16), C.c_uint32, C.c_int32]),
     "av1g_engine_create": (C.c_int, [C.POINTER(Config), C.POINTER(C.c_void_p)]),
     "av1g_engine_destroy": (None, [C.c_void_p]),
     "av1g_engine_get_stats": (C.c_int, [C.c_void_p, C.POINTER(EngineStats)]),

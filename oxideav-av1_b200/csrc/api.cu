@@ -422,6 +422,7 @@ int32_t av1g_struct_size(const char* name) {
     if (!strcmp(name, "av1g_tile_list_job")) return (int32_t)sizeof(av1g_tile_list_job);
     if (!strcmp(name, "av1g_tile_list_header")) return (int32_t)sizeof(av1g_tile_list_header);
     if (!strcmp(name, "av1g_tile_list_obu_entry")) return (int32_t)sizeof(av1g_tile_list_obu_entry);
+    if (!strcmp(name, "av1g_symbol_decoder")) return (int32_t)sizeof(av1g_symbol_decoder);
     return -1;
 }
 

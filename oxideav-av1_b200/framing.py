@@ -25,7 +25,9 @@ VARIANTS = {abi.FE_UNEXPECTED_END: "UnexpectedEnd", abi.FE_FORBIDDEN_BIT_SET: "F
             abi.FE_OPERATING_POINT_OUT_OF_RANGE: "OperatingPointOutOfRange",
             abi.FE_OUTPUT_TOO_SMALL: "OutputTooSmall", abi.FE_UNSUPPORTED_OBU: "UnsupportedObu",
             abi.FE_TEMPORAL_POINT_INFO_UNSUPPORTED: "TemporalPointInfoUnsupported",
-            abi.FE_TILE_LIST_INVALID: "TileListInvalid"}
+            abi.FE_TILE_LIST_INVALID: "TileListInvalid",
+            abi.FE_SYMBOL_STATE_INVARIANT: "SymbolStateInvariantBroken",
+            abi.FE_SYMBOL_EXIT_UNDERFLOW: "SymbolExitUnderflow"}
 
 OBU_NAMES = {1: "SequenceHeader", 2: "TemporalDelimiter", 3: "FrameHeader", 4: "TileGroup", 5: "Metadata",
              6: "Frame", 7: "RedundantFrameHeader", 8: "TileList", 15: "Padding"}
@@ -272,3 +274,58 @@ def write_tile_list_obu(tl):
     out = (C.c_uint8 * max(1, need.value))()
     _check(lib, lib.av1g_write_tile_list(C.byref(hdr), ents, len(tl.entries), p, out, need.value, C.byref(need)))
     return bytes(out)[: need.value]
+
+
+class SymbolDecoder:
+    """SymbolDecoder (src/symbol_decoder.rs) over the library's §8.2 decoder:
+    init_symbol, read_symbol (a CDF is a list of n values plus the counter,
+    adapted in place), read_bool, read_literal, read_ns,
+    decode_signed_subexp_with_ref_bool and exit_symbol."""
+
+    def __init__(self, data, sz, disable_cdf_update):
+        self._lib = abi.load()
+        self._data, p = _buf(data)
+        self.s = abi.SymbolDecoder()
+        _check(self._lib, self._lib.av1g_symbol_init(C.byref(self.s), p, sz, int(disable_cdf_update)))
+
+    @property
+    def position(self):
+        return self.s.pos
+
+    def read_symbol(self, cdf):
+        arr = (C.c_uint16 * len(cdf))(*cdf)
+        out = C.c_uint32()
+        _check(self._lib, self._lib.av1g_symbol_read(C.byref(self.s), arr, len(cdf) - 1, C.byref(out)))
+        cdf[:] = list(arr)
+        return out.value
+
+    def read_bool(self):
+        out = C.c_uint32()
+        _check(self._lib, self._lib.av1g_symbol_read_bool(C.byref(self.s), C.byref(out)))
+        return out.value
+
+    def read_literal(self, n):
+        out = C.c_uint32()
+        _check(self._lib, self._lib.av1g_symbol_read_literal(C.byref(self.s), n, C.byref(out)))
+        return out.value
+
+    def read_ns(self, n):
+        out = C.c_uint32()
+        _check(self._lib, self._lib.av1g_symbol_read_ns(C.byref(self.s), n, C.byref(out)))
+        return out.value
+
+    def decode_signed_subexp_with_ref_bool(self, low, high, k, r):
+        out = C.c_int64()
+        _check(self._lib, self._lib.av1g_symbol_read_signed_subexp(C.byref(self.s), low, high, k, r, C.byref(out)))
+        return out.value
+
+    def exit_symbol(self):
+        t, e = C.c_uint64(), C.c_uint64()
+        _check(self._lib, self._lib.av1g_symbol_exit(C.byref(self.s), C.byref(t), C.byref(e)))
+        return t.value, e.value
+
+
+def update_cdf(cdf, symbol, n):
+    arr = (C.c_uint16 * len(cdf))(*cdf)
+    abi.load().av1g_update_cdf(arr, symbol, n)
+    cdf[:] = list(arr)
