@@ -907,6 +907,85 @@ typedef struct av1g_frame_prefix {
 av1g_status av1g_frame_header_prefix(const uint8_t* payload, size_t n, const av1g_sequence_header* sh,
                                      av1g_frame_prefix* out);
 
+/* §5.9 uncompressed header (parse_frame_header_with_refs,
+ * src/frame_header.rs:726; the parameter blocks of
+ * src/uncompressed_header_tail.rs and src/tile_info.rs).  The §7.20
+ * reference state the header reads (RefInfo) is caller-owned: initialise it
+ * with av1g_ref_state_init, parse each frame header against it and apply
+ * av1g_ref_state_update once the frame is decoded (or at once for a shown
+ * existing frame). */
+typedef struct av1g_ref_state {
+    int32_t valid[8];
+    int32_t frame_id[8];
+    int32_t frame_type[8];
+    int32_t order_hint[8];
+    int32_t saved_order_hints[8][8];
+    int32_t upscaled_width[8], frame_width[8], frame_height[8], render_width[8], render_height[8];
+    int32_t mi_cols[8], mi_rows[8];
+    int32_t gm_params[8][8][6];       /* [slot][ref LAST..ALTREF at 1..7][i] */
+    int8_t lf_ref_deltas[8][8];
+    int8_t lf_mode_deltas[8][2];
+    uint8_t seg_feature_enabled[8][8][8];
+    int16_t seg_feature_data[8][8][8];
+    av1g_film_grain film_grain[8];
+} av1g_ref_state;
+
+/* Everything a frame header fixes, flattened.  pf is the post-filter header
+ * the chain kernels take (sizes, format, loop filter, segmentation loop-filter
+ * features, CDEF, loop restoration, resolved film grain), filled from the
+ * bitstream; the rest are the §5.9 syntax elements and derived values the
+ * reconstruction needs. */
+typedef struct av1g_parsed_frame_header {
+    av1g_frame_header pf;
+    int32_t show_existing_frame, frame_to_show_map_idx, frame_type, show_frame, showable_frame;
+    int32_t error_resilient_mode, disable_cdf_update, allow_screen_content_tools, force_integer_mv;
+    int32_t current_frame_id, frame_size_override_flag, order_hint, primary_ref_frame, refresh_frame_flags;
+    int32_t frame_refs_short_signaling, ref_frame_idx[7];
+    int32_t allow_high_precision_mv, interpolation_filter, is_motion_mode_switchable, use_ref_frame_mvs;
+    int32_t order_hints[8];                   /* OrderHints[LAST_FRAME + i] at [1 + i] */
+    int32_t render_width, render_height, superres_denom, disable_frame_end_update_cdf;
+    int32_t tile_cols, tile_rows, tile_cols_log2, tile_rows_log2, context_update_tile_id, tile_size_bytes;
+    int32_t mi_col_starts[65], mi_row_starts[65];
+    int32_t base_q_idx, delta_q_y_dc, delta_q_u_dc, delta_q_u_ac, delta_q_v_dc, delta_q_v_ac;
+    int32_t using_qmatrix, qm_y, qm_u, qm_v;
+    int32_t segmentation_enabled, segmentation_update_map, segmentation_temporal_update;
+    int32_t segmentation_update_data;
+    uint8_t seg_feature_enabled[8][8];
+    int16_t seg_feature_data[8][8];
+    int32_t delta_q_present, delta_q_res, delta_lf_present, delta_lf_res;
+    int32_t lossless[8], all_lossless;
+    int32_t lr_unit_shift, lr_uv_shift;
+    int32_t tx_mode, reference_select, skip_mode_present, skip_mode_frame[2];
+    int32_t allow_warped_motion, reduced_tx_set;
+    int32_t gm_type[8];
+    int32_t gm_params[8][6];
+    int32_t update_grain, film_grain_params_ref_idx;
+    int32_t temporal_id, spatial_id;          /* of the OBU that carried it (input) */
+    uint32_t header_bits;                     /* bits the uncompressed header took */
+} av1g_parsed_frame_header;
+
+#define AV1G_FE_FRAME_HEADER_INVALID 20   /* a header the reference rejects (invalid syntax or
+                                             state it does not handle)                        */
+void av1g_ref_state_init(av1g_ref_state* st);
+/* temporal_id / spatial_id: the carrying OBU's extension ids (0 without). */
+av1g_status av1g_parse_frame_header(const uint8_t* payload, size_t n, const av1g_sequence_header* sh,
+                                    const av1g_ref_state* st, int32_t temporal_id, int32_t spatial_id,
+                                    av1g_parsed_frame_header* out);
+/* §7.20 reference_frame_update of the header state (and §7.21 for a shown
+ * existing key frame). */
+av1g_status av1g_ref_state_update(av1g_ref_state* st, const av1g_parsed_frame_header* fh);
+
+/* §5.11.1 tile group: the tile range and each tile's bytes in the payload
+ * (a tile group OBU, or the rest of a frame OBU after its byte-aligned
+ * header). */
+typedef struct av1g_tile_span {
+    int32_t tile_num;
+    int32_t pad;
+    uint64_t offset, size;
+} av1g_tile_span;
+av1g_status av1g_parse_tile_group(const uint8_t* payload, size_t n, const av1g_parsed_frame_header* fh,
+                                  int32_t* tg_start, int32_t* tg_end, av1g_tile_span* tiles, int32_t cap);
+
 /* §8.2 symbol decoder (SymbolDecoder, src/symbol_decoder.rs), the first
  * piece of the host parse layer: the arithmetic decoder the tile walker reads
  * every symbol with.  The state is caller-owned and plain; `data` must stay

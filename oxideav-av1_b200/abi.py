@@ -303,6 +303,56 @@ FE_TILE_LIST_INVALID = 17
 FE_SYMBOL_STATE_INVARIANT, FE_SYMBOL_EXIT_UNDERFLOW = 18, 19
 
 
+_I32 = C.c_int32
+
+
+class RefState(C.Structure):
+    _fields_ = [(n, _I32 * 8) for n in ("valid", "frame_id", "frame_type", "order_hint")] + \
+              [("saved_order_hints", (_I32 * 8) * 8)] + \
+              [(n, _I32 * 8) for n in ("upscaled_width", "frame_width", "frame_height", "render_width",
+                                       "render_height", "mi_cols", "mi_rows")] + \
+              [("gm_params", ((_I32 * 6) * 8) * 8), ("lf_ref_deltas", (C.c_int8 * 8) * 8),
+               ("lf_mode_deltas", (C.c_int8 * 2) * 8), ("seg_feature_enabled", ((C.c_uint8 * 8) * 8) * 8),
+               ("seg_feature_data", ((C.c_int16 * 8) * 8) * 8), ("film_grain", FilmGrain * 8)]
+
+
+class ParsedFrameHeader(C.Structure):
+    _fields_ = [("pf", FrameHeader)] + \
+              [(n, _I32) for n in ("show_existing_frame", "frame_to_show_map_idx", "frame_type", "show_frame",
+                                   "showable_frame", "error_resilient_mode", "disable_cdf_update",
+                                   "allow_screen_content_tools", "force_integer_mv", "current_frame_id",
+                                   "frame_size_override_flag", "order_hint", "primary_ref_frame",
+                                   "refresh_frame_flags", "frame_refs_short_signaling")] + \
+              [("ref_frame_idx", _I32 * 7)] + \
+              [(n, _I32) for n in ("allow_high_precision_mv", "interpolation_filter", "is_motion_mode_switchable",
+                                   "use_ref_frame_mvs")] + \
+              [("order_hints", _I32 * 8)] + \
+              [(n, _I32) for n in ("render_width", "render_height", "superres_denom",
+                                   "disable_frame_end_update_cdf", "tile_cols", "tile_rows", "tile_cols_log2",
+                                   "tile_rows_log2", "context_update_tile_id", "tile_size_bytes")] + \
+              [("mi_col_starts", _I32 * 65), ("mi_row_starts", _I32 * 65)] + \
+              [(n, _I32) for n in ("base_q_idx", "delta_q_y_dc", "delta_q_u_dc", "delta_q_u_ac", "delta_q_v_dc",
+                                   "delta_q_v_ac", "using_qmatrix", "qm_y", "qm_u", "qm_v", "segmentation_enabled",
+                                   "segmentation_update_map", "segmentation_temporal_update",
+                                   "segmentation_update_data")] + \
+              [("seg_feature_enabled", (C.c_uint8 * 8) * 8), ("seg_feature_data", (C.c_int16 * 8) * 8)] + \
+              [(n, _I32) for n in ("delta_q_present", "delta_q_res", "delta_lf_present", "delta_lf_res")] + \
+              [("lossless", _I32 * 8)] + \
+              [(n, _I32) for n in ("all_lossless", "lr_unit_shift", "lr_uv_shift", "tx_mode", "reference_select",
+                                   "skip_mode_present")] + \
+              [("skip_mode_frame", _I32 * 2), ("allow_warped_motion", _I32), ("reduced_tx_set", _I32),
+               ("gm_type", _I32 * 8), ("gm_params", (_I32 * 6) * 8)] + \
+              [(n, _I32) for n in ("update_grain", "film_grain_params_ref_idx", "temporal_id", "spatial_id")] + \
+              [("header_bits", C.c_uint32)]
+
+
+class TileSpan(C.Structure):
+    _fields_ = [("tile_num", _I32), ("pad", _I32), ("offset", C.c_uint64), ("size", C.c_uint64)]
+
+
+FE_FRAME_HEADER_INVALID = 20
+
+
 class SymbolDecoder(C.Structure):
     _fields_ = [("data", C.c_void_p), ("size", C.c_uint64), ("pos", C.c_uint64), ("max_bits", C.c_int64),
                 ("value", C.c_uint32), ("range", C.c_uint32), ("disable_cdf_update", C.c_int32),
@@ -330,7 +380,8 @@ _STRUCTS = {"av1g_film_grain": FilmGrain, "av1g_frame_header": FrameHeader, "av1
             "av1g_sequence_header": SequenceHeader, "av1g_frame_prefix": FramePrefix,
             "av1g_tile_list_entry": TileListEntry, "av1g_tile_list_job": TileListJob,
             "av1g_tile_list_header": TileListHeader, "av1g_tile_list_obu_entry": TileListObuEntry,
-            "av1g_symbol_decoder": SymbolDecoder}
+            "av1g_symbol_decoder": SymbolDecoder, "av1g_ref_state": RefState,
+            "av1g_parsed_frame_header": ParsedFrameHeader, "av1g_tile_span": TileSpan}
 
 # exported entry points and their ctypes signatures
 _SIGS = {
@@ -391,6 +442,13 @@ _SIGS = {
                                                  C.c_int64, C.POINTER(C.c_int64)]),
     "av1g_symbol_exit": (C.c_int, [C.POINTER(SymbolDecoder), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "av1g_update_cdf": (None, [C.POINTER(C.c_uint16), C.c_uint32, C.c_int32]),
+    "av1g_ref_state_init": (None, [C.POINTER(RefState)]),
+    "av1g_parse_frame_header": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(SequenceHeader), C.POINTER(RefState),
+                                          C.c_int32, C.c_int32, C.POINTER(ParsedFrameHeader)]),
+    "av1g_ref_state_update": (C.c_int, [C.POINTER(RefState), C.POINTER(ParsedFrameHeader)]),
+    "av1g_parse_tile_group": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(ParsedFrameHeader),
+                                        C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(TileSpan),
+                                        C.c_int32]),
     "av1g_engine_create": (C.c_int, [C.POINTER(Config), C.POINTER(C.c_void_p)]),
     "av1g_engine_destroy": (None, [C.c_void_p]),
     "av1g_engine_get_stats": (C.c_int, [C.c_void_p, C.POINTER(EngineStats)]),

@@ -423,6 +423,9 @@ int32_t av1g_struct_size(const char* name) {
     if (!strcmp(name, "av1g_tile_list_header")) return (int32_t)sizeof(av1g_tile_list_header);
     if (!strcmp(name, "av1g_tile_list_obu_entry")) return (int32_t)sizeof(av1g_tile_list_obu_entry);
     if (!strcmp(name, "av1g_symbol_decoder")) return (int32_t)sizeof(av1g_symbol_decoder);
+    if (!strcmp(name, "av1g_ref_state")) return (int32_t)sizeof(av1g_ref_state);
+    if (!strcmp(name, "av1g_parsed_frame_header")) return (int32_t)sizeof(av1g_parsed_frame_header);
+    if (!strcmp(name, "av1g_tile_span")) return (int32_t)sizeof(av1g_tile_span);
     return -1;
 }
 

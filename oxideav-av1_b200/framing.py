@@ -27,7 +27,8 @@ VARIANTS = {abi.FE_UNEXPECTED_END: "UnexpectedEnd", abi.FE_FORBIDDEN_BIT_SET: "F
             abi.FE_TEMPORAL_POINT_INFO_UNSUPPORTED: "TemporalPointInfoUnsupported",
             abi.FE_TILE_LIST_INVALID: "TileListInvalid",
             abi.FE_SYMBOL_STATE_INVARIANT: "SymbolStateInvariantBroken",
-            abi.FE_SYMBOL_EXIT_UNDERFLOW: "SymbolExitUnderflow"}
+            abi.FE_SYMBOL_EXIT_UNDERFLOW: "SymbolExitUnderflow",
+            abi.FE_FRAME_HEADER_INVALID: "FrameHeaderInvalid"}
 
 OBU_NAMES = {1: "SequenceHeader", 2: "TemporalDelimiter", 3: "FrameHeader", 4: "TileGroup", 5: "Metadata",
              6: "Frame", 7: "RedundantFrameHeader", 8: "TileList", 15: "Padding"}
@@ -329,3 +330,72 @@ def update_cdf(cdf, symbol, n):
     arr = (C.c_uint16 * len(cdf))(*cdf)
     abi.load().av1g_update_cdf(arr, symbol, n)
     cdf[:] = list(arr)
+
+
+def new_ref_state():
+    st = abi.RefState()
+    abi.load().av1g_ref_state_init(C.byref(st))
+    return st
+
+
+def parse_frame_header(payload, seq, state, temporal_id=0, spatial_id=0):
+    """The §5.9 uncompressed header (av1g_parsed_frame_header) of a frame
+    header or frame OBU payload against the reference state."""
+    lib = abi.load()
+    data, p = _buf(payload)
+    out = abi.ParsedFrameHeader()
+    _check(lib, lib.av1g_parse_frame_header(p, len(data), C.byref(seq), C.byref(state), temporal_id, spatial_id,
+                                            C.byref(out)))
+    return out
+
+
+def parse_tile_group(payload, fh):
+    """(tg_start, tg_end, [(tile_num, offset, size)]) of a tile group."""
+    lib = abi.load()
+    data, p = _buf(payload)
+    cap = max(1, fh.tile_cols * fh.tile_rows)
+    spans = (abi.TileSpan * cap)()
+    a, b = C.c_int32(), C.c_int32()
+    _check(lib, lib.av1g_parse_tile_group(p, len(data), C.byref(fh), C.byref(a), C.byref(b), spans, cap))
+    return a.value, b.value, [(spans[i].tile_num, spans[i].offset, spans[i].size) for i in range(b.value - a.value + 1)]
+
+
+def stream_frame_headers(temporal_units, chosen_op=0):
+    """Walks a stream's temporal units as the reference's
+    decode_temporal_unit_spec does (frame_driver.rs:1618-1700): every frame
+    header is parsed against the reference state, the tile groups of each
+    frame are laid out until the frame's last tile, and the state is updated
+    per decoded (or shown existing) frame.  Returns a list of
+    (parsed header, [tile spans]) in decode order."""
+    lib = abi.load()
+    walker = TemporalUnitWalker(chosen_op)
+    state = new_ref_state()
+    out = []
+    for tu in temporal_units:
+        pending = None
+        for d in walker.walk(tu):
+            if d.obu_type in (3, 6):  # frame header, frame
+                fh = parse_frame_header(d.payload, walker.seq, state, d.temporal_id, d.spatial_id)
+                if fh.show_existing_frame:
+                    _check(lib, lib.av1g_ref_state_update(C.byref(state), C.byref(fh)))
+                    out.append((fh, []))
+                    continue
+                if d.obu_type == 3:
+                    pending = (fh, [])
+                    continue
+                start = (fh.header_bits + 7) >> 3
+                a, b, spans = parse_tile_group(d.payload[start:], fh)
+                assert a == 0 and b == fh.tile_cols * fh.tile_rows - 1
+                _check(lib, lib.av1g_ref_state_update(C.byref(state), C.byref(fh)))
+                out.append((fh, spans))
+            elif d.obu_type == 4 and pending is not None:  # tile group
+                fh, spans = pending
+                a, b, more = parse_tile_group(d.payload, fh)
+                assert a == (spans[-1][0] + 1 if spans else 0)
+                spans = spans + more
+                pending = (fh, spans)
+                if b == fh.tile_cols * fh.tile_rows - 1:
+                    _check(lib, lib.av1g_ref_state_update(C.byref(state), C.byref(fh)))
+                    out.append((fh, spans))
+                    pending = None
+    return out

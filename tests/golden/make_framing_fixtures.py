@@ -13,6 +13,9 @@ Reads (text only; nothing of the reference is executed):
                                      the field values the test expects
   tests/annexb_conformance.rs        the external Annex B stream, its shown-
                                      frame count and digest
+  tests/frame_header_fixtures.rs     the 16 first-frame header payloads with
+                                     the field values the test expects, and
+                                     the inter-frame header it pins
 and writes framing_fixtures.json.gz next to this script.
 """
 import base64
@@ -65,6 +68,51 @@ def sequence_headers(ref):
     return out
 
 
+def _bytes_of(text):
+    return bytes(int(v, 16) for v in re.findall(r'0x([0-9a-fA-F]{2})', text))
+
+
+def _fields(text):
+    out = {}
+    for k, v in re.findall(r'(\w+):\s*(true|false|None|FrameType::\w+|Some\(\d+\)|0x[0-9a-fA-F]+|\d+)', text):
+        if v.startswith("0x"):
+            out[k] = int(v, 16)
+        elif v in ("true", "false"):
+            out[k] = v == "true"
+        elif v == "None":
+            out[k] = None
+        elif v.startswith("FrameType::"):
+            out[k] = v.split("::")[1]
+        elif v.startswith("Some("):
+            out[k] = int(v[5:-1])
+        else:
+            out[k] = int(v)
+    return out
+
+
+def frame_headers(ref):
+    """tests/frame_header_fixtures.rs: per fixture the sequence and first
+    frame OBU payloads and the expected header fields (film grain ones under
+    film_grain when the fixture has them), plus the inter-frame payloads of
+    parses_iftp_inter_frame_header."""
+    src = (ref / "tests" / "frame_header_fixtures.rs").read_text()
+    src = re.sub(r"//[^\n]*", "", src)
+    out = []
+    for m in re.finditer(r'Fixture\s*\{\s*name:\s*"([^"]+)",\s*seq_payload:\s*&\[([^\]]*)\],\s*'
+                         r'frame_payload:\s*&\[([^\]]*)\],\s*expected:\s*Expected\s*\{(.*?)trace_film_grain:\s*'
+                         r'(None|Some\(FilmGrainExpected\s*\{(.*?)\}\))', src, re.S):
+        name, seq, frame, fields, fg, fg_fields = m.groups()
+        exp = _fields(fields)
+        exp["film_grain"] = _fields(fg_fields) if fg_fields else None
+        out.append({"name": name, "seq_payload": _bytes_of(seq).hex(), "frame_payload": _bytes_of(frame).hex(),
+                    "expected": exp})
+    iftp = {}
+    for const in ("IFTP_SEQ_PAYLOAD", "IFTP_INTER_FRAME_PAYLOAD"):
+        mm = re.search(const + r'\s*:\s*&\[u8\]\s*=\s*&\[([^\]]*)\]', src, re.S)
+        iftp[const] = _bytes_of(mm.group(1)).hex()
+    return out, iftp
+
+
 def annexb_stream(ref):
     src = (ref / "tests" / "annexb_conformance.rs").read_text()
     consts = _consts(src)
@@ -76,14 +124,16 @@ def annexb_stream(ref):
 
 def main():
     ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
-    data = {"source": "reference tests: fixture_conformance.rs, sequence_header_fixtures.rs, annexb_conformance.rs",
+    data = {"source": "reference tests: fixture_conformance.rs, sequence_header_fixtures.rs, annexb_conformance.rs, "
+                      "frame_header_fixtures.rs",
             "ivf_streams": ivf_streams(ref), "sequence_headers": sequence_headers(ref),
             "annexb": annexb_stream(ref)}
+    data["frame_headers"], data["iftp"] = frame_headers(ref)
     out = HERE / "framing_fixtures.json.gz"
     with gzip.open(out, "wt") as f:
         json.dump(data, f, sort_keys=True)
     print(f"{out}: {len(data['ivf_streams'])} IVF streams, {len(data['sequence_headers'])} sequence headers, "
-          f"1 Annex B stream")
+          f"1 Annex B stream, {len(data['frame_headers'])} frame headers")
 
 
 if __name__ == "__main__":
