@@ -126,6 +126,8 @@ void frame_size_with_refs(Reader& r, const av1g_sequence_header& s, const av1g_r
 // §5.9.15 tile_info
 void tile_info(Reader& r, const av1g_sequence_header& s, av1g_parsed_frame_header& h) {
     const int mi_cols = h.pf.mi_cols, mi_rows = h.pf.mi_rows;
+    // a size taken from a reference slot that never held a frame
+    if (mi_cols <= 0 || mi_rows <= 0) throw Fail{AV1G_FE_FRAME_HEADER_INVALID, "frame header: empty frame size"};
     const bool sb128 = s.use_128x128_superblock;
     const int sb_cols = sb128 ? (mi_cols + 31) >> 5 : (mi_cols + 15) >> 4;
     const int sb_rows = sb128 ? (mi_rows + 31) >> 5 : (mi_rows + 15) >> 4;

@@ -126,3 +126,29 @@ def test_truncated_headers_are_rejected():
     with pytest.raises(FramingError) as e:
         framing.parse_frame_header(payload[:cut], seq, framing.new_ref_state())
     assert e.value.variant == "UnexpectedEnd"
+
+
+def test_corrupted_headers_error_cleanly():
+    """The reference's decoder never panics on malformed input (its fuzz
+    contract): every single-bit corruption of the first bytes of real frame
+    headers, parsed against the state the stream carries at that frame (slots
+    that never held a frame included), either parses or raises a framing
+    error.  Among them are headers that take their size from an empty slot,
+    which must be rejected rather than divide by a zero tile width."""
+    for st in GOLDEN["ivf_streams"][:12]:
+        tus = [f.payload for f in framing.IvfReader(base64.b64decode(st["ivf"])).read_all()]
+        walker = framing.TemporalUnitWalker()
+        state = framing.new_ref_state()
+        for tu in tus[:3]:
+            for d in walker.walk(tu):
+                if d.obu_type not in (3, 6):
+                    continue
+                for bit in range(min(48, 8 * len(d.payload))):
+                    p = bytearray(d.payload)
+                    p[bit >> 3] ^= 0x80 >> (bit & 7)
+                    try:
+                        framing.parse_frame_header(bytes(p), walker.seq, state)
+                    except FramingError:
+                        pass
+            # carry the state past the unit's frames, as the stream walk does
+        framing.stream_frame_headers(tus)
