@@ -131,8 +131,8 @@ def test_truncated_headers_are_rejected():
 def test_corrupted_headers_error_cleanly():
     """The reference's decoder never panics on malformed input (its fuzz
     contract): every single-bit corruption of the first bytes of real frame
-    headers, parsed against the state the stream carries at that frame (slots
-    that never held a frame included), either parses or raises a framing
+    headers of the first temporal units, parsed against an empty reference
+    state (slots that never held a frame), either parses or raises a framing
     error.  Among them are headers that take their size from an empty slot,
     which must be rejected rather than divide by a zero tile width."""
     for st in GOLDEN["ivf_streams"][:12]:
@@ -150,5 +150,4 @@ def test_corrupted_headers_error_cleanly():
                         framing.parse_frame_header(bytes(p), walker.seq, state)
                     except FramingError:
                         pass
-            # carry the state past the unit's frames, as the stream walk does
-        framing.stream_frame_headers(tus)
+        framing.stream_frame_headers(tus)  # the uncorrupted stream still parses end to end
