@@ -3,7 +3,7 @@
 Each test restates an assertion of the reference crate's `#[cfg(test)]`
 modules (src/loop_filter.rs, src/cdef.rs, src/superres.rs,
 src/loop_restoration.rs, src/film_grain.rs) against the oracle's C
-restatement, so the oracle that judges the CUDA kernels is itself checked
+restatement, so the oracle the CUDA kernels are compared with is itself checked
 against the reference's known answers.
 """
 import ctypes as C
