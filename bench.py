@@ -63,6 +63,22 @@ def frame_seed(rank, i):
     return 1_000_003 * (rank + 1) + i
 
 
+def max_over_ranks(ms, world, device):
+    """The slowest rank's time: each rank's own device-timed milliseconds,
+    all-reduced with MAX over the process group (one process per GPU)."""
+    import torch
+    t = torch.tensor([float(ms)], device=device, dtype=torch.float64)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, frames_per_rank, ms_per_step):
+    """Whole-job frames/s: every rank's frames over the slowest rank's step."""
+    return world * frames_per_rank / (ms_per_step / 1e3)
+
+
 def make_frames(rank, n, bit_depth):
     return [synth.make_frame(frame_seed(rank, i), WIDTH, HEIGHT, bit_depth=bit_depth) for i in range(n)]
 
@@ -283,12 +299,9 @@ def run_gpu(args):
             stage_ms[name] += d
             total_ms += d
             prev = ev_stage[k][i]
-    t = torch.tensor([total_ms], device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, world, dev)
     ms_per_step = total_ms / args.steps
-    value = world * n / (ms_per_step / 1e3)
+    value = job_rate(world, n, ms_per_step)
 
     # plain one-frame-per-launch path (same kernels, a launch per stage per frame)
     with torch.cuda.stream(stream):
@@ -300,9 +313,9 @@ def run_gpu(args):
             postfilter.run_postfilter(dframes, mode=abi.MODE_PER_FRAME, stream=stream, jobs=jobs)
         e1.record(stream)
     torch.cuda.synchronize()
-    per_frame_ms = e0.elapsed_time(e1) / args.steps
+    per_frame_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, dev)
 
-    graph = run_graphs(lib, jobs, n, stream, args.steps)
+    graph = run_graphs(lib, jobs, n, stream, args.steps, world, dev)
     e2e = run_e2e(args, frames, dframes, jobs, stream, dev, world)
     clk.__exit__(None, None, None)
     clocks = clk.summary()
@@ -341,7 +354,7 @@ def run_gpu(args):
                      "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                      if peak_kind == "measured" else "fallback 6650 GB/s", "issue": issue},
         "stages": stage_frac,
-        "per_frame_path": {"value": world * n / (per_frame_ms / 1e3), "unit": UNIT, "ms_per_step": per_frame_ms,
+        "per_frame_path": {"value": job_rate(world, n, per_frame_ms), "unit": UNIT, "ms_per_step": per_frame_ms,
                            "launches_per_step": None},
         "graph": graph,
         "autotune": autotune,
@@ -380,7 +393,7 @@ def run_autotune(lib, jobs, n, stream, hbd):
     return out
 
 
-def run_graphs(lib, jobs, n, stream, steps):
+def run_graphs(lib, jobs, n, stream, steps, world=1, dev=None):
     """The same chain (deblock, CDEF, LR) captured once as a CUDA graph
     (av1g_chain_graph_create) and replayed: batched (one launch per stage)
     and per-frame (a launch per stage per frame, all inside the graph)."""
@@ -402,8 +415,8 @@ def run_graphs(lib, jobs, n, stream, steps):
                     abi.check(lib.av1g_chain_graph_launch(g, sp))
                 e1.record(stream)
             torch.cuda.synchronize()
-            ms = e0.elapsed_time(e1) / steps
-            out[name] = {"value": n / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
+            ms = max_over_ranks(e0.elapsed_time(e1) / steps, world, dev)
+            out[name] = {"value": job_rate(world, n, ms), "unit": UNIT, "ms_per_step": ms,
                          "kernels_per_replay": lib.av1g_chain_graph_launches(g)}
         finally:
             abi.check(lib.av1g_chain_graph_destroy(g))
@@ -871,15 +884,10 @@ def run_e2e(args, frames, dframes, jobs, stream, dev, world, chunks=8, graphs=Tr
     stream.wait_stream(s_out)
     e1.record(stream)
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
-    t = torch.tensor([ms], device=dev)
-    if world > 1:
-        import torch.distributed as dist
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, dev)
     for gh in ggraph:
         abi.check(lib.av1g_chain_graph_destroy(gh))
-    return {"value": world * n / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+    return {"value": job_rate(world, n, ms), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
             "ms_per_step": ms,
             "path": f"{'av1g_chain_graph_launch (one captured chain per group)' if graphs else 'av1g_run_postfilter'}"
                     f" with pinned-host inputs/outputs copied every step, {len(groups)} groups of frames (one copy "
