@@ -36,7 +36,7 @@ namespace {
 constexpr int TW = 64, TH = 32, H3 = 3;
 constexpr int SW = TW + 2 * H3, SP = SW + 2;  // source window row pitch (u16)
 constexpr int SH = TH + 2 * H3;
-constexpr int VW = TW + 2 * H3;               // column-sum width
+constexpr int VW = TW + 2 * H3 + 1;           // column-sum row pitch (odd: rows fall on distinct banks)
 constexpr int AR = TH + 2, AP = TW + 2 + 1;   // A/B grid rows / pitch
 
 __constant__ int8_t c_sgr_params[16][4] = {
@@ -77,7 +77,8 @@ __device__ __forceinline__ int count_units(int us, int sz) {
 
 // Box sums, a/b coefficients (box_filter, loop_restoration.rs:594-700) for
 // radius r over the A/B grid rows i in [-1, th] (stored at i + 1), columns
-// j in [-1, tw].  odd_only: only rows whose plane row is odd.  Column sums
+// j in [-1, tw].  odd_only: only rows whose plane row is odd, whose column
+// sums are then stored compactly (grid row i + 1 at i + 1 >> 1).  Column sums
 // slide down the rows and row sums slide along the columns, so each sum
 // costs two loads instead of 2r + 1.
 __device__ void box_coeffs(Smem& s, int th, int tw, int bd, int r, int eps, bool odd_only, int y0) {
@@ -88,8 +89,9 @@ __device__ void box_coeffs(Smem& s, int th, int tw, int bd, int r, int eps, bool
     const int sa = 2 * (bd - 8), sb = bd - 8;
     const int vw = tw + 2 * H3;
     const int rows = th + 2;
-    // column sums: one thread per (column, run of 8 grid rows)
-    constexpr int RUN = 8;
+    // column sums: one thread per (column, run of 12 grid rows): 3 x 71
+    // items, one round of the 256 threads
+    constexpr int RUN = 12;
     const int runs = (rows + RUN - 1) / RUN;
     for (int k = threadIdx.x; k < runs * VW; k += blockDim.x) {
         const int ru = k / VW, jj = k - ru * VW;
@@ -105,8 +107,9 @@ __device__ void box_coeffs(Smem& s, int th, int tw, int bd, int r, int eps, bool
         }
         for (int row = ra;; row++) {
             if (!odd_only || ((y0 + row - 1) & 1)) {
-                s.v1[row * VW + jj] = s1;
-                s.v2[row * VW + jj] = s2;
+                const int cr = odd_only ? row >> 1 : row;
+                s.v1[cr * VW + jj] = s1;
+                s.v2[cr * VW + jj] = s2;
             }
             if (row + 1 >= rb) break;
             const int vo = c[top * SP], vn = c[(top + 2 * r + 1) * SP];
@@ -116,20 +119,25 @@ __device__ void box_coeffs(Smem& s, int th, int tw, int bd, int r, int eps, bool
         }
     }
     __syncthreads();
-    // row sums and coefficients: one thread per (grid row, run of 8 columns);
-    // with odd_only the work list holds only the odd-plane-row grid rows, so
-    // no lane of a warp idles on a skipped row
-    constexpr int SEGS = (TW + 2 + RUN - 1) / RUN;
+    // row sums and coefficients: one thread per (grid row, run of columns),
+    // consecutive threads on consecutive rows of one run, so their column-sum
+    // loads are an odd pitch apart (distinct banks); with odd_only the work
+    // list holds only the odd-plane-row grid rows, so no lane of a warp idles
+    // on a skipped row.  Runs of 11 columns (34 rows x 6) or, odd rows only,
+    // 5 columns (17 rows x 14): one round of the 256 threads either way.
+    const int crun = odd_only ? 5 : 11;
+    const int segs = (TW + 2 + crun - 1) / crun;
     const int first = odd_only ? ((y0 & 1) ? 1 : 0) : 0;  // grid row r holds plane row y0 + r - 1
     const int step = odd_only ? 2 : 1;
     const int nrows = (rows - first + step - 1) / step;
-    for (int k = threadIdx.x; k < nrows * SEGS; k += blockDim.x) {
-        const int rk = k / SEGS, sg = k - rk * SEGS;
+    for (int k = threadIdx.x; k < nrows * segs; k += blockDim.x) {
+        const int sg = k / nrows, rk = k - sg * nrows;
         const int row = first + rk * step;
-        const int ja = sg * RUN - 1, jb = min(tw + 1, ja + RUN);  // j in [ja, jb)
+        const int ja = sg * crun - 1, jb = min(tw + 1, ja + crun);  // j in [ja, jb)
         if (ja >= jb) continue;
-        const int* c1 = s.v1 + row * VW;
-        const int* c2 = s.v2 + row * VW;
+        const int cr = odd_only ? rk : row;  // rk == row >> 1 for the odd-only rows
+        const int* c1 = s.v1 + cr * VW;
+        const int* c2 = s.v2 + cr * VW;
         int left = ja + H3 - r;
         int b = 0, a = 0;
         for (int d = 0; d <= 2 * r; d++) {
