@@ -26,6 +26,7 @@ namespace av1g {
 namespace {
 
 constexpr int FB = 64, H2 = 2, WMAX = FB + 2 * H2, WP = WMAX + 4;
+constexpr int kCdefThreads = 256;  // cdef_kernel's CTA size
 constexpr int16_t NA = -32768;
 
 __constant__ int8_t c_cdef_dirs[8][2][2] = {
@@ -135,7 +136,7 @@ __device__ __forceinline__ int filter_px(const int16_t* c, int xv, const Taps& T
     return clip3(mn, mx, xv + ((8 + sum - (sum < 0)) >> 4));
 }
 
-__global__ void __launch_bounds__(256, 3) cdef_kernel(const FrameDev* __restrict__ frames,
+__global__ void __launch_bounds__(kCdefThreads, 3) cdef_kernel(const FrameDev* __restrict__ frames,
                                                       const int32_t* __restrict__ starts, int n, int total) {
     __shared__ __align__(16) int16_t win[3][WMAX * WP];
     __shared__ BlockParams bp[64];
@@ -170,25 +171,38 @@ __global__ void __launch_bounds__(256, 3) cdef_kernel(const FrameDev* __restrict
             if (x0 >= 4 && y0 >= H2 && x0 + bw + 4 <= S.w && y0 + bh + H2 <= S.h) {
                 // interior: aligned 4-sample loads over [x0 - 4, x0 + bw + 4),
                 // every one inside the plane
-                const int ng = (bw + 8) >> 2;
+                // every thread issues its (at most 5) loads before it unpacks
+                // any, so their latencies overlap
+                const int ng = (bw + 8) >> 2, items = wh * ng;
                 const unsigned mag = (1u << 16) / ng + 1;  // i / ng for i < 4096
+                constexpr int PER = (WMAX * ((FB + 8) >> 2) + kCdefThreads - 1) / kCdefThreads;
                 int16_t* wrow = win[p];
-                for (int i = threadIdx.x; i < wh * ng; i += blockDim.x) {
-                    int r = (int)(((unsigned)i * mag) >> 16), g = i - r * ng;
+                uint2 q[PER];
+#pragma unroll
+                for (int k = 0; k < PER; k++) {
+                    const int i = threadIdx.x + k * kCdefThreads;
+                    if (i >= items) break;
+                    const int r = (int)(((unsigned)i * mag) >> 16), g = i - r * ng;
                     const uint8_t* row = S.p + (size_t)(y0 - H2 + r) * S.stride;
+                    if (hbd) q[k] = *reinterpret_cast<const uint2*>(row + 2 * (x0 - 4 + 4 * g));
+                    else q[k].x = *reinterpret_cast<const uint32_t*>(row + x0 - 4 + 4 * g);
+                }
+#pragma unroll
+                for (int k = 0; k < PER; k++) {
+                    const int i = threadIdx.x + k * kCdefThreads;
+                    if (i >= items) break;
+                    const int r = (int)(((unsigned)i * mag) >> 16), g = i - r * ng;
                     int v[4];
                     if (hbd) {
-                        uint2 q = *reinterpret_cast<const uint2*>(row + 2 * (x0 - 4 + 4 * g));
-                        v[0] = q.x & 0xffff;
-                        v[1] = q.x >> 16;
-                        v[2] = q.y & 0xffff;
-                        v[3] = q.y >> 16;
+                        v[0] = q[k].x & 0xffff;
+                        v[1] = q[k].x >> 16;
+                        v[2] = q[k].y & 0xffff;
+                        v[3] = q[k].y >> 16;
                     } else {
-                        uint32_t q = *reinterpret_cast<const uint32_t*>(row + x0 - 4 + 4 * g);
-                        v[0] = q & 0xff;
-                        v[1] = (q >> 8) & 0xff;
-                        v[2] = (q >> 16) & 0xff;
-                        v[3] = q >> 24;
+                        v[0] = q[k].x & 0xff;
+                        v[1] = (q[k].x >> 8) & 0xff;
+                        v[2] = (q[k].x >> 16) & 0xff;
+                        v[3] = q[k].x >> 24;
                     }
 #pragma unroll
                     for (int e = 0; e < 4; e++) {
@@ -331,7 +345,7 @@ int tiles_cdef(const FrameDev& f) { return ((f.h.mi_rows + 15) >> 4) * ((f.h.mi_
 void launch_cdef(const FrameDev* frames, const int32_t* starts, int n, int total, const StageShape& sh,
                  cudaStream_t s) {
     if (total <= 0) return;
-    cdef_kernel<<<shape_grid(sh, total), 256, 0, s>>>(frames, starts, n, total);
+    cdef_kernel<<<shape_grid(sh, total), kCdefThreads, 0, s>>>(frames, starts, n, total);
 }
 
 }  // namespace av1g

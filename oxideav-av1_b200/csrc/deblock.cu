@@ -32,6 +32,8 @@ __constant__ AV1T_TX_HEIGHT_TYPE c_txh AV1T_TX_HEIGHT_DIMS = AV1T_TX_HEIGHT_INIT
 namespace {
 
 constexpr int TILE = 64, HALO = 16, WIN = TILE + 2 * HALO, PITCH = WIN + 1, CELLS = WIN / 4;
+constexpr int kDbThreads = 256;  // deblock_kernel's CTA size
+static_assert(WIN * (WIN / 4) % kDbThreads == 0, "window groups split evenly over the CTA");
 constexpr int BLOCK_SIZES = 22, BLOCK_INVALID = 22;
 
 struct Grid {
@@ -232,7 +234,7 @@ __device__ void filter_line(int* b, int st, uint32_t prm, int plane, int bd) {
     }
 }
 
-__global__ void __launch_bounds__(256) deblock_kernel(const FrameDev* __restrict__ frames,
+__global__ void __launch_bounds__(kDbThreads, 5) deblock_kernel(const FrameDev* __restrict__ frames,
                                                       const int32_t* __restrict__ starts, int n, int total) {
     __shared__ int win[WIN * PITCH];
     __shared__ uint32_t ev[CELLS * CELLS], eh[CELLS * CELLS];
@@ -254,7 +256,41 @@ __global__ void __launch_bounds__(256) deblock_kernel(const FrameDev* __restrict
         const int gx0 = tx * TILE - HALO, gy0 = ty * TILE - HALO;
         __syncthreads();  // previous tile done with shared memory
         // window: 4 consecutive samples per thread, one vector load when the
-        // group lies inside the plane (rows are 4-sample aligned: gx0 % 4 == 0)
+        // group lies inside the plane (rows are 4-sample aligned: gx0 % 4 == 0).
+        // A window inside the plane horizontally (almost every tile) issues
+        // all of a thread's loads before it unpacks any, so their latencies
+        // overlap instead of adding up.
+        if (gx0 >= 0 && gx0 + WIN <= S.w) {
+            constexpr int G = WIN / 4, PER = WIN * G / kDbThreads;
+            const uint8_t* base = S.p + (size_t)(hbd ? 2 : 1) * gx0;
+            if (hbd) {
+                uint2 v[PER];
+#pragma unroll
+                for (int q = 0; q < PER; q++) {
+                    const int i = threadIdx.x + q * kDbThreads, r = i / G, c = (i - r * G) * 4;
+                    v[q] = *reinterpret_cast<const uint2*>(base + (size_t)clip3(0, S.h - 1, gy0 + r) * S.stride + 2 * c);
+                }
+#pragma unroll
+                for (int q = 0; q < PER; q++) {
+                    const int i = threadIdx.x + q * kDbThreads, r = i / G, c = (i - r * G) * 4;
+                    int* w = &win[r * PITCH + c];
+                    w[0] = v[q].x & 0xffff; w[1] = v[q].x >> 16; w[2] = v[q].y & 0xffff; w[3] = v[q].y >> 16;
+                }
+            } else {
+                uint32_t v[PER];
+#pragma unroll
+                for (int q = 0; q < PER; q++) {
+                    const int i = threadIdx.x + q * kDbThreads, r = i / G, c = (i - r * G) * 4;
+                    v[q] = *reinterpret_cast<const uint32_t*>(base + (size_t)clip3(0, S.h - 1, gy0 + r) * S.stride + c);
+                }
+#pragma unroll
+                for (int q = 0; q < PER; q++) {
+                    const int i = threadIdx.x + q * kDbThreads, r = i / G, c = (i - r * G) * 4;
+                    int* w = &win[r * PITCH + c];
+                    w[0] = v[q] & 0xff; w[1] = (v[q] >> 8) & 0xff; w[2] = (v[q] >> 16) & 0xff; w[3] = v[q] >> 24;
+                }
+            }
+        } else
         for (int i = threadIdx.x; i < WIN * (WIN / 4); i += blockDim.x) {
             int r = i / (WIN / 4), c = (i % (WIN / 4)) * 4;
             int gy = clip3(0, S.h - 1, gy0 + r), gx = gx0 + c;
@@ -276,12 +312,23 @@ __global__ void __launch_bounds__(256) deblock_kernel(const FrameDev* __restrict
         const int cy0 = gy0 / 4, cx0 = gx0 / 4;  // gx0,gy0 are multiples of 4 (may be negative)
         const int cw = S.w >> 2, ch = S.h >> 2, sharp = F.h.lf_sharpness;
         const uint16_t* codes = F.lf_codes[plane];
-        for (int i = threadIdx.x; i < CELLS * CELLS; i += blockDim.x) {
-            int cr = i / CELLS, cc = i % CELLS;
-            int cy = cy0 + cr, cx = cx0 + cc;
-            uint32_t code = (cy >= 0 && cx >= 0 && cy < ch && cx < cw) ? codes[cy * cw + cx] : 0;
-            ev[i] = decode_code(code & 0xff, sharp);
-            eh[i] = decode_code(code >> 8, sharp);
+        {
+            // the edge codes: a thread's (at most 3) loads first, then the decodes
+            constexpr int PER = (CELLS * CELLS + kDbThreads - 1) / kDbThreads;
+            uint32_t code[PER];
+#pragma unroll
+            for (int q = 0; q < PER; q++) {
+                const int i = threadIdx.x + q * kDbThreads, cr = i / CELLS, cc = i - cr * CELLS;
+                const int cy = cy0 + cr, cx = cx0 + cc;
+                code[q] = (i < CELLS * CELLS && cy >= 0 && cx >= 0 && cy < ch && cx < cw) ? codes[cy * cw + cx] : 0;
+            }
+#pragma unroll
+            for (int q = 0; q < PER; q++) {
+                const int i = threadIdx.x + q * kDbThreads;
+                if (i >= CELLS * CELLS) break;
+                ev[i] = decode_code(code[q] & 0xff, sharp);
+                eh[i] = decode_code(code[q] >> 8, sharp);
+            }
         }
         __syncthreads();
         // vertical pass: window rows x edge columns 12..84 (cells 3..21: a
@@ -346,7 +393,7 @@ void launch_deblock(const FrameDev* frames, const int32_t* starts, int n, int to
                     const StageShape& sh, cudaStream_t s) {
     if (total <= 0) return;
     lf_prep_kernel<<<dim3((max_cells + 255) / 256, n), 256, 0, s>>>(frames);
-    deblock_kernel<<<shape_grid(sh, total), 256, 0, s>>>(frames, starts, n, total);
+    deblock_kernel<<<shape_grid(sh, total), kDbThreads, 0, s>>>(frames, starts, n, total);
 }
 
 }  // namespace av1g

@@ -34,6 +34,7 @@ namespace av1g {
 namespace {
 
 constexpr int TW = 64, TH = 32, H3 = 3;
+constexpr int kLrThreads = 256;  // lr_kernel's CTA size
 constexpr int SW = TW + 2 * H3, SP = SW + 2;  // source window row pitch (u16)
 constexpr int SH = TH + 2 * H3;
 constexpr int VW = TW + 2 * H3 + 1;           // column-sum row pitch (odd: rows fall on distinct banks)
@@ -222,7 +223,7 @@ __device__ __forceinline__ void box_weight4(const Smem& s, int i, int j0, const 
     }
 }
 
-__global__ void __launch_bounds__(256) lr_kernel(const FrameDev* __restrict__ frames,
+__global__ void __launch_bounds__(kLrThreads) lr_kernel(const FrameDev* __restrict__ frames,
                                                  const int32_t* __restrict__ starts, int n, int total) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem& s = *reinterpret_cast<Smem*>(smem_raw);
@@ -284,9 +285,16 @@ __global__ void __launch_bounds__(256) lr_kernel(const FrameDev* __restrict__ fr
             // columns [x0 - 4, x0 + tw + 4) lie inside the plane (and inside
             // both source planes, which are at least pw wide): aligned
             // 4-sample loads, the row routed once per load
-            const int ng = (tw + 8) >> 2;
+            // every thread issues its (at most 3) loads before it unpacks
+            // any, so their latencies overlap
+            const int ng = (tw + 8) >> 2, items = (th + 2 * H3) * ng;
             const unsigned mag = (1u << 16) / ng + 1;  // k / ng for k < 38 * ng
-            for (int k = threadIdx.x; k < (th + 2 * H3) * ng; k += blockDim.x) {
+            constexpr int PER = (SH * ((TW + 8) >> 2) + kLrThreads - 1) / kLrThreads;
+            uint2 q[PER];
+#pragma unroll
+            for (int e = 0; e < PER; e++) {
+                const int k = threadIdx.x + e * kLrThreads;
+                if (k >= items) break;
                 const int i = (int)(((unsigned)k * mag) >> 16), g = k - i * ng;
                 const int y = clip3(0, ph - 1, y0 - H3 + i);
                 const PlaneDev* P;
@@ -303,24 +311,30 @@ __global__ void __launch_bounds__(256) lr_kernel(const FrameDev* __restrict__ fr
                 }
                 const uint8_t* row = P->p + (size_t)yy * P->stride;
                 const int xs = x0 - 4 + 4 * g;
+                if (hbd) q[e] = *reinterpret_cast<const uint2*>(row + 2 * xs);
+                else q[e].x = *reinterpret_cast<const uint32_t*>(row + xs);
+            }
+#pragma unroll
+            for (int e = 0; e < PER; e++) {
+                const int k = threadIdx.x + e * kLrThreads;
+                if (k >= items) break;
+                const int i = (int)(((unsigned)k * mag) >> 16), g = k - i * ng;
                 int v[4];
                 if (hbd) {
-                    uint2 q = *reinterpret_cast<const uint2*>(row + 2 * xs);
-                    v[0] = q.x & 0xffff;
-                    v[1] = q.x >> 16;
-                    v[2] = q.y & 0xffff;
-                    v[3] = q.y >> 16;
+                    v[0] = q[e].x & 0xffff;
+                    v[1] = q[e].x >> 16;
+                    v[2] = q[e].y & 0xffff;
+                    v[3] = q[e].y >> 16;
                 } else {
-                    uint32_t q = *reinterpret_cast<const uint32_t*>(row + xs);
-                    v[0] = q & 0xff;
-                    v[1] = (q >> 8) & 0xff;
-                    v[2] = (q >> 16) & 0xff;
-                    v[3] = q >> 24;
+                    v[0] = q[e].x & 0xff;
+                    v[1] = (q[e].x >> 8) & 0xff;
+                    v[2] = (q[e].x >> 16) & 0xff;
+                    v[3] = q[e].x >> 24;
                 }
 #pragma unroll
-                for (int e = 0; e < 4; e++) {
-                    const int j = 4 * g + e - 1;
-                    if (j >= 0 && j < sw) s.src[i * SP + j] = (uint16_t)v[e];
+                for (int t = 0; t < 4; t++) {
+                    const int j = 4 * g + t - 1;
+                    if (j >= 0 && j < sw) s.src[i * SP + j] = (uint16_t)v[t];
                 }
             }
         } else {
@@ -451,7 +465,7 @@ void launch_lr(const FrameDev* frames, const int32_t* starts, int n, int total, 
     if (total <= 0) return;
     size_t bytes = lr_smem_bytes();
     cudaFuncSetAttribute(lr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    lr_kernel<<<shape_grid(sh, total), 256, bytes, s>>>(frames, starts, n, total);
+    lr_kernel<<<shape_grid(sh, total), kLrThreads, bytes, s>>>(frames, starts, n, total);
 }
 
 }  // namespace av1g
