@@ -145,6 +145,7 @@ __global__ void __launch_bounds__(kCdefThreads, 3) cdef_kernel(const FrameDev* _
     // that 32 lanes reading 8 bytes each from 32 blocks hit distinct banks
     __shared__ __align__(16) int16_t blkx[64][68];
     __shared__ int16_t toff[16];
+    __shared__ int8_t blive[64];  // 8x8 luma block filtered (inside the mi grid, not all skip)
     if (threadIdx.x < 16) toff[threadIdx.x] = c_cdef_dirs[threadIdx.x >> 1][threadIdx.x & 1][0] * WP +
                                               c_cdef_dirs[threadIdx.x >> 1][threadIdx.x & 1][1];
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
@@ -221,6 +222,23 @@ __global__ void __launch_bounds__(kCdefThreads, 3) cdef_kernel(const FrameDev* _
             }
         }
         __syncthreads();
+        // which 8x8 blocks are filtered (cdef_block's skip test, cdef.rs:229-262):
+        // the four mi skip flags loaded together, out-of-grid ones read as skip
+        if (threadIdx.x < 64) {
+            const int blk = threadIdx.x, r = fbr * 16 + (blk >> 3) * 2, c = fbc * 16 + (blk & 7) * 2;
+            bool live = idx >= 0 && r < h.mi_rows && c < h.mi_cols;
+            if (live) {
+                const uint8_t* sk = F.g.skip;
+                const int mc = h.mi_cols;
+                const bool rn = r + 1 < h.mi_rows, cn = c + 1 < mc;
+                const int s00 = sk[r * mc + c];
+                const int s10 = rn ? sk[(r + 1) * mc + c] : 1;
+                const int s01 = cn ? sk[r * mc + c + 1] : 1;
+                const int s11 = rn && cn ? sk[(r + 1) * mc + c + 1] : 1;
+                live = !(s00 && s10 && s01 && s11);
+            }
+            blive[blk] = live;
+        }
         // block-major centred luma for the direction search (only blocks
         // inside the mi grid are searched, and those lie inside the plane)
         for (int k = threadIdx.x; k < 64 * 64; k += blockDim.x) {
@@ -234,19 +252,8 @@ __global__ void __launch_bounds__(kCdefThreads, 3) cdef_kernel(const FrameDev* _
         // and one thread per block takes the arg-max
         for (int q = threadIdx.x; q < 64 * 8; q += blockDim.x) {
             const int d = (q >> 5) & 7, blk = (q >> 8) * 32 + (q & 31);
-            const int bi = blk >> 3, bj = blk & 7;
-            const int r = fbr * 16 + bi * 2, c = fbc * 16 + bj * 2;
-            bool live = idx >= 0 && r < h.mi_rows && c < h.mi_cols;
-            if (live) {
-                const uint8_t* sk = F.g.skip;
-                int mc = h.mi_cols;
-                bool skip = sk[r * mc + c] && (r + 1 >= h.mi_rows || sk[(r + 1) * mc + c]) &&
-                            (c + 1 >= mc || sk[r * mc + c + 1]) &&
-                            (r + 1 >= h.mi_rows || c + 1 >= mc || sk[(r + 1) * mc + c + 1]);
-                live = !skip;
-            }
             int cost = -1;  // marks a block that is not filtered
-            if (live) {
+            if (blive[blk]) {
                 const int16_t* w = blkx[blk];
                 switch (d) {
                     case 0: cost = dir_cost<0>(w); break;
