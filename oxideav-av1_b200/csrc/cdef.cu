@@ -90,9 +90,10 @@ __device__ __forceinline__ int dir_cost(const int16_t* blk) {
 }
 
 __device__ __forceinline__ int constrain_adj(int diff, int threshold, int adj) {
-    // constrain (cdef.rs:592-606) with dampingAdj precomputed
+    // constrain (cdef.rs:592-606) with dampingAdj precomputed:
+    // min(|d|, max(t - (|d| >> adj), 0)) == max(min(|d|, t - (|d| >> adj)), 0) as |d| >= 0
     int ad = abs(diff);
-    int v = min(ad, max(threshold - (ad >> adj), 0));
+    int v = __vimin_s32_relu(ad, threshold - (ad >> adj));
     return diff < 0 ? -v : v;
 }
 
@@ -113,10 +114,17 @@ __device__ __forceinline__ Taps taps_of(const int16_t* toff, int dir) {
 template <bool BORDER>
 __device__ __forceinline__ void tap2(const int16_t* c, int o, int xv, int w, int thr, int adj, int& sum, int& mn,
                                      int& mx) {
+    if (!BORDER) {  // both taps available: one weight product, three-input min / max
+        const int x0 = c[o], x1 = c[-o];
+        sum += w * (constrain_adj(x0 - xv, thr, adj) + constrain_adj(x1 - xv, thr, adj));
+        mx = __vimax3_s32(mx, x0, x1);
+        mn = __vimin3_s32(mn, x0, x1);
+        return;
+    }
 #pragma unroll
     for (int s = 0; s < 2; s++) {
         const int x = s ? c[-o] : c[o];
-        if (BORDER && x == NA) continue;
+        if (x == NA) continue;
         sum += w * constrain_adj(x - xv, thr, adj);
         mx = max(mx, x);
         mn = min(mn, x);

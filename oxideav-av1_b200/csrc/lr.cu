@@ -77,16 +77,20 @@ __device__ __forceinline__ int count_units(int us, int sz) {
 }
 
 // Box sums, a/b coefficients (box_filter, loop_restoration.rs:594-700) for
-// radius r over the A/B grid rows i in [-1, th] (stored at i + 1), columns
-// j in [-1, tw].  odd_only: only rows whose plane row is odd, whose column
-// sums are then stored compactly (grid row i + 1 at i + 1 >> 1).  Column sums
-// slide down the rows and row sums slide along the columns, so each sum
-// costs two loads instead of 2r + 1.
-__device__ void box_coeffs(Smem& s, int th, int tw, int bd, int r, int eps, bool odd_only, int y0) {
-    const int n = (2 * r + 1) * (2 * r + 1);
+// radius R over the A/B grid rows i in [-1, th] (stored at i + 1), columns
+// j in [-1, tw].  The self-guided sets use R = 2 only for the first pass,
+// which needs only the rows whose plane row is odd; their column sums are
+// stored compactly (grid row i + 1 at i + 1 >> 1).  Column sums slide down
+// the rows and row sums slide along the columns, so each sum costs two loads
+// instead of 2R + 1; the runs have fixed lengths so the loops unroll and the
+// coefficient arithmetic of neighbouring positions overlaps.
+template <int R>
+__device__ void box_coeffs(Smem& s, int th, int tw, int bd, int eps, int y0) {
+    constexpr bool ODD = R == 2;
+    constexpr int n = (2 * R + 1) * (2 * R + 1);
     const long long n2e = (long long)n * n * eps;
     const unsigned sm = (unsigned)(((1LL << 20) + n2e / 2) / n2e);
-    const int one_over_n = ((1 << 12) + n / 2) / n;
+    constexpr int one_over_n = ((1 << 12) + n / 2) / n;
     const int sa = 2 * (bd - 8), sb = bd - 8;
     const int vw = tw + 2 * H3;
     const int rows = th + 2;
@@ -97,55 +101,60 @@ __device__ void box_coeffs(Smem& s, int th, int tw, int bd, int r, int eps, bool
     for (int k = threadIdx.x; k < runs * VW; k += blockDim.x) {
         const int ru = k / VW, jj = k - ru * VW;
         if (jj >= vw) continue;
-        const int ra = ru * RUN, rb = min(rows, ra + RUN);
-        const uint16_t* c = s.src + jj;
-        int top = ra - 1 + H3 - r;  // first source row of grid row ra's window
+        const int ra = ru * RUN;
+        const uint16_t* c = s.src + jj + (ra - 1 + H3 - R) * SP;  // first source row of grid row ra's window
         int s1 = 0, s2 = 0;
-        for (int d = 0; d <= 2 * r; d++) {
-            int v = c[(top + d) * SP];
+#pragma unroll
+        for (int d = 0; d <= 2 * R; d++) {
+            const int v = c[d * SP];
             s1 += v;
             s2 += v * v;
         }
-        for (int row = ra;; row++) {
-            if (!odd_only || ((y0 + row - 1) & 1)) {
-                const int cr = odd_only ? row >> 1 : row;
+#pragma unroll
+        for (int t = 0; t < RUN; t++) {
+            const int row = ra + t;
+            if (row >= rows) break;
+            if (!ODD || ((y0 + row - 1) & 1)) {
+                const int cr = ODD ? row >> 1 : row;
                 s.v1[cr * VW + jj] = s1;
                 s.v2[cr * VW + jj] = s2;
             }
-            if (row + 1 >= rb) break;
-            const int vo = c[top * SP], vn = c[(top + 2 * r + 1) * SP];
+            const int vo = c[t * SP], vn = c[(t + 2 * R + 1) * SP];
             s1 += vn - vo;
             s2 += vn * vn - vo * vo;
-            top++;
         }
     }
     __syncthreads();
     // row sums and coefficients: one thread per (grid row, run of columns),
     // consecutive threads on consecutive rows of one run, so their column-sum
-    // loads are an odd pitch apart (distinct banks); with odd_only the work
-    // list holds only the odd-plane-row grid rows, so no lane of a warp idles
-    // on a skipped row.  Runs of 11 columns (34 rows x 6) or, odd rows only,
-    // 5 columns (17 rows x 14): one round of the 256 threads either way.
-    const int crun = odd_only ? 5 : 11;
-    const int segs = (TW + 2 + crun - 1) / crun;
-    const int first = odd_only ? ((y0 & 1) ? 1 : 0) : 0;  // grid row r holds plane row y0 + r - 1
-    const int step = odd_only ? 2 : 1;
-    const int nrows = (rows - first + step - 1) / step;
-    for (int k = threadIdx.x; k < nrows * segs; k += blockDim.x) {
+    // loads are an odd pitch apart (distinct banks); with ODD the work list
+    // holds only the odd-plane-row grid rows, so no lane of a warp idles on a
+    // skipped row.  Runs of 11 columns (34 rows x 6) or, odd rows only, 5
+    // columns (17 rows x 14): one round of the 256 threads either way.
+    constexpr int CRUN = ODD ? 5 : 11;
+    constexpr int SEGS = (TW + 2 + CRUN - 1) / CRUN;
+    const int first = ODD ? ((y0 & 1) ? 1 : 0) : 0;  // grid row r holds plane row y0 + r - 1
+    constexpr int STEP = ODD ? 2 : 1;
+    const int nrows = (rows - first + STEP - 1) / STEP;
+    for (int k = threadIdx.x; k < nrows * SEGS; k += blockDim.x) {
         const int sg = k / nrows, rk = k - sg * nrows;
-        const int row = first + rk * step;
-        const int ja = sg * crun - 1, jb = min(tw + 1, ja + crun);  // j in [ja, jb)
+        const int row = first + rk * STEP;
+        const int ja = sg * CRUN - 1, jb = min(tw + 1, ja + CRUN);  // j in [ja, jb)
         if (ja >= jb) continue;
-        const int cr = odd_only ? rk : row;  // rk == row >> 1 for the odd-only rows
-        const int* c1 = s.v1 + cr * VW;
-        const int* c2 = s.v2 + cr * VW;
-        int left = ja + H3 - r;
+        const int cr = ODD ? rk : row;  // rk == row >> 1 for the odd-only rows
+        const int* c1 = s.v1 + cr * VW + ja + H3 - R;
+        const int* c2 = s.v2 + cr * VW + ja + H3 - R;
         int b = 0, a = 0;
-        for (int d = 0; d <= 2 * r; d++) {
-            b += c1[left + d];
-            a += c2[left + d];
+#pragma unroll
+        for (int d = 0; d <= 2 * R; d++) {
+            b += c1[d];
+            a += c2[d];
         }
-        for (int j = ja;; j++) {
+        uint16_t* ao = s.A + row * AP + ja + 1;
+        int* bo = s.B + row * AP + ja + 1;
+#pragma unroll
+        for (int t = 0; t < CRUN; t++) {
+            if (ja + t >= jb) break;
             int ar = sa ? (a + (1 << (sa - 1))) >> sa : a;
             int dr = sb ? (b + (1 << (sb - 1))) >> sb : b;
             int p = ar * n - dr * dr;
@@ -154,12 +163,10 @@ __device__ void box_coeffs(Smem& s, int th, int tw, int bd, int r, int eps, bool
             int a2 = z >= 255 ? 256 : s.a2lut[z];
             // b2 uses the raw box sum b, as the reference does (loop_restoration.rs:660-661)
             long long b2 = (long long)((256 - a2) * b) * one_over_n;
-            s.A[row * AP + j + 1] = (uint16_t)a2;
-            s.B[row * AP + j + 1] = (int)((b2 + (1 << 11)) >> 12);
-            if (j + 1 >= jb) break;
-            b += c1[left + 2 * r + 1] - c1[left];
-            a += c2[left + 2 * r + 1] - c2[left];
-            left++;
+            ao[t] = (uint16_t)a2;
+            bo[t] = (int)((b2 + (1 << 11)) >> 12);
+            b += c1[t + 2 * R + 1] - c1[t];
+            a += c2[t + 2 * R + 1] - c2[t];
         }
     }
     __syncthreads();
@@ -391,7 +398,7 @@ __global__ void __launch_bounds__(kLrThreads) lr_kernel(const FrameDev* __restri
         // outputs in runs of four along a row
         constexpr int Q = TW / 4;
         if (r0) {
-            box_coeffs(s, th, tw, bd, r0, e0, true, y0);
+            box_coeffs<2>(s, th, tw, bd, e0, y0);  // r0 is 2 in every set that has it
             // rows of one parity run together (the odd-row and even-row
             // weightings differ), so a warp's two rows share a code path
             const int n_odd = (th + ((y0 & 1) ? 1 : 0)) >> 1;      // rows i with (y0 + i) odd
@@ -409,7 +416,7 @@ __global__ void __launch_bounds__(kLrThreads) lr_kernel(const FrameDev* __restri
             }
             __syncthreads();
         }
-        if (r1) box_coeffs(s, th, tw, bd, r1, e1, false, y0);
+        if (r1) box_coeffs<1>(s, th, tw, bd, e1, y0);  // r1 is 1 in every set that has it
         for (int k = threadIdx.x; k < th * Q; k += blockDim.x) {
             int i = k / Q, j0 = (k - i * Q) * 4;
             if (j0 >= tw) continue;
