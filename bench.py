@@ -688,7 +688,9 @@ def run_serving(args, local):
     out = {"streams": n_streams, "frames": sum(len(templates[t]) for t in mix),
            "stream_shapes": [f"{w}x{h} {bd}-bit 4:2:0, {f} frames" for (w, h, bd, f) in SERVE_SHAPES],
            "stream_weights": SERVE_WEIGHTS, "timing": "host wall clock, first submit to last completion; 8 client threads, each owning a group of "
-                     "streams (submit, then poll and fetch)"}
+                     "streams (submit, then poll and fetch)",
+           # the engine's host work (descriptor validation, planning, uploads) runs on these
+           "host_cpus": len(os.sched_getaffinity(0)), "host_load_avg_1min": os.getloadavg()[0]}
     consistent = True
     for name, mb, lanes in [("batched", 64, args.serve_lanes), ("per_frame", 1, 1)]:
         eng = engine.Engine(device=local, max_batch=mb, lanes=lanes)

@@ -189,26 +189,30 @@ __device__ void filter_line(int* b, int st, uint32_t prm, int plane, int bd) {
     int bds = bd - 8;
     int q0 = b[0], q1 = b[st], q2 = b[2 * st], q3 = b[3 * st];
     int p0 = b[-st], p1 = b[-2 * st], p2 = b[-3 * st], p3 = b[-4 * st];
+    // every test below is "some |difference| > bound": the largest
+    // difference against the bound, the shared ones computed once
+    const int d1 = max(abs(p1 - p0), abs(q1 - q0));
     int thr = thresh << bds;
-    bool hev = abs(p1 - p0) > thr || abs(q1 - q0) > thr;
+    bool hev = d1 > thr;
     int flen = fs == 4 ? 4 : (plane ? 6 : (fs == 8 ? 8 : 16));
     int lim = limit << bds, blim = blimit << bds;
-    bool mask = abs(p1 - p0) > lim || abs(q1 - q0) > lim || abs(p0 - q0) * 2 + abs(p1 - q1) / 2 > blim;
-    if (flen >= 6) mask |= abs(p2 - p1) > lim || abs(q2 - q1) > lim;
-    if (flen >= 8) mask |= abs(p3 - p2) > lim || abs(q3 - q2) > lim;
-    if (mask) return;
+    int dl = d1;
+    if (flen >= 6) dl = __vimax3_s32(dl, abs(p2 - p1), abs(q2 - q1));
+    if (flen >= 8) dl = __vimax3_s32(dl, abs(p3 - p2), abs(q3 - q2));
+    if (dl > lim || abs(p0 - q0) * 2 + abs(p1 - q1) / 2 > blim) return;
     int one = 1 << bds;
     bool flat = false, flat2 = false;
     if (fs >= 8) {
-        bool m = abs(p1 - p0) > one || abs(q1 - q0) > one || abs(p2 - p0) > one || abs(q2 - q0) > one;
-        if (flen >= 8) m |= abs(p3 - p0) > one || abs(q3 - q0) > one;
-        flat = !m;
+        int df = __vimax3_s32(d1, abs(p2 - p0), abs(q2 - q0));
+        if (flen >= 8) df = __vimax3_s32(df, abs(p3 - p0), abs(q3 - q0));
+        flat = df <= one;
     }
     if (fs >= 16 && flat) {
         int q4 = b[4 * st], q5 = b[5 * st], q6 = b[6 * st];
         int p4 = b[-5 * st], p5 = b[-6 * st], p6 = b[-7 * st];
-        flat2 = !(abs(p6 - p0) > one || abs(q6 - q0) > one || abs(p5 - p0) > one || abs(q5 - q0) > one ||
-                  abs(p4 - p0) > one || abs(q4 - q0) > one);
+        const int d2 = __vimax3_s32(__vimax3_s32(abs(p6 - p0), abs(q6 - q0), abs(p5 - p0)),
+                                    __vimax3_s32(abs(q5 - q0), abs(p4 - p0), abs(q4 - q0)), 0);
+        flat2 = d2 <= one;
     }
     if (fs == 4 || !flat) {
         int half = 0x80 << bds;
