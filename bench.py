@@ -889,8 +889,37 @@ def run_e2e(args, frames, dframes, jobs, stream, dev, world, chunks=8, graphs=Tr
     ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, dev)
     for gh in ggraph:
         abi.check(lib.av1g_chain_graph_destroy(gh))
+
+    def copies_ms(h2d_on, d2h_on, reps=3):
+        """The step's copies alone, on the same pinned buffers and streams:
+        the PCIe floor the end-to-end step can approach."""
+        torch.cuda.synchronize()
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        s_in.wait_event(c0)
+        s_out.wait_event(c0)
+        for _ in range(reps):
+            for gi in range(len(groups)):
+                if h2d_on:
+                    with torch.cuda.stream(s_in):
+                        d_in[gi].copy_(h_in[gi], non_blocking=True)
+                if d2h_on:
+                    with torch.cuda.stream(s_out):
+                        h_out[gi].copy_(d_out[gi], non_blocking=True)
+        stream.wait_stream(s_in)
+        stream.wait_stream(s_out)
+        c1.record(stream)
+        torch.cuda.synchronize()
+        return c0.elapsed_time(c1) / reps
+
+    t_in, t_out, t_both = copies_ms(True, False), copies_ms(False, True), copies_ms(True, True)
+    pcie = {"h2d_gbs": h2d / t_in / 1e6, "d2h_gbs": d2h / t_out / 1e6, "both_ms_per_step": t_both,
+            "floor_ms_per_step": max(t_in, t_out, t_both),
+            "e2e_frac_of_floor": max(t_in, t_out, t_both) / ms,
+            "note": "the step's pinned copies alone (same buffers and streams, no kernels): h2d and d2h each "
+                    "alone, then both at once; floor = the slowest of the three"}
     return {"value": job_rate(world, n, ms), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-            "ms_per_step": ms,
+            "ms_per_step": ms, "pcie": pcie,
             "path": f"{'av1g_chain_graph_launch (one captured chain per group)' if graphs else 'av1g_run_postfilter'}"
                     f" with pinned-host inputs/outputs copied every step, {len(groups)} groups of frames (one copy "
                     f"in and one copy out per group) pipelined over copy-in / compute / copy-out streams"}

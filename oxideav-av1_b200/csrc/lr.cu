@@ -371,22 +371,58 @@ __global__ void __launch_bounds__(kLrThreads) lr_kernel(const FrameDev* __restri
             const int rr0 = bd == 12 ? 5 : 3, rr1 = bd == 12 ? 9 : 11;
             const int off = 1 << (bd + 7 - rr0 - 1);
             const int lim = (1 << (bd + 1 + 7 - rr0)) - 1;
+            // four adjacent outputs per thread in both passes: the source
+            // samples and intermediate rows they share are loaded once, as
+            // vectors (source and intermediate rows start on 16-byte
+            // boundaries; columns past tw are computed and not stored)
             int* inter = s.v1;  // (th + 6) x TW
-            for (int k = threadIdx.x; k < (th + 6) * TW; k += blockDim.x) {
-                int i = k >> 6, j = k & (TW - 1);
-                if (j >= tw) continue;
-                const uint16_t* w = s.src + i * SP + j;
-                int acc = hf[3] * w[3] + hf[0] * (w[0] + w[6]) + hf[1] * (w[1] + w[5]) + hf[2] * (w[2] + w[4]);
-                inter[i * TW + j] = clip3(-off, lim - off, (acc + (1 << (rr0 - 1))) >> rr0);
+            constexpr int Q4 = TW / 4;
+            for (int k = threadIdx.x; k < (th + 6) * Q4; k += blockDim.x) {
+                const int i = k / Q4, j0 = (k - i * Q4) * 4;
+                if (j0 >= tw) continue;
+                const uint2* w2 = reinterpret_cast<const uint2*>(s.src + i * SP + j0);
+                int w[12];
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    const uint2 v = w2[q];
+                    w[4 * q] = v.x & 0xffff;
+                    w[4 * q + 1] = v.x >> 16;
+                    w[4 * q + 2] = v.y & 0xffff;
+                    w[4 * q + 3] = v.y >> 16;
+                }
+                int o[4];
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const int acc = hf[3] * w[e + 3] + hf[0] * (w[e] + w[e + 6]) + hf[1] * (w[e + 1] + w[e + 5]) +
+                                    hf[2] * (w[e + 2] + w[e + 4]);
+                    o[e] = clip3(-off, lim - off, (acc + (1 << (rr0 - 1))) >> rr0);
+                }
+                *reinterpret_cast<int4*>(inter + i * TW + j0) = make_int4(o[0], o[1], o[2], o[3]);
             }
             __syncthreads();
-            for (int k = threadIdx.x; k < th * TW; k += blockDim.x) {
-                int i = k >> 6, j = k & (TW - 1);
-                if (j >= tw) continue;
-                const int* c = inter + i * TW + j;
-                int acc = vf[3] * c[3 * TW] + vf[0] * (c[0] + c[6 * TW]) + vf[1] * (c[TW] + c[5 * TW]) +
-                          vf[2] * (c[2 * TW] + c[4 * TW]);
-                st_px(O, hbd, y0 + i, x0 + j, clip3(0, maxv, (acc + (1 << (rr1 - 1))) >> rr1));
+            for (int k = threadIdx.x; k < th * Q4; k += blockDim.x) {
+                const int i = k / Q4, j0 = (k - i * Q4) * 4;
+                if (j0 >= tw) continue;
+                int4 r[7];
+#pragma unroll
+                for (int d = 0; d < 7; d++) r[d] = *reinterpret_cast<const int4*>(inter + (i + d) * TW + j0);
+                int o[4];
+#define LR_VTAP(F) (vf[3] * r[3].F + vf[0] * (r[0].F + r[6].F) + vf[1] * (r[1].F + r[5].F) + vf[2] * (r[2].F + r[4].F))
+                const int acc[4] = {LR_VTAP(x), LR_VTAP(y), LR_VTAP(z), LR_VTAP(w)};
+#undef LR_VTAP
+#pragma unroll
+                for (int e = 0; e < 4; e++) o[e] = clip3(0, maxv, (acc[e] + (1 << (rr1 - 1))) >> rr1);
+                if (j0 + 4 <= tw && !((x0 + j0) & 3)) {  // one aligned vector store
+                    uint8_t* row = O.p + (size_t)(y0 + i) * O.stride;
+                    if (hbd)
+                        *reinterpret_cast<uint2*>(row + 2 * (x0 + j0)) =
+                            make_uint2((uint32_t)o[0] | (uint32_t)o[1] << 16, (uint32_t)o[2] | (uint32_t)o[3] << 16);
+                    else
+                        *reinterpret_cast<uint32_t*>(row + x0 + j0) =
+                            (uint32_t)o[0] | (uint32_t)o[1] << 8 | (uint32_t)o[2] << 16 | (uint32_t)o[3] << 24;
+                } else {
+                    for (int e = 0; e < 4 && j0 + e < tw; e++) st_px(O, hbd, y0 + i, x0 + j0 + e, o[e]);
+                }
             }
             continue;
         }
