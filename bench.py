@@ -142,16 +142,25 @@ class ClockSampler:
         self.proc = None
 
     def __enter__(self):
+        self.first = []
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                  "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+            return self
+        # return once the tool has started and printed a sample (at most 5 s):
+        # its start-up talks to the driver, which must not overlap timed work
+        import select
+        if select.select([self.proc.stdout], [], [], 5.0)[0]:
+            line = self.proc.stdout.readline()
+            if line.strip():
+                self.first.append(line)
         return self
 
     def __exit__(self, *exc):
-        self.lines = []
+        self.lines = list(getattr(self, "first", []))
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -159,7 +168,7 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
                 out, _ = self.proc.communicate()
-            self.lines = [l for l in out.splitlines() if l.strip()]
+            self.lines += [l for l in out.splitlines() if l.strip()]
 
     def summary(self):
         sm, mx, reasons = [], None, set()
@@ -272,6 +281,10 @@ def run_gpu(args):
             if events is not None:
                 events[i].record(stream)
 
+    # clocks sampled over the warm-up, the timed steps and the per-frame / e2e
+    # runs that follow; started (and settled) before the warm-up
+    clk = ClockSampler(local)
+    clk.__enter__()
     with torch.cuda.stream(stream):
         for _ in range(max(args.warmup, 3)):
             step()
@@ -281,9 +294,11 @@ def run_gpu(args):
     torch.cuda.synchronize()
     ev_start = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ev_stage = [[torch.cuda.Event(enable_timing=True) for _ in stages] for _ in range(args.steps)]
-    clk = ClockSampler(local)
-    clk.__enter__()   # clocks sampled over the timed steps and the per-frame / e2e runs that follow
     with torch.cuda.stream(stream):
+        # a ~20 ms spin ahead of the first event keeps the stream busy while
+        # the host enqueues the first steps, so a host pause there cannot open
+        # an idle gap inside the timed region (the spin itself is not timed)
+        torch.cuda._sleep(40_000_000)
         for k in range(args.steps):
             ev_start[k].record(stream)
             step(ev_stage[k])

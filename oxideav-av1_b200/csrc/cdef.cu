@@ -144,7 +144,7 @@ __device__ __forceinline__ int filter_px(const int16_t* c, int xv, const Taps& T
     return clip3(mn, mx, xv + ((8 + sum - (sum < 0)) >> 4));
 }
 
-__global__ void __launch_bounds__(kCdefThreads, 3) cdef_kernel(const FrameDev* __restrict__ frames,
+__global__ void __launch_bounds__(kCdefThreads, 4) cdef_kernel(const FrameDev* __restrict__ frames,
                                                       const int32_t* __restrict__ starts, int n, int total) {
     __shared__ __align__(16) int16_t win[3][WMAX * WP];
     __shared__ BlockParams bp[64];
