@@ -34,6 +34,9 @@ CASES = [
     dict(seed=26, width=98, height=66, mono=True, film_grain=True),         # monochrome grain
     dict(seed=27, width=177, height=143, film_grain=True),                  # odd sizes, grain
     dict(seed=28, width=322, height=182, bit_depth=10, ssx=1, ssy=0, film_grain=True),  # 4:2:2 10-bit grain
+    # 32-sample chroma restoration units: LR tiles half as wide as the four-output runs assume
+    dict(seed=29, width=200, height=120, lr_unit=64, lr_uv_shift=1),
+    dict(seed=30, width=210, height=100, bit_depth=10, lr_unit=64, lr_uv_shift=1, lr_none_frac=0.2),
 ]
 
 
