@@ -42,7 +42,11 @@ typedef enum av1g_status {
     AV1G_EDEVICE = 5,        /* CUDA error (launch, copy, allocation)        */
     AV1G_EPARITY = 6,        /* debug self-check mismatch                    */
     AV1G_ENOTSUP = 7,        /* feature not handled by this build            */
-    AV1G_ENOTREADY = 8       /* ticket not finished yet (non-blocking poll)  */
+    AV1G_ENOTREADY = 8,      /* ticket not finished yet (non-blocking poll);
+                                av1g_decoder_receive_frame: no frame queued
+                                (the reference's NeedMore)                    */
+    AV1G_EOF = 9             /* av1g_decoder_receive_frame after flush with
+                                nothing left (the reference's Eof)            */
 } av1g_status;
 
 /* ---------------------------------------------------------------------
@@ -1048,6 +1052,53 @@ av1g_status av1g_parse_tile_list(const uint8_t* payload, size_t n, av1g_tile_lis
  * `data`).  out == NULL only measures. */
 av1g_status av1g_write_tile_list(const av1g_tile_list_header* hdr, const av1g_tile_list_obu_entry* entries,
                                  int32_t count, const uint8_t* data, uint8_t* out, size_t cap, uint64_t* out_len);
+
+/* ---------------------------------------------------------------------
+ * Stream decoder: the registry Decoder API over the whole path
+ * ------------------------------------------------------------------- */
+
+/* The reference's oxideav_core::Decoder implementation (Av1Decoder,
+ * src/registry.rs:103-195) over its decode session (SpecDecodeSession,
+ * src/decoder/frame_driver.rs:1295-1400): packets in, shown frames out.
+ * Host side per frame: the §7.5 OBU walk, the §5.9 header, the §5.11 tile
+ * walk (symbols, CDF contexts, motion vector prediction) producing the
+ * av1g_frame_desc of the frame; the GPU engine then reconstructs, filters and
+ * stores it.  engine == NULL gives a parse-only decoder that records every
+ * frame's descriptor (av1g_decoder_parsed_frame) and produces no pixels.
+ * operating_point: the §6.7.5 choice (0 = the preferred point). */
+typedef struct av1g_decoder av1g_decoder;
+av1g_status av1g_decoder_create(av1g_engine* engine, int32_t operating_point, av1g_decoder** out);
+/* Waits (bounded) for the frames in flight and frees the decoder. */
+void av1g_decoder_destroy(av1g_decoder* d);
+/* send_packet (registry.rs:132-166): a whole IVF file (DKIF magic) is split
+ * into its frame records, anything else is one §7.5 temporal unit; pts is
+ * carried to the frame (IVF records carry their own).  A malformed packet
+ * returns AV1G_EINVAL (av1g_last_error names the cause); the reference maps
+ * its typed errors to CoreError::invalid the same way. */
+av1g_status av1g_decoder_send_packet(av1g_decoder* d, const uint8_t* data, size_t n, int64_t pts);
+/* receive_frame (registry.rs:168-179): AV1G_OK with the next shown frame in
+ * output order (cropped planes, tight strides, u8 or little-endian u16 —
+ * the SpecFrame layout), valid until the next call; AV1G_ENOTREADY when no
+ * frame is queued (NeedMore); AV1G_EOF after av1g_decoder_flush once the
+ * queue is empty.  Waits (bounded) for the frame's GPU work. */
+av1g_status av1g_decoder_receive_frame(av1g_decoder* d, av1g_frame_out* out, int64_t* pts);
+/* flush (registry.rs:181-184): no more packets; receive drains, then EOF. */
+av1g_status av1g_decoder_flush(av1g_decoder* d);
+/* reset (registry.rs:186-195): drops queued frames and the reference state
+ * (reset_references, frame_driver.rs:1401), keeps the sequence header. */
+av1g_status av1g_decoder_reset(av1g_decoder* d);
+/* Parse-only decoders: the number of frames parsed so far and frame i's
+ * descriptor (pointers valid while the decoder lives) with its header. */
+int32_t av1g_decoder_parsed_count(const av1g_decoder* d);
+av1g_status av1g_decoder_parsed_frame(const av1g_decoder* d, int32_t i, av1g_frame_desc* out,
+                                      av1g_parsed_frame_header* fh);
+/* The current sequence header. */
+av1g_status av1g_decoder_sequence(const av1g_decoder* d, av1g_sequence_header* out);
+/* Host milliseconds spent in send_packet (framing, headers, tile walk). */
+double av1g_decoder_host_ms(const av1g_decoder* d);
+/* Frames so far whose tile data did not end at its §8.2.4 trailing bit
+ * after the walk (a stream the walk read differently from its encoder). */
+int32_t av1g_decoder_frames_out_of_sync(const av1g_decoder* d);
 
 /* ---------------------------------------------------------------------
  * Library

@@ -21,7 +21,8 @@ AV1G_EDEVICE = 5
 AV1G_EPARITY = 6
 AV1G_ENOTSUP = 7
 AV1G_ENOTREADY = 8
-STATUS_NAMES = {0: "OK", 1: "EINVAL", 2: "ENOMEM_BUDGET", 3: "EBUSY", 4: "TIMEOUT", 5: "EDEVICE",
+AV1G_EOF = 9
+STATUS_NAMES = {0: "OK", 1: "EINVAL", 2: "ENOMEM_BUDGET", 3: "EBUSY", 4: "TIMEOUT", 5: "EDEVICE", 9: "EOF",
                 6: "EPARITY", 7: "ENOTSUP", 8: "ENOTREADY"}
 
 MODE_BATCHED = 0
@@ -461,6 +462,18 @@ _SIGS = {
     "av1g_release_output": (C.c_int, [C.c_void_p, C.c_uint64]),
     "av1g_warp_estimation": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                        C.c_int16, C.c_int16, C.POINTER(C.c_int32), C.POINTER(C.c_uint8)]),
+    "av1g_decoder_create": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)]),
+    "av1g_decoder_destroy": (None, [C.c_void_p]),
+    "av1g_decoder_send_packet": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int64]),
+    "av1g_decoder_receive_frame": (C.c_int, [C.c_void_p, C.POINTER(FrameOut), C.POINTER(C.c_int64)]),
+    "av1g_decoder_flush": (C.c_int, [C.c_void_p]),
+    "av1g_decoder_reset": (C.c_int, [C.c_void_p]),
+    "av1g_decoder_parsed_count": (C.c_int32, [C.c_void_p]),
+    "av1g_decoder_parsed_frame": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(FrameDesc),
+                                            C.POINTER(ParsedFrameHeader)]),
+    "av1g_decoder_sequence": (C.c_int, [C.c_void_p, C.POINTER(SequenceHeader)]),
+    "av1g_decoder_host_ms": (C.c_double, [C.c_void_p]),
+    "av1g_decoder_frames_out_of_sync": (C.c_int32, [C.c_void_p]),
 }
 
 NOALLOC_MAX_FRAMES = 16

@@ -2,13 +2,15 @@
 
 Run in a checkout that has the reference crate beside it:
 
-    python tests/golden/make_framing_fixtures.py /root/reference
+    python tests/golden/make_framing_fixtures.py <reference checkout>
 
 Reads (text only; nothing of the reference is executed):
   tests/fixture_conformance.rs       every IVF stream a test decodes, with the
-                                     shown-frame count the test asserts and,
-                                     where present, the SHA-256 digest of the
-                                     decoded planes
+                                     shown-frame count the test asserts and
+                                     the SHA-256 digest of the decoded planes
+                                     (the digest the test asserts, or the
+                                     digest of the raw / run-length expected
+                                     planes it compares byte for byte)
   tests/sequence_header_fixtures.rs  the 16 SEQUENCE_HEADER OBU payloads and
                                      the field values the test expects
   tests/annexb_conformance.rs        the external Annex B stream, its shown-
@@ -20,6 +22,7 @@ and writes framing_fixtures.json.gz next to this script.
 """
 import base64
 import gzip
+import hashlib
 import json
 import re
 import sys
@@ -45,13 +48,30 @@ def ivf_streams(ref):
     pat = re.compile(r'(assert_decodes_byte_exact_rle|assert_decodes_byte_exact|assert_decodes_to_digest)\(\s*'
                      r'"([^"]+)"\s*,\s*([A-Z0-9_]+)\s*,\s*("([0-9a-f]{64})"|[A-Z0-9_]+)\s*,\s*(\d+)\s*,?\s*\)', re.S)
     for m in pat.finditer(src):
-        kind, name, ivf_const, _, digest, frames = m.groups()
+        kind, name, ivf_const, expected, digest, frames = m.groups()
         hexs = consts.get(ivf_const)
         if not hexs or not hexs.lower().startswith("444b4946"):
             continue
+        if kind == "assert_decodes_to_digest":
+            sha = digest or consts.get(expected)
+            source = "digest"
+        else:
+            # the test compares the decoded planes with these bytes: keep their digest
+            body = consts[expected]
+            raw = _unrle(body) if kind == "assert_decodes_byte_exact_rle" else bytes.fromhex(body)
+            sha = hashlib.sha256(raw).hexdigest()
+            source = "expected planes"
         streams[name] = {"name": name, "const": ivf_const, "ivf": base64.b64encode(bytes.fromhex(hexs)).decode(),
-                         "shown_frames": int(frames), "sha256": digest if kind == "assert_decodes_to_digest" else None}
+                         "shown_frames": int(frames), "sha256": sha, "sha256_source": source}
     return list(streams.values())
+
+
+def _unrle(body):
+    """(value u8, count u16) triples, six hex digits each (fixture_conformance.rs unrle)."""
+    out = bytearray()
+    for i in range(0, len(body), 6):
+        out += bytes([int(body[i:i + 2], 16)]) * int(body[i + 2:i + 6], 16)
+    return bytes(out)
 
 
 def sequence_headers(ref):
@@ -123,7 +143,9 @@ def annexb_stream(ref):
 
 
 def main():
-    ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_framing_fixtures.py <reference checkout>")
+    ref = Path(sys.argv[1])
     data = {"source": "reference tests: fixture_conformance.rs, sequence_header_fixtures.rs, annexb_conformance.rs, "
                       "frame_header_fixtures.rs",
             "ivf_streams": ivf_streams(ref), "sequence_headers": sequence_headers(ref),
