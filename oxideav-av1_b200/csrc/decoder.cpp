@@ -12,7 +12,6 @@
 // candidates) is kept here, as the reference keeps it in SpecRefSlot
 // (frame_driver.rs:84-139, reference_frame_update 1409).
 #include <chrono>
-#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <deque>
@@ -267,9 +266,6 @@ av1g_status decode_frame(av1g_decoder* d, const av1g_parsed_frame_header& fh, co
     av1g_status st = av1w::walk_frame(d->seq, fh, d->refs, d->slots, tiles, *fo, err);
     if (st != AV1G_OK) return dfail(st, err);
     if (!fo->tiles_in_sync) d->frames_out_of_sync++;
-    if (getenv("AV1W_DEBUG"))
-        fprintf(stderr, "frame %d type %d show %d %dx%d sync %d q %d\n", (int)d->parsed.size(), fh.frame_type,
-                fh.show_frame, fh.pf.frame_width, fh.pf.frame_height, (int)fo->tiles_in_sync, fh.base_q_idx);
     if (av1g_status s2 = submit(d, fh, fo, pts)) return s2;
     update_slots(d, fh, fo);
     if (av1g_status s3 = av1g_ref_state_update(&d->refs, &fh)) return s3;

@@ -2070,7 +2070,7 @@ void Walker::find_warp_samples() {
             for (int i = 0; i < std::min(bw4, MiCols - MiCol); i += step) {
                 srcSize = MiSizes[cell(MiRow - 1, MiCol + i)];
                 srcW = Num_4x4_Blocks_Wide[srcSize];
-                step = std::max(srcW, 2);
+                step = std::min(bw4, srcW);
                 add_sample(-1, i);
             }
         }
@@ -2087,7 +2087,7 @@ void Walker::find_warp_samples() {
             for (int i = 0; i < std::min(bh4, MiRows - MiRow); i += step) {
                 srcSize = MiSizes[cell(MiRow + i, MiCol - 1)];
                 srcH = Num_4x4_Blocks_High[srcSize];
-                step = std::max(srcH, 2);
+                step = std::min(bh4, srcH);
                 add_sample(i, -1);
             }
         }
