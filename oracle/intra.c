@@ -312,10 +312,24 @@ void ora_intra_predict(const ora_plane* p, int sx, int sy, int tx, int mode, int
     }
 }
 
-/* predict_chroma_from_luma_into_curr_frame (cdf.rs:17256-17340), without the
- * luma overhang store (luma outside the plane reads as 0). */
-static void cfl(ora_plane* luma, ora_plane* p, int sx, int sy, int tx, int ssx, int ssy, int alpha, int bd,
-                int max_luma_w, int max_luma_h) {
+/* The luma a transform writes past the mi-grid plane (LumaOverhang,
+ * cdf.rs:15938-15990: up to 64 samples right of and below the plane), kept
+ * for chroma from luma. */
+typedef struct {
+    int32_t* s;
+    int rows, cols; /* plane rows + 64, plane cols + 64 */
+} overhang;
+
+static int32_t luma_at(const ora_plane* luma, const overhang* oh, int yy, int xx) {
+    if (yy < luma->rows && xx < luma->cols) return luma->s[(size_t)yy * luma->cols + xx];
+    if (oh && yy < oh->rows && xx < oh->cols) return oh->s[(size_t)yy * oh->cols + xx];
+    return 0;
+}
+
+/* predict_chroma_from_luma_into_curr_frame (cdf.rs:17256-17340): luma past
+ * the plane comes from the overhang store (read at cdf.rs:17292-17305). */
+static void cfl(ora_plane* luma, const overhang* oh, ora_plane* p, int sx, int sy, int tx, int ssx, int ssy,
+                int alpha, int bd, int max_luma_w, int max_luma_h) {
     int w = TW_[tx], h = TH_[tx];
     int cx = max_luma_w - (1 << ssx), cy = max_luma_h - (1 << ssy);
     if (cx < 0) cx = 0;
@@ -332,7 +346,7 @@ static void cfl(ora_plane* luma, ora_plane* p, int sx, int sy, int tx, int ssx, 
             for (int dy = 0; dy <= ssy; dy++)
                 for (int dx = 0; dx <= ssx; dx++) {
                     int yy = ly + dy, xx = lx + dx;
-                    t += (yy < luma->rows && xx < luma->cols) ? luma->s[(size_t)yy * luma->cols + xx] : 0;
+                    t += luma_at(luma, oh, yy, xx);
                 }
             int64_t v = t << (3 - ssx - ssy);
             l[i * w + j] = v;
@@ -364,12 +378,16 @@ int ora_intra_frame(const av1g_frame_header* hdr, const av1g_quant_params* q, co
                     const int32_t* coeffs, ora_plane planes[3], const uint8_t* maps, int64_t map_bytes,
                     const ora_plane* side) {
     uint16_t* pred = (uint16_t*)malloc(sizeof(uint16_t) * 64 * 64);
+    int32_t* full = (int32_t*)malloc(sizeof(int32_t) * 64 * 64);
+    overhang oh = {NULL, planes[0].rows + 64, planes[0].cols + 64};
+    oh.s = (int32_t*)calloc((size_t)oh.rows * oh.cols, sizeof(int32_t));
     int rc = 0;
     for (int k = 0; k < n; k++) {
         const av1g_intra_tu* t = &tus[k];
         ora_plane* p = &planes[t->plane];
         int w = TW_[t->tx_size], h = TH_[t->tx_size];
         int have_pred = t->mode < INTRA_MODES;
+        int luma_overhang = t->plane == 0 && !t->interintra && (t->x + w > p->cols || t->y + h > p->rows);
         if (t->interintra) {
             static const int ii_to_intra[4] = {0, 1, 2, 9};
             if (t->interintra > 2 || t->interintra_mode > 3 || t->mode != ii_to_intra[t->interintra_mode] ||
@@ -421,10 +439,31 @@ int ora_intra_frame(const av1g_frame_header* hdr, const av1g_quant_params* q, co
                 }
         }
         if ((t->flags & AV1G_INTRA_CFL) && t->plane > 0)
-            cfl(&planes[0], p, t->x, t->y, t->tx_size, hdr->subsampling_x, hdr->subsampling_y, t->cfl_alpha,
+            cfl(&planes[0], &oh, p, t->x, t->y, t->tx_size, hdr->subsampling_x, hdr->subsampling_y, t->cfl_alpha,
                 hdr->bit_depth, t->max_luma_w, t->max_luma_h);
+        if (luma_overhang && have_pred) {
+            /* the whole transform (prediction + residual) for the samples past
+             * the plane (the merge's side-store writes, cdf.rs:17441-17477) */
+            for (int i = 0; i < w * h; i++) full[i] = pred[i];
+            if (t->flags & AV1G_INTRA_RESIDUAL) {
+                av1g_tu r = t->res;
+                r.x = 0;
+                r.y = 0;
+                r.plane = 0;
+                ora_plane tp[3] = {{full, h, w}, {full, h, w}, {full, h, w}};
+                ora_recon_frame(hdr, q, &r, 1, coeffs, tp);
+            }
+            for (int i = 0; i < h; i++)
+                for (int j = 0; j < w; j++) {
+                    int yy = t->y + i, xx = t->x + j;
+                    if ((yy >= p->rows || xx >= p->cols) && yy < oh.rows && xx < oh.cols)
+                        oh.s[(size_t)yy * oh.cols + xx] = full[i * w + j];
+                }
+        }
         if (t->flags & AV1G_INTRA_RESIDUAL) ora_recon_frame(hdr, q, &t->res, 1, coeffs, planes);
     }
     free(pred);
+    free(full);
+    free(oh.s);
     return rc;
 }

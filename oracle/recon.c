@@ -266,7 +266,8 @@ void ora_inverse_transform_2d(const int64_t* dq, int tx, int tt, int bit_depth, 
     }
 }
 
-/* curr_frame_step3_merge (cdf.rs:17398-17470), without the luma overhang store */
+/* curr_frame_step3_merge (cdf.rs:17398-17470) inside the plane; ora_intra_frame
+ * keeps the luma past the plane (the overhang store) itself */
 static void merge(ora_plane* p, int x0, int y0, int tx, int tt, const int64_t* res, int bit_depth) {
     int w = TXW_[tx], h = TXH_[tx];
     int fud = tt == FLIPADST_DCT || tt == FLIPADST_ADST || tt == V_FLIPADST || tt == FLIPADST_FLIPADST;

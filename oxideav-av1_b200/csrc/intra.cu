@@ -572,8 +572,12 @@ __device__ void intra_tu(const G& g, S& s, const IntraFrame& F, const SbCtx& c, 
         g.sync();
     }
     if ((t.flags & AV1G_INTRA_CFL) && pl > 0) {
-        // predict_chroma_from_luma_into_curr_frame (cdf.rs:17256-17340); luma
-        // outside the luma plane reads as 0
+        // predict_chroma_from_luma_into_curr_frame (cdf.rs:17256-17340).  The
+        // block's luma transforms may run past the mi-grid plane; their
+        // samples there stay in the superblock's staged copy (the reference's
+        // LumaOverhang side store, cdf.rs:15938, read at cdf.rs:17292-17305),
+        // which spans the whole superblock.  Luma neither in the plane nor in
+        // that copy reads as 0.
         const PlaneDev& Y = F.planes[0];
         const int ssx = F.ssx, ssy = F.ssy;
         const int cx = max((int)t.max_luma_w - (1 << ssx), 0), cy = max((int)t.max_luma_h - (1 << ssy), 0);
@@ -585,7 +589,9 @@ __device__ void intra_tu(const G& g, S& s, const IntraFrame& F, const SbCtx& c, 
             for (int ddy = 0; ddy <= ssy; ddy++)
                 for (int ddx = 0; ddx <= ssx; ddx++) {
                     int yy = ly + ddy, xx = lx + ddx;
-                    acc += (yy < Y.h && xx < Y.w) ? rdp(F, c, cache, 0, yy, xx) : 0;
+                    const bool staged = (unsigned)(yy - c.y0[0]) < (unsigned)c.h[0] &&
+                                        (unsigned)(xx - c.x0[0]) < (unsigned)c.w[0];
+                    acc += (staged || (yy < Y.h && xx < Y.w)) ? rdp(F, c, cache, 0, yy, xx) : 0;
                 }
             int v = acc << (3 - ssx - ssy);
             s.buf[k] = v;
@@ -605,13 +611,15 @@ __device__ void intra_tu(const G& g, S& s, const IntraFrame& F, const SbCtx& c, 
         g.sync();
     }
     if (has_res) {
-        // curr_frame_step3_merge (cdf.rs:17398-17470): Clip1(pred + residual)
+        // curr_frame_step3_merge (cdf.rs:17398-17470): Clip1(pred + residual);
+        // luma past the plane is merged too, in the staged copy only (the
+        // overhang chroma from luma reads)
 #pragma unroll
         for (int q = 0; q < (G::N == 32 ? KP : (W * H + G::N - 1) / G::N); q++) {
             const int k = tid + q * G::N;
             if (k >= W * H) break;
             const int i = k >> LW, j = k & (W - 1);
-            if (sy + i >= P.h || sx + j >= P.w) continue;
+            if (pl != 0 && (sy + i >= P.h || sx + j >= P.w)) continue;
             int v;
             if constexpr (G::N == 32) v = rv[q];
             else v = __ldg(rp + k);

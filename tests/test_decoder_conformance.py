@@ -27,11 +27,8 @@ from oxideav_av1_b200 import decoder
 HERE = Path(__file__).resolve().parent
 STREAMS = json.load(gzip.open(HERE / "golden" / "framing_fixtures.json.gz"))["ivf_streams"]
 
-# Streams the build does not yet reproduce, with the reason.
-KNOWN_DIFFERENT = {
-    "cfl-tu-overhang-10bit": "CfL reads the luma a transform writes past the mi grid (the reference's luma "
-                             "overhang side store); this build reads 0 there",
-}
+# Streams the build does not reproduce, with the reason (none at present).
+KNOWN_DIFFERENT = {}
 
 
 def _ivf(s):
