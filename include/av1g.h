@@ -352,13 +352,23 @@ typedef struct av1g_intra_job {
 /* §7.11.2 intra prediction (DC, V, H, directional with edge filter and
  * upsampling, SMOOTH*, PAETH, recursive filter intra), §7.11.5 chroma from
  * luma, then dequant + inverse transform + merge, for every intra TU of `n`
- * frames.  Replaces predict_intra_into_curr_frame (src/cdf.rs:16789),
+ * frames.  Returns once the launch has finished: AV1G_EDEVICE names the job
+ * one of whose superblock dependency waits ran out of time (a bounded wait,
+ * 2 s; only that job's samples are incomplete, and later calls are not
+ * affected).  Replaces predict_intra_into_curr_frame (src/cdf.rs:16789),
  * intra_predict_block_samples (cdf.rs:16990-17250), the kernels at
  * cdf.rs:1348-3120 and predict_chroma_from_luma_into_curr_frame
  * (cdf.rs:17256) as called from transform_block_emit (cdf.rs:32482).
  * Superblocks run as a wavefront (level = column + 2 * row): one launch per
  * level across all frames, each superblock's TUs in decode order. */
 av1g_status av1g_run_intra(const av1g_intra_job* jobs, int32_t n, void* stream);
+
+/* Test hook for the wait bound above, on the current device: wait_ns sets
+ * the bound (<= 0 restores 2 s) and, while frame_width > 0, every intra job
+ * whose frame is that wide gets a superblock wait that nothing satisfies, so
+ * its wait runs out after wait_ns.  No counterpart in the reference (its
+ * decode is single-threaded and never waits). */
+av1g_status av1g_test_intra_wait_fault(int64_t wait_ns, int32_t frame_width);
 
 /* ---------------------------------------------------------------------
  * Inter prediction

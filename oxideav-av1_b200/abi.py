@@ -474,6 +474,7 @@ _SIGS = {
     "av1g_decoder_sequence": (C.c_int, [C.c_void_p, C.POINTER(SequenceHeader)]),
     "av1g_decoder_host_ms": (C.c_double, [C.c_void_p]),
     "av1g_decoder_frames_out_of_sync": (C.c_int32, [C.c_void_p]),
+    "av1g_test_intra_wait_fault": (C.c_int, [C.c_int64, C.c_int32]),
 }
 
 NOALLOC_MAX_FRAMES = 16

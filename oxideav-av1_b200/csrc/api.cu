@@ -24,6 +24,8 @@ namespace av1g {
 size_t lr_smem_bytes();
 av1g_status recon_run(const av1g_recon_job* jobs, int n, cudaStream_t s, std::string& err);
 av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t s, std::string& err);
+av1g_status intra_run_status(const av1g_intra_job* jobs, int n, cudaStream_t s, std::string& err,
+                             int32_t* frame_status);
 av1g_status inter_run(const av1g_inter_job* jobs, int n, cudaStream_t s, std::string& err);
 av1g_status mf_store_run(const av1g_mf_store_job* jobs, int n, cudaStream_t s, std::string& err);
 av1g_status mf_project_run(const av1g_mf_project_job* jobs, int n, cudaStream_t s, std::string& err);
@@ -461,10 +463,30 @@ av1g_status av1g_run_intra(const av1g_intra_job* jobs, int32_t n, void* stream) 
     g_err.clear();
     if (n < 0 || (n > 0 && !jobs)) return fail(AV1G_EINVAL, "bad job array");
     if (n == 0) return AV1G_OK;
+    // each job's wait status lands in pinned memory after the launch; the
+    // call returns once the launch has finished so that it reports it
+    thread_local int32_t* t_status = nullptr;
+    thread_local int32_t t_cap = 0;
+    if (t_cap < n) {
+        if (t_status) cudaFreeHost(t_status);
+        t_status = nullptr;
+        t_cap = 0;
+        cudaError_t e = cudaHostAlloc((void**)&t_status, sizeof(int32_t) * (size_t)n, cudaHostAllocDefault);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaHostAlloc");
+        t_cap = n;
+    }
     std::string err;
-    av1g_status st = intra_run(jobs, n, (cudaStream_t)stream, err);
-    if (st != AV1G_OK) g_err = err;
-    return st;
+    av1g_status st = intra_run_status(jobs, n, (cudaStream_t)stream, err, t_status);
+    if (st != AV1G_OK) {
+        g_err = err;
+        return st;
+    }
+    cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+    for (int i = 0; i < n; i++)
+        if (t_status[i])
+            return fail(AV1G_EDEVICE, "intra job %d: a superblock dependency wait ran out of time", i);
+    return AV1G_OK;
 }
 av1g_status av1g_run_inter(const av1g_inter_job* jobs, int32_t n, void* stream) {
     g_err.clear();

@@ -40,6 +40,8 @@
 namespace av1g {
 av1g_status recon_run(const av1g_recon_job* jobs, int n, cudaStream_t s, std::string& err);
 av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t s, std::string& err);
+av1g_status intra_run_status(const av1g_intra_job* jobs, int n, cudaStream_t s, std::string& err,
+                             int32_t* frame_status);
 av1g_status inter_run(const av1g_inter_job* jobs, int n, cudaStream_t s, std::string& err);
 av1g_status postfilter_run(const av1g_frame_job* jobs, int n, cudaStream_t s, std::string& err);
 av1g_status postfilter_result_planes(const av1g_frame_job& j, PlaneDev pre[3], PlaneDev out[3], std::string& err);
@@ -116,6 +118,10 @@ struct Ticket {
 struct Step {
     cudaEvent_t ev = nullptr, ev0 = nullptr;
     std::vector<std::shared_ptr<Ticket>> tickets;
+    // the intra launch's per-frame wait status (pinned, filled in stream
+    // order) and the ticket of each of its jobs
+    int32_t* intra_status = nullptr;
+    std::vector<std::shared_ptr<Ticket>> intra_tickets;
     size_t work_bytes = 0;
     Clock::time_point t_enqueued;
 };
@@ -482,7 +488,36 @@ void enqueue_step(av1g_engine* E, cudaStream_t cs, std::vector<std::shared_ptr<T
             jobs.push_back(j);
             ws.push_back(&w);
         }
-        run_stage(ws, jobs, intra_run, cs);
+        if (!jobs.empty()) {
+            // every job's wait status is read back after the step (the
+            // completer fails that frame's ticket if its wait ran out)
+            step.intra_status = (int32_t*)E->pinned_get(sizeof(int32_t) * jobs.size());
+            if (!step.intra_status) {
+                run_stage(ws, jobs, intra_run, cs);  // no pinned memory: no status readback
+                goto intra_done;
+            }
+            {
+            std::string err;
+            av1g_status st = intra_run_status(jobs.data(), (int)jobs.size(), cs, err, step.intra_status);
+            if (st == AV1G_OK) {
+                for (Work* w : ws) step.intra_tickets.push_back(w->t);
+            } else {
+                // the batch was rejected: per frame, so that only the offending frames fail
+                for (size_t i = 0; i < jobs.size(); i++) {
+                    std::string e1;
+                    av1g_status s1 = intra_run_status(&jobs[i], 1, cs, e1, step.intra_status + i);
+                    if (s1 != AV1G_OK) fail_work(*ws[i], s1, e1);
+                    else step.intra_tickets.push_back(ws[i]->t);
+                    if (s1 != AV1G_OK) step.intra_status[i] = 0;
+                }
+                // keep the job-to-ticket order: rejected jobs map to no ticket
+                std::vector<std::shared_ptr<Ticket>> tk;
+                for (size_t i = 0; i < jobs.size(); i++) tk.push_back(ws[i]->failed ? nullptr : ws[i]->t);
+                step.intra_tickets.swap(tk);
+            }
+            }
+        }
+    intra_done:;
     }
     lap(3);
     // the §7.4 chain
@@ -715,6 +750,16 @@ void completer_loop(av1g_engine* E) {
                 Step step = std::move(front);
                 L->steps.pop_front();
                 auto now = Clock::now();
+                if (q == cudaSuccess && step.intra_status) {
+                    for (size_t i = 0; i < step.intra_tickets.size(); i++) {
+                        auto& t = step.intra_tickets[i];
+                        if (t && step.intra_status[i] && t->status == AV1G_OK) {
+                            t->status = AV1G_EDEVICE;
+                            t->err = "intra: a superblock dependency wait ran out of time";
+                        }
+                    }
+                }
+                if (step.intra_status && !expired) E->pinned_put((uint8_t*)step.intra_status);
                 for (auto& t : step.tickets) {
                     if (q != cudaSuccess && t->status == AV1G_OK) {
                         t->status = expired ? AV1G_TIMEOUT : AV1G_EDEVICE;

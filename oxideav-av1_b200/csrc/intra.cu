@@ -25,9 +25,14 @@
 // per warp, then its large TUs with the whole CTA — writes the samples back and
 // publishes a done flag.  A CTA only waits for superblocks claimed before its
 // own, by CTAs that are running, so every wait ends; the time bound only
-// guards against a broken invariant (it sets a sticky fault word and the
-// launch drains).
+// guards against a broken invariant: a wait that runs out sets its frame's
+// abort word in the launch's control block, every superblock of that frame
+// then skips its remaining TUs (still publishing its levels, so no wait of
+// the launch is left hanging), and the host reports that frame of that
+// launch as AV1G_EDEVICE.  Other frames of the batch are not affected: waits
+// never cross frames.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -51,7 +56,7 @@ constexpr int kSmallPx = kIntraSmallPx;
 constexpr int kLvChunk = 64;        // level-table entries staged at a time
 constexpr int kTuWin = 128;         // TU records staged at a time
 constexpr int kWaitWin = 32;        // waits staged per superblock (more: read from HBM)
-constexpr long long kWaitNs = 2000000000LL;
+constexpr long long kWaitNs = 2000000000LL;  // the bound of one dependency wait
 
 __constant__ AV1T_MODE_TO_ANGLE_TYPE c_mode_angle AV1T_MODE_TO_ANGLE_DIMS = AV1T_MODE_TO_ANGLE_INIT;
 __constant__ AV1T_DR_INTRA_DERIVATIVE_TYPE c_dr AV1T_DR_INTRA_DERIVATIVE_DIMS = AV1T_DR_INTRA_DERIVATIVE_INIT;
@@ -71,7 +76,9 @@ struct SbCtx {
 
 __device__ const AV1T_II_WEIGHTS_1D_TYPE g_ii_w AV1T_II_WEIGHTS_1D_DIMS = AV1T_II_WEIGHTS_1D_INIT;
 __device__ const wedge::Master g_wmaster = wedge::kMaster;
-__device__ unsigned g_wave_fault;  // sticky: a dependency wait ran out of time
+// The wait bound in effect (kWaitNs unless a test shortens it, see
+// av1g_test_intra_wait_fault).
+__device__ long long g_wait_ns = kWaitNs;
 
 // The intra half of an inter-intra block: blend of the intra prediction
 // with the inter half (mask_blend_interintra, src/inter_pred.rs:3272).  The
@@ -790,6 +797,7 @@ __global__ void __launch_bounds__(kT) intra_kernel(const IntraFrame* __restrict_
                                                    const SbItem* __restrict__ items, const int2* __restrict__ lvs,
                                                    const int4* __restrict__ waits, int* prog, int* ctl, int nitems,
                                                    const int32_t* __restrict__ res) {
+    // ctl[0]: the claim counter; ctl[1 + f]: frame f's abort word
     // dynamic shared memory: Shared | TU window | superblock copy
     extern __shared__ __align__(16) uint8_t dsm[];
     Shared& S = *reinterpret_cast<Shared*>(dsm);
@@ -853,16 +861,17 @@ __global__ void __launch_bounds__(kT) intra_kernel(const IntraFrame* __restrict_
                     const int w0 = wq;
                     while (wq < it.nwait && wsrc[wq].x <= lg) wq++;
                     next_wait = wq < it.nwait ? wsrc[wq].x : 0x7fffffff;
+                    int* abort_word = ctl + 1 + it.frame;
+                    const long long bound = *(volatile long long*)&g_wait_ns;
                     for (int q = w0 + tid; q < wq; q += kT) {
                         const int4 w = wsrc[q];
                         const volatile int* f = prog + w.y;
                         if (*f < w.z) {
                             const long long t0 = gtimer();
                             while (*f < w.z) {
-                                if (*(volatile int*)(ctl + 1)) break;
-                                if (gtimer() - t0 > kWaitNs) {
-                                    atomicOr(&g_wave_fault, 1u);
-                                    atomicExch(ctl + 1, 1);
+                                if (*(volatile int*)abort_word) break;
+                                if (gtimer() - t0 > bound) {
+                                    atomicExch(abort_word, 1);
                                     break;
                                 }
                                 __nanosleep(64);
@@ -871,7 +880,7 @@ __global__ void __launch_bounds__(kT) intra_kernel(const IntraFrame* __restrict_
                         ld_acquire(prog + w.y);
                     }
                     __syncthreads();
-                    if (tid == 0 && *(volatile int*)(ctl + 1)) S.abort_seen = 1;
+                    if (tid == 0 && *(volatile int*)abort_word) S.abort_seen = 1;
                     __syncthreads();
                 }
                 const bool publish = S.lv[L].y & kLevelPublished;
@@ -923,35 +932,46 @@ __global__ void __launch_bounds__(kT) intra_kernel(const IntraFrame* __restrict_
     }
 }
 
-// Pinned host mirror of g_wave_fault, per device.
-volatile unsigned* fault_mirror(int dev) {
-    static std::mutex mu;
-    static std::unordered_map<int, unsigned*> words;
-    std::lock_guard<std::mutex> lk(mu);
-    auto it = words.find(dev);
-    if (it != words.end()) return it->second;
-    unsigned* w = nullptr;
-    if (cudaHostAlloc((void**)&w, sizeof(unsigned), cudaHostAllocDefault) != cudaSuccess) return nullptr;
-    *w = 0;
-    words[dev] = w;
-    return w;
-}
-
 }  // namespace
 
 
-// Host side of av1g_run_intra: the plan (intra_plan.cu), its upload, one launch.
-av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t st, std::string& err) {
+namespace {
+// Test hook state: a never-satisfied wait is planned into the first
+// superblock of every job whose frame is this wide (0: none).
+std::atomic<int> g_fault_width{0};
+
+// Before its first level, the first superblock of job f waits for its own
+// progress to reach a value it never reaches.
+void plan_fault_wait(IntraPlan& plan, int f) {
+    for (size_t i = 0; i < plan.items.size(); i++) {
+        SbItem& it = plan.items[i];
+        if (it.frame != f) continue;
+        plan.waits.insert(plan.waits.begin() + it.wait_first, int4{0, (int)i, 0x3fffffff, 0});
+        it.nwait++;
+        for (size_t k = 0; k < plan.items.size(); k++)
+            if (k != i && plan.items[k].wait_first >= it.wait_first) plan.items[k].wait_first++;
+        return;
+    }
+}
+}  // namespace
+
+// Host side of av1g_run_intra: the plan (intra_plan.cu), its upload, one
+// launch.  frame_status (pinned host memory of n words, or null) receives,
+// in stream order after the launch, each job's abort word: non-zero when a
+// dependency wait of that frame ran out of time.
+av1g_status intra_run_status(const av1g_intra_job* jobs, int n, cudaStream_t st, std::string& err,
+                             int32_t* frame_status) {
     int dev = 0;
     cudaGetDevice(&dev);
-    volatile unsigned* fault = fault_mirror(dev);
-    if (fault && *fault) {
-        err = "an earlier intra launch on this device gave up waiting for a superblock";
-        return AV1G_EDEVICE;
-    }
     IntraPlan plan;
     av1g_status rc = intra_plan(jobs, n, plan, err);
-    if (rc != AV1G_OK || plan.items.empty()) return rc;
+    if (rc != AV1G_OK || plan.items.empty()) {
+        if (rc == AV1G_OK && frame_status) memset(frame_status, 0, sizeof(int32_t) * n);
+        return rc;
+    }
+    if (int fw = g_fault_width.load(); fw > 0)
+        for (int i = 0; i < n; i++)
+            if (jobs[i].hdr->frame_width == fw) plan_fault_wait(plan, i);
     const int nitems = (int)plan.items.size();
     // residual tasks; each TU's device record points at its residual block
     std::vector<ResTask> rs, rl;
@@ -976,7 +996,7 @@ av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t st, std::s
     const size_t off_waits = al(off_lv + sizeof(int2) * plan.lvtab.size());
     const size_t off_done = al(off_waits + sizeof(int4) * plan.waits.size());
     const size_t off_ctl = al(off_done + sizeof(int) * plan.items.size());
-    const size_t off_rs = al(off_ctl + 2 * sizeof(int));
+    const size_t off_rs = al(off_ctl + (1 + (size_t)n) * sizeof(int));
     const size_t off_rl = al(off_rs + sizeof(ResTask) * rs.size());
     const size_t off_maps = al(off_rl + sizeof(ResTask) * rl.size());
     const size_t bytes = off_maps + plan.maps.size();  // uploaded
@@ -1028,8 +1048,9 @@ av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t st, std::s
             (int*)(dev_buf + off_ctl), nitems, dres);
         e = cudaGetLastError();
     }
-    if (e == cudaSuccess && fault)
-        e = cudaMemcpyFromSymbolAsync((void*)fault, g_wave_fault, sizeof(unsigned), 0, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && frame_status)
+        e = cudaMemcpyAsync(frame_status, dev_buf + off_ctl + sizeof(int), sizeof(int32_t) * n,
+                            cudaMemcpyDeviceToHost, st);
     cudaFreeAsync(dev_buf, st);
     if (e != cudaSuccess) {
         err = std::string("intra launch: ") + cudaGetErrorString(e);
@@ -1038,4 +1059,16 @@ av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t st, std::s
     return AV1G_OK;
 }
 
+av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t st, std::string& err) {
+    return intra_run_status(jobs, n, st, err, nullptr);
+}
+
 }  // namespace av1g
+
+extern "C" av1g_status av1g_test_intra_wait_fault(int64_t wait_ns, int32_t frame_width) {
+    long long ns = wait_ns > 0 ? (long long)wait_ns : av1g::kWaitNs;
+    cudaError_t e = cudaMemcpyToSymbol(av1g::g_wait_ns, &ns, sizeof ns);
+    if (e != cudaSuccess) return AV1G_EDEVICE;
+    av1g::g_fault_width.store(frame_width > 0 ? frame_width : 0);
+    return AV1G_OK;
+}
