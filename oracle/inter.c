@@ -155,7 +155,7 @@ static int setup_shear(const int32_t p[6], int* valid, int32_t abcd[4]) {
     int32_t fac;
     int sh;
     if (resolve_divisor(p[2], &fac, &sh)) return ERR;
-    int64_t v = (int64_t)p[4] << 16;
+    int64_t v = (int64_t)p[4] * 65536;
     int32_t gamma0 = clip3(-32768, 32767, (int32_t)rnd2s(sat_mul(v, fac), sh));
     int64_t w = (int64_t)p[3] * p[4];
     int32_t corr = (int32_t)rnd2s(sat_mul(w, fac), sh);

@@ -298,6 +298,9 @@ int launch_all(const Prepared& P, const uint8_t* dev, cudaStream_t s) {
     int nl = 0;
     auto launch_stage = [&](int st, const FrameDev* fr, const int32_t* starts, const int32_t* starts_tmpl, int nn,
                             int total, int total_tmpl, int cells) {
+        static const char* const names[ST_COUNT] = {"av1g deblock", "av1g cdef", "av1g superres",
+                                                     "av1g loop restoration", "av1g film grain"};
+        NvtxRange range(names[st]);
         switch (st) {
             case ST_DEBLOCK: if (total) { launch_deblock(fr, starts, nn, total, cells, P.shape[st], s); nl += 2; } break;
             case ST_CDEF: if (total) { launch_cdef(fr, starts, nn, total, P.shape[st], s); nl++; } break;
@@ -451,6 +454,7 @@ av1g_status av1g_run_film_grain(const av1g_frame_job* jobs, int32_t n, void* str
     return run(jobs, n, 1 << ST_GRAIN, AV1G_MODE_BATCHED, stream, nullptr);
 }
 av1g_status av1g_run_recon(const av1g_recon_job* jobs, int32_t n, void* stream) {
+    NvtxRange range("av1g recon");
     g_err.clear();
     if (n < 0 || (n > 0 && !jobs)) return fail(AV1G_EINVAL, "bad job array");
     if (n == 0) return AV1G_OK;
@@ -460,6 +464,7 @@ av1g_status av1g_run_recon(const av1g_recon_job* jobs, int32_t n, void* stream) 
     return st;
 }
 av1g_status av1g_run_intra(const av1g_intra_job* jobs, int32_t n, void* stream) {
+    NvtxRange range("av1g intra");
     g_err.clear();
     if (n < 0 || (n > 0 && !jobs)) return fail(AV1G_EINVAL, "bad job array");
     if (n == 0) return AV1G_OK;
@@ -489,6 +494,7 @@ av1g_status av1g_run_intra(const av1g_intra_job* jobs, int32_t n, void* stream) 
     return AV1G_OK;
 }
 av1g_status av1g_run_inter(const av1g_inter_job* jobs, int32_t n, void* stream) {
+    NvtxRange range("av1g inter");
     g_err.clear();
     if (n < 0 || (n > 0 && !jobs)) return fail(AV1G_EINVAL, "bad job array");
     if (n == 0) return AV1G_OK;
@@ -498,6 +504,7 @@ av1g_status av1g_run_inter(const av1g_inter_job* jobs, int32_t n, void* stream) 
     return st;
 }
 av1g_status av1g_run_mf_store(const av1g_mf_store_job* jobs, int32_t n, void* stream) {
+    NvtxRange range("av1g motion field store");
     g_err.clear();
     if (n < 0 || (n > 0 && !jobs)) return fail(AV1G_EINVAL, "bad job array");
     if (n == 0) return AV1G_OK;
@@ -507,6 +514,7 @@ av1g_status av1g_run_mf_store(const av1g_mf_store_job* jobs, int32_t n, void* st
     return st;
 }
 av1g_status av1g_run_mf_project(const av1g_mf_project_job* jobs, int32_t n, void* stream) {
+    NvtxRange range("av1g motion field projection");
     g_err.clear();
     if (n < 0 || (n > 0 && !jobs)) return fail(AV1G_EINVAL, "bad job array");
     if (n == 0) return AV1G_OK;
@@ -516,6 +524,7 @@ av1g_status av1g_run_mf_project(const av1g_mf_project_job* jobs, int32_t n, void
     return st;
 }
 av1g_status av1g_run_tile_list_output(const av1g_tile_list_job* jobs, int32_t n, void* stream) {
+    NvtxRange range("av1g tile list output");
     g_err.clear();
     if (n < 0 || (n > 0 && !jobs)) return fail(AV1G_EINVAL, "bad job array");
     if (n == 0) return AV1G_OK;

@@ -13,10 +13,20 @@
 #include <functional>
 #include <string>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "av1g.h"
 
 namespace av1g {
+
+// An NVTX range over a host scope (a stage's planning and launches), so that
+// a profiler's timeline shows each stage by name; free when no tool listens.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 constexpr int kSMs = 148;  // B200
 

@@ -21,6 +21,8 @@
 #include <thread>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "av1g.h"
 #include "walker.h"
 
@@ -263,7 +265,9 @@ av1g_status decode_frame(av1g_decoder* d, const av1g_parsed_frame_header& fh, co
         fo = keep.get();
     }
     std::string err;
+    nvtxRangePushA("av1g tile walk");
     av1g_status st = av1w::walk_frame(d->seq, fh, d->refs, d->slots, tiles, *fo, err);
+    nvtxRangePop();
     if (st != AV1G_OK) return dfail(st, err);
     if (!fo->tiles_in_sync) d->frames_out_of_sync++;
     if (av1g_status s2 = submit(d, fh, fo, pts)) return s2;

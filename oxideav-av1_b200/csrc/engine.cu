@@ -337,6 +337,7 @@ void run_stage(std::vector<Work*>& ws, std::vector<Job>& jobs, Fn fn, cudaStream
 
 void enqueue_step(av1g_engine* E, cudaStream_t cs, std::vector<std::shared_ptr<Ticket>>& batch, Step& step,
                   double part_ms[6]) {
+    NvtxRange range("av1g engine step");
     auto tp = Clock::now();
     auto lap = [&](int k) {
         auto now = Clock::now();

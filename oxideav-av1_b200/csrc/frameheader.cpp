@@ -426,7 +426,7 @@ void global_motion(Reader& r, const av1g_ref_state& st, av1g_parsed_frame_header
         const int sub = (idx % 3) == 2 ? 1 << prec_bits : 0;
         const int mx = 1 << abs_bits;
         const int rr = (prev[ref][idx] >> prec_diff) - sub;
-        h.gm_params[ref][idx] = (decode_signed_subexp_with_ref(r, -mx, mx + 1, rr) << prec_diff) + round;
+        h.gm_params[ref][idx] = decode_signed_subexp_with_ref(r, -mx, mx + 1, rr) * (1 << prec_diff) + round;
     };
     for (int ref = LAST; ref <= ALTREF; ref++) {
         int type = IDENTITY;

@@ -957,7 +957,7 @@ void Walker::read_delta_qindex() {
     if (a) {
         int sign = L(1);
         int red = sign ? -a : a;
-        CurrentQIndex = clip3(1, 255, CurrentQIndex + (red << fh.delta_q_res));
+        CurrentQIndex = clip3(1, 255, CurrentQIndex + red * (1 << fh.delta_q_res));
     }
 }
 
@@ -978,7 +978,7 @@ void Walker::read_delta_lf() {
         if (a) {
             int sign = L(1);
             int red = sign ? -a : a;
-            DeltaLF[i] = clip3(-63, 63, DeltaLF[i] + (red << fh.delta_lf_res));
+            DeltaLF[i] = clip3(-63, 63, DeltaLF[i] + red * (1 << fh.delta_lf_res));
         }
     }
 }
