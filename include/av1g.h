@@ -359,9 +359,25 @@ typedef struct av1g_intra_job {
  * intra_predict_block_samples (cdf.rs:16990-17250), the kernels at
  * cdf.rs:1348-3120 and predict_chroma_from_luma_into_curr_frame
  * (cdf.rs:17256) as called from transform_block_emit (cdf.rs:32482).
- * Superblocks run as a wavefront (level = column + 2 * row): one launch per
- * level across all frames, each superblock's TUs in decode order. */
+ * One persistent launch for all frames: the host plan records, per
+ * superblock, which levels of which earlier superblocks its TUs read (the
+ * edges and copies the TUs' availability flags and vectors name), and a
+ * superblock waits only for those, so superblocks of different tiles (whose
+ * TUs read nothing across the tile edge) run side by side. */
 av1g_status av1g_run_intra(const av1g_intra_job* jobs, int32_t n, void* stream);
+
+/* The plan av1g_run_intra would build for these jobs, without running it
+ * (host only; the jobs' device pointers are not read).  depth: superblocks
+ * on the longest chain of waits; width: most superblocks at one depth. */
+typedef struct av1g_intra_plan_stats {
+    int32_t superblocks;
+    int32_t tus;
+    int32_t waits;
+    int32_t depth;
+    int32_t width;
+    int32_t pad;
+} av1g_intra_plan_stats;
+av1g_status av1g_intra_plan_stats_get(const av1g_intra_job* jobs, int32_t n, av1g_intra_plan_stats* out);
 
 /* Test hook for the wait bound above, on the current device: wait_ns sets
  * the bound (<= 0 restores 2 s) and, while frame_width > 0, every intra job
@@ -1159,7 +1175,10 @@ av1g_status av1g_run_film_grain(const av1g_frame_job* jobs, int32_t n, void* str
 /* The whole §7.4 chain of frame_driver.rs:830-1096 for `n` jobs:
  * deblock, CDEF, superres, loop restoration, film grain, with the
  * reference's gating.  mode = AV1G_MODE_BATCHED or AV1G_MODE_PER_FRAME.
- * *launches (optional) receives the number of kernels launched. */
+ * *launches (optional) receives the number of stage kernels launched; the
+ * frame records of a batch up to 32 KB (about 28 frames) travel as the
+ * parameters of one small store kernel per 16 KB (no copy engine), larger
+ * ones by a copy. */
 av1g_status av1g_run_postfilter(const av1g_frame_job* jobs, int32_t n, int32_t mode,
                                 void* stream, int32_t* launches);
 
@@ -1212,7 +1231,10 @@ av1g_status av1g_chain_graph_destroy(av1g_chain_graph* g);
  * AV1G_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
  * exit.  The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture.  At most AV1G_NOALLOC_MAX_FRAMES jobs per call,
+ * before any stream capture.  The address is kept per device ordinal for the
+ * life of the process, so calls must run in the device's primary context
+ * (the CUDA runtime's default) and not after cudaDeviceReset.  At most
+ * AV1G_NOALLOC_MAX_FRAMES jobs per call,
  * and the batch's scratch must fit the array; larger requests return
  * AV1G_EINVAL with a message naming the limit.  All calls on a device share
  * the array: calls that overlap on the GPU race on it. */

@@ -125,6 +125,11 @@ class IntraJob(C.Structure):
                 ("palette_maps", C.c_void_p), ("palette_map_bytes", C.c_int64), ("interintra_in", Plane * 3)]
 
 
+class IntraPlanStats(C.Structure):
+    _fields_ = [("superblocks", C.c_int32), ("tus", C.c_int32), ("waits", C.c_int32), ("depth", C.c_int32),
+                ("width", C.c_int32), ("pad", C.c_int32)]
+
+
 class RefFrame(C.Structure):
     _fields_ = [("planes", Plane * 3), ("upscaled_width", C.c_int32), ("frame_height", C.c_int32)]
 
@@ -372,6 +377,7 @@ _STRUCTS = {"av1g_film_grain": FilmGrain, "av1g_frame_header": FrameHeader, "av1
             "av1g_mi_grid": MiGrid, "av1g_plane": Plane, "av1g_frame_job": FrameJob,
             "av1g_quant_params": QuantParams, "av1g_tu": Tu, "av1g_recon_job": ReconJob,
             "av1g_intra_tu": IntraTu, "av1g_intra_job": IntraJob, "av1g_ref_frame": RefFrame,
+            "av1g_intra_plan_stats": IntraPlanStats,
             "av1g_warp_ctx": WarpCtx, "av1g_obmc_neighbour": ObmcNeighbour, "av1g_inter_pred": InterPred,
             "av1g_inter_job": InterJob, "av1g_warp_sample": WarpSample, "av1g_config": Config,
             "av1g_seq_info": SeqInfo, "av1g_frame_desc": FrameDesc, "av1g_frame_out": FrameOut,
@@ -475,6 +481,7 @@ _SIGS = {
     "av1g_decoder_host_ms": (C.c_double, [C.c_void_p]),
     "av1g_decoder_frames_out_of_sync": (C.c_int32, [C.c_void_p]),
     "av1g_test_intra_wait_fault": (C.c_int, [C.c_int64, C.c_int32]),
+    "av1g_intra_plan_stats_get": (C.c_int, [C.POINTER(IntraJob), C.c_int32, C.POINTER(IntraPlanStats)]),
 }
 
 NOALLOC_MAX_FRAMES = 16

@@ -339,7 +339,9 @@ av1g_status run(const av1g_frame_job* jobs, int n, int stage_mask, int mode, voi
     cudaError_t e = cudaMallocAsync((void**)&dev, P.total_bytes, s);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
     bind(P, dev);
-    e = upload(dev, P.host.data(), P.off_scratch, s);
+    // the prefix is 256-byte aligned; one or two launches carry a small one
+    e = P.off_scratch <= 2 * kUploadChunk ? upload_by_launch(dev, P.host.data(), P.off_scratch, s)
+                                          : upload(dev, P.host.data(), P.off_scratch, s);
     if (e != cudaSuccess) {
         cudaFreeAsync(dev, s);
         return cuda_fail(e, "cudaMemcpyAsync");
@@ -402,6 +404,7 @@ int32_t av1g_struct_size(const char* name) {
     if (!strcmp(name, "av1g_tu")) return (int32_t)sizeof(av1g_tu);
     if (!strcmp(name, "av1g_recon_job")) return (int32_t)sizeof(av1g_recon_job);
     if (!strcmp(name, "av1g_intra_tu")) return (int32_t)sizeof(av1g_intra_tu);
+    if (!strcmp(name, "av1g_intra_plan_stats")) return (int32_t)sizeof(av1g_intra_plan_stats);
     if (!strcmp(name, "av1g_intra_job")) return (int32_t)sizeof(av1g_intra_job);
     if (!strcmp(name, "av1g_ref_frame")) return (int32_t)sizeof(av1g_ref_frame);
     if (!strcmp(name, "av1g_warp_ctx")) return (int32_t)sizeof(av1g_warp_ctx);

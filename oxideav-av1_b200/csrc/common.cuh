@@ -85,6 +85,12 @@ __device__ __forceinline__ int floor_log2u(unsigned x) { return x ? 31 - __clz(x
 // (returns once enqueued; the host bytes may be reused immediately).
 cudaError_t upload(void* dev, const void* host, size_t n, cudaStream_t s);
 cudaError_t upload_with(void* dev, size_t n, cudaStream_t s, const std::function<void(uint8_t*)>& fill);
+// Writes n bytes (a multiple of 16, dev 16-byte aligned) by kernel launches
+// that carry the bytes as their parameters, kUploadChunk bytes per launch:
+// no copy engine, so a small record upload on a compute stream never queues
+// behind large copies another stream has on the copy engines.
+constexpr size_t kUploadChunk = 16384;
+cudaError_t upload_by_launch(void* dev, const void* host, size_t n, cudaStream_t s);
 
 __device__ __forceinline__ int ld_px(const PlaneDev& P, int hbd, int y, int x) {
     const uint8_t* row = P.p + (size_t)y * P.stride;

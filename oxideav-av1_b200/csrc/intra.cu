@@ -1065,6 +1065,18 @@ av1g_status intra_run(const av1g_intra_job* jobs, int n, cudaStream_t st, std::s
 
 }  // namespace av1g
 
+extern "C" av1g_status av1g_intra_plan_stats_get(const av1g_intra_job* jobs, int32_t n,
+                                                  av1g_intra_plan_stats* out) {
+    if (!out || n < 0 || (n > 0 && !jobs)) return AV1G_EINVAL;
+    av1g::IntraPlan plan;
+    std::string err;
+    av1g_status rc = av1g::intra_plan(jobs, n, plan, err);
+    if (rc != AV1G_OK) return rc;
+    *out = av1g_intra_plan_stats{(int32_t)plan.items.size(), (int32_t)plan.tus.size(), (int32_t)plan.waits.size(),
+                                 plan.depth, plan.width, 0};
+    return AV1G_OK;
+}
+
 extern "C" av1g_status av1g_test_intra_wait_fault(int64_t wait_ns, int32_t frame_width) {
     long long ns = wait_ns > 0 ? (long long)wait_ns : av1g::kWaitNs;
     cudaError_t e = cudaMemcpyToSymbol(av1g::g_wait_ns, &ns, sizeof ns);

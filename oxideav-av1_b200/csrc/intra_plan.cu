@@ -439,6 +439,7 @@ av1g_status intra_plan(const av1g_intra_job* jobs, int n, IntraPlan& plan, std::
     for (size_t q = 0, run = 0; q < claim.size(); q++) {
         run = (q > 0 && sbs_all[claim[q]].depth == sbs_all[claim[q - 1]].depth) ? run + 1 : 1;
         plan.width = std::max(plan.width, (int)run);
+        plan.depth = std::max(plan.depth, sbs_all[claim[q]].depth + 1);
     }
     // the levels some superblock waits for are published (progress z means
     // z levels done: published after level z - 1)

@@ -49,6 +49,7 @@ struct IntraPlan {
     std::vector<int4> waits;            // before level x, superblock y has finished z levels
     size_t cache_bytes = 0;             // the largest superblock copy (all planes, u16)
     int width = 0;                      // most superblocks at one dependency depth
+    int depth = 0;                      // dependency depths (the critical path in superblocks)
 };
 
 // Validates the jobs and builds the plan.  AV1G_OK with no items when there

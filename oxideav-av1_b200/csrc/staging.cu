@@ -127,4 +127,26 @@ cudaError_t upload(void* dev, const void* host, size_t n, cudaStream_t s) {
     return upload_with(dev, n, s, [&](uint8_t* p) { memcpy(p, host, n); });
 }
 
+namespace {
+struct ParamChunk {
+    uint4 w[kUploadChunk / 16];
+};
+__global__ void __launch_bounds__(256) param_store_kernel(const __grid_constant__ ParamChunk c, uint4* dst, int nvec) {
+    for (int i = threadIdx.x; i < nvec; i += blockDim.x) dst[i] = c.w[i];
+}
+}  // namespace
+
+cudaError_t upload_by_launch(void* dev, const void* host, size_t n, cudaStream_t s) {
+    if ((n & 15) || (reinterpret_cast<uintptr_t>(dev) & 15)) return cudaErrorInvalidValue;
+    ParamChunk c;
+    const uint8_t* src = static_cast<const uint8_t*>(host);
+    uint4* dst = static_cast<uint4*>(dev);
+    for (size_t off = 0; off < n; off += kUploadChunk) {
+        const size_t len = n - off < kUploadChunk ? n - off : kUploadChunk;
+        memcpy(c.w, src + off, len);
+        param_store_kernel<<<1, 256, 0, s>>>(c, dst + off / 16, static_cast<int>(len / 16));
+    }
+    return cudaGetLastError();
+}
+
 }  // namespace av1g

@@ -460,15 +460,32 @@ def _blocks(rng, x0, y0, n, pw, ph, out, split=0.55):
         out.append((x0, y0, n, n))
 
 
+def tile_grid(mi_rows, mi_cols, sb_size, tile_cols_log2=0, tile_rows_log2=0):
+    """Uniformly spaced tiles (§5.9.15 with uniform_tile_spacing_flag): the
+    luma-sample edges [x0, x1) and [y0, y1) of the tile columns and rows."""
+    sb_cols = -(-mi_cols * 4 // sb_size)
+    sb_rows = -(-mi_rows * 4 // sb_size)
+
+    def edges(n_sb, log2, limit):
+        step = (n_sb + (1 << log2) - 1) >> log2
+        xs = list(range(0, n_sb, step)) + [n_sb]
+        return [(a * sb_size, min(b * sb_size, limit)) for a, b in zip(xs[:-1], xs[1:])]
+    return edges(sb_cols, tile_cols_log2, mi_cols * 4), edges(sb_rows, tile_rows_log2, mi_rows * 4)
+
+
 def make_intra_frame(seed, width=176, height=144, bit_depth=8, ssx=1, ssy=1, mono=False, sb_size=64,
-                     edge_filter=True, palette=0.0, intrabc=0.0, intrabc_order="wavefront", split=0.55):
+                     edge_filter=True, palette=0.0, intrabc=0.0, intrabc_order="wavefront", split=0.55, tiles=(0, 0)):
     """Intra TUs in decode order.  palette / intrabc: probability that a block
     is a palette block / an intra-block-copy block; split: probability of a
     quad split in the block partition.  intrabc_order picks where
     copies read from: "wavefront" (the superblock row above, within reach of
     the level-2 wavefront), "steep" (further right in the row above, which
     needs a steeper wavefront) or "raster" (the row below, not yet decoded,
-    which only decode order reproduces)."""
+    which only decode order reproduces).  tiles = (tile_cols_log2,
+    tile_rows_log2): superblocks in tile order, and the edge availability of
+    every TU bounded by its tile as the tile walker sets it (AvailU / AvailL
+    and the above-right / below-left tests stop at the tile edge); intra
+    block copies then stay off."""
     rng = np.random.default_rng(seed)
     base = make_recon_frame(seed + 1000, width, height, bit_depth, ssx, ssy, mono)
     f = IntraFrame()
@@ -482,11 +499,18 @@ def make_intra_frame(seed, width=176, height=144, bit_depth=8, ssx=1, ssy=1, mon
     decoded = [np.zeros(((f.plane_dims(p)[0] + 3) // 4, (f.plane_dims(p)[1] + 3) // 4), bool)
                for p in range(h.num_planes)]
     lossless_seg = [s for s in range(8) if f.quant.lossless[s]]
-    for sby in range(0, h.mi_rows * 4, sb_size):
-        for sbx in range(0, h.mi_cols * 4, sb_size):
+    tcols, trows = tile_grid(h.mi_rows, h.mi_cols, sb_size, *tiles)
+    if tiles != (0, 0):
+        intrabc = 0.0
+    order = [(ty0, ty1, tx0, tx1, sby, sbx) for (ty0, ty1) in trows for (tx0, tx1) in tcols
+             for sby in range(ty0, ty1, sb_size) for sbx in range(tx0, tx1, sb_size)]
+    for (ty0, ty1, tx0, tx1, sby, sbx) in order:
+        if True:
             for p in range(h.num_planes):
                 sx_, sy_ = (h.subsampling_x, h.subsampling_y) if p else (0, 0)
                 ph, pw = f.plane_dims(p)
+                # the tile in this plane's samples
+                tpx0, tpx1, tpy0, tpy1 = tx0 >> sx_, min(tx1 >> sx_, pw), ty0 >> sy_, min(ty1 >> sy_, ph)
                 blocks = []
                 _blocks(rng, sbx >> sx_, sby >> sy_, sb_size >> max(sx_, sy_), pw, ph, blocks, split)
                 for (bx, by, bw, bh) in blocks:
@@ -542,14 +566,16 @@ def make_intra_frame(seed, width=176, height=144, bit_depth=8, ssx=1, ssy=1, mon
                             if ty >= ph or tx_ >= pw:
                                 continue
                             flags = 0
-                            if ty > 0:
+                            if ty > tpy0:
                                 flags |= abi.INTRA_HAVE_ABOVE
-                            if tx_ > 0:
+                            if tx_ > tpx0:
                                 flags |= abi.INTRA_HAVE_LEFT
                             cy, cx = ty // 4, tx_ // 4
-                            if cy > 0 and (tx_ + tw) // 4 < decoded[p].shape[1] and decoded[p][cy - 1, (tx_ + tw) // 4]:
+                            if ty > tpy0 and tx_ + tw < tpx1 and (tx_ + tw) // 4 < decoded[p].shape[1] and \
+                                    decoded[p][cy - 1, (tx_ + tw) // 4]:
                                 flags |= abi.INTRA_HAVE_ABOVE_RIGHT
-                            if cx > 0 and (ty + th) // 4 < decoded[p].shape[0] and decoded[p][(ty + th) // 4, cx - 1]:
+                            if tx_ > tpx0 and ty + th < tpy1 and (ty + th) // 4 < decoded[p].shape[0] and \
+                                    decoded[p][(ty + th) // 4, cx - 1]:
                                 flags |= abi.INTRA_HAVE_BELOW_LEFT
                             if edge_filter:
                                 flags |= abi.INTRA_EDGE_FILTER
@@ -904,12 +930,13 @@ def _intra_tus_for_blocks(rng, h, quant, blocks, sb_size, coeff_base):
 
 
 def make_stream(seed, n_frames=4, width=176, height=144, bit_depth=8, ssx=1, ssy=1, mono=False, superres_denom=8,
-                film_grain=False, sb_size=64, show_existing_at=(), palette=0.1):
+                film_grain=False, sb_size=64, show_existing_at=(), palette=0.1, tiles=(0, 0)):
     """A key frame (intra TUs, palette blocks) then inter frames (inter calls
     over a random partition with some intra blocks, residual TUs), each with
     the post-filter side data of make_frame, random references among the
     eight slots and random refresh flags.  Frames listed in show_existing_at
-    are show_existing_frame outputs of a random slot instead."""
+    are show_existing_frame outputs of a random slot instead.  tiles: the
+    key frame's tile grid (make_intra_frame)."""
     rng = np.random.default_rng(seed)
     frames = []
     for k in range(n_frames):
@@ -928,7 +955,7 @@ def make_stream(seed, n_frames=4, width=176, height=144, bit_depth=8, ssx=1, ssy
         fr = StreamFrame()
         fr.hdr, fr.grid, fr.cdef_idx, fr.lr_units = h, base.grid, base.cdef_idx, base.lr_units
         if k == 0:
-            it = make_intra_frame(fs, fw, height, bit_depth, ssx, ssy, mono, sb_size, palette=palette)
+            it = make_intra_frame(fs, fw, height, bit_depth, ssx, ssy, mono, sb_size, palette=palette, tiles=tiles)
             fr.quant, fr.intra_tus, fr.coeffs, fr.palette_maps = it.quant, it.tus, it.coeffs, it.palette_maps
             fr.refresh = 0xFF
         else:

@@ -52,3 +52,10 @@ def test_empty_batch_is_ok_without_device():
     lib = abi.load()
     assert lib.av1g_run_postfilter(None, 0, 0, None, None) == abi.AV1G_OK
     assert lib.av1g_run_postfilter(None, -1, 0, None, None) == abi.AV1G_EINVAL
+
+
+def test_noalloc_limits_match_the_header():
+    text = (ROOT / "include" / "av1g.h").read_text()
+    defs = dict(re.findall(r"#define\s+(AV1G_NOALLOC_[A-Z_]+)\s+(.+)", text))
+    assert eval(defs["AV1G_NOALLOC_MAX_FRAMES"], {}) == abi.NOALLOC_MAX_FRAMES
+    assert eval(defs["AV1G_NOALLOC_SCRATCH_BYTES"], {}) == abi.NOALLOC_SCRATCH_BYTES

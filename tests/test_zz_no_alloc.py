@@ -18,6 +18,7 @@ import pytest
 
 torch = pytest.importorskip("torch")
 
+import oracle  # noqa: E402
 from oxideav_av1_b200 import abi, postfilter, synth  # noqa: E402
 
 pytestmark = pytest.mark.gpu
@@ -50,6 +51,41 @@ def _assert_same(a, b):
             assert len(d) == 0, f"plane {p}: {len(d)} samples differ, first at {tuple(d[0])}"
 
 
+def _assert_oracle(frames, b):
+    """The grain stage's input here is the cropped reconstruction (every
+    other stage is off); oracle.film_grain restates film_grain_synthesis."""
+    for f, fb in zip(frames, b):
+        crop = [np.ascontiguousarray(f.recon[p][: f.out_dims(p)[0], : f.out_dims(p)[1]]).astype(np.int32)
+                for p in range(f.hdr.num_planes)]
+        want = oracle.film_grain(f, crop)
+        for p, (g, e) in enumerate(zip(fb.download("out"), want)):
+            assert np.array_equal(g.astype(np.int64), e), f"plane {p} differs from the oracle"
+
+
+# The default memory pool of the current device (the stream-ordered allocator
+# the allocating entry points draw from), read through the driver API:
+# CU_MEMPOOL_ATTR_USED_MEM_CURRENT = 7, CU_MEMPOOL_ATTR_USED_MEM_HIGH = 8.
+def _pool():
+    cu = C.CDLL("libcuda.so.1")
+    dev, pool = C.c_int(), C.c_void_p()
+    assert cu.cuDeviceGet(C.byref(dev), C.c_int(torch.cuda.current_device())) == 0
+    assert cu.cuDeviceGetDefaultMemPool(C.byref(pool), dev) == 0
+    return cu, pool
+
+
+def _pool_attr(attr):
+    cu, pool = _pool()
+    v = C.c_uint64()
+    assert cu.cuMemPoolGetAttribute(pool, C.c_int(attr), C.byref(v)) == 0
+    return v.value
+
+
+def _reset_pool_high():
+    cu, pool = _pool()
+    zero = C.c_uint64(0)  # resets the high-water mark to the current use
+    assert cu.cuMemPoolSetAttribute(pool, C.c_int(8), C.byref(zero)) == 0
+
+
 def test_noalloc_film_grain_matches_allocating_entry_point_twice():
     first = _batch([dict(seed=301, width=352, height=288), dict(seed=302, width=200, height=120, bit_depth=10),
                     dict(seed=303, width=130, height=70, ssx=0, ssy=0)])
@@ -62,6 +98,28 @@ def test_noalloc_film_grain_matches_allocating_entry_point_twice():
                      dict(seed=307, width=1920, height=1080)])
     a, b = _run_both(second)
     _assert_same(a, b)
+    _assert_oracle(second, b)
+
+
+def test_noalloc_draws_nothing_from_the_device_memory_pool():
+    lib = abi.load()
+    sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    frames = _batch([dict(seed=320, width=640, height=360), dict(seed=321, width=320, height=240, bit_depth=10)])
+    b = [postfilter.DeviceFrame(f) for f in frames]
+    jb = postfilter.jobs_array(b)
+    abi.check(lib.av1g_run_film_grain_noalloc(jb, len(b), sp))   # first call on the device: symbol address
+    torch.cuda.synchronize()
+    used = _pool_attr(7)
+    _reset_pool_high()
+    abi.check(lib.av1g_run_film_grain_noalloc(jb, len(b), sp))
+    torch.cuda.synchronize()
+    assert _pool_attr(8) == used, "the allocation-free entry point allocated from the memory pool"
+    _assert_oracle(frames, b)
+    # the allocating entry point does draw from the same pool: the probe sees allocations
+    a = [postfilter.DeviceFrame(f) for f in frames]
+    abi.check(lib.av1g_run_film_grain(postfilter.jobs_array(a), len(a), sp))
+    torch.cuda.synchronize()
+    assert _pool_attr(8) > used
 
 
 def test_noalloc_rejects_batches_beyond_its_limit():
