@@ -109,16 +109,18 @@ __device__ __forceinline__ Taps taps_of(const int16_t* toff, int dir) {
 }
 
 // One tap pair (+o and -o) of weight w: constrain (cdef.rs:592-606) with the
-// damping shift precomputed, accumulated into sum; min / max of the samples
-// taken (the reference's clip range, cdef.rs:540-560).
-template <bool BORDER>
+// damping shift precomputed, accumulated into sum; with MINMAX, min / max of
+// the samples taken (the reference's clip range, cdef.rs:540-560).
+template <bool BORDER, bool MINMAX>
 __device__ __forceinline__ void tap2(const int16_t* c, int o, int xv, int w, int thr, int adj, int& sum, int& mn,
                                      int& mx) {
     if (!BORDER) {  // both taps available: one weight product, three-input min / max
         const int x0 = c[o], x1 = c[-o];
         sum += w * (constrain_adj(x0 - xv, thr, adj) + constrain_adj(x1 - xv, thr, adj));
-        mx = __vimax3_s32(mx, x0, x1);
-        mn = __vimin3_s32(mn, x0, x1);
+        if (MINMAX) {
+            mx = __vimax3_s32(mx, x0, x1);
+            mn = __vimin3_s32(mn, x0, x1);
+        }
         return;
     }
 #pragma unroll
@@ -126,22 +128,55 @@ __device__ __forceinline__ void tap2(const int16_t* c, int o, int xv, int w, int
         const int x = s ? c[-o] : c[o];
         if (x == NA) continue;
         sum += w * constrain_adj(x - xv, thr, adj);
-        mx = max(mx, x);
-        mn = min(mn, x);
+        if (MINMAX) {
+            mx = max(mx, x);
+            mn = min(mn, x);
+        }
     }
 }
 
-template <bool BORDER>
+// One sample of cdef_filter (cdef.rs:465-590).  MODE 3: primary and
+// secondary taps, clipped to the taps' range as the reference always does.
+// MODE 1 / 2: only the primary / only the secondary strength is non-zero;
+// the taps of a zero strength add nothing (constrain with threshold 0 is 0)
+// and the clip is the identity, so both are left out: the remaining taps'
+// weights sum to 12 (2 x (4 + 2), 2 x (3 + 3), or 2 x 2 x (2 + 1)), each
+// constrained difference has its tap's sign and at most its magnitude, so
+// with D the largest positive difference sum <= 12 D and
+// (8 + sum) >> 4 <= D (and symmetrically below): x + offset stays inside
+// [min, max] of the taps, and the unclipped value is the clipped one.
+template <bool BORDER, int MODE>
 __device__ __forceinline__ int filter_px(const int16_t* c, int xv, const Taps& T, int pri, int sec, int padj,
                                          int sadj, int pt0, int pt1) {
+    constexpr bool MM = MODE == 3;
     int sum = 0, mx = xv, mn = xv;
-    tap2<BORDER>(c, T.p0, xv, pt0, pri, padj, sum, mn, mx);
-    tap2<BORDER>(c, T.p1, xv, pt1, pri, padj, sum, mn, mx);
-    tap2<BORDER>(c, T.a0, xv, 2, sec, sadj, sum, mn, mx);
-    tap2<BORDER>(c, T.b0, xv, 2, sec, sadj, sum, mn, mx);
-    tap2<BORDER>(c, T.a1, xv, 1, sec, sadj, sum, mn, mx);
-    tap2<BORDER>(c, T.b1, xv, 1, sec, sadj, sum, mn, mx);
-    return clip3(mn, mx, xv + ((8 + sum - (sum < 0)) >> 4));
+    if (MODE & 1) {
+        tap2<BORDER, MM>(c, T.p0, xv, pt0, pri, padj, sum, mn, mx);
+        tap2<BORDER, MM>(c, T.p1, xv, pt1, pri, padj, sum, mn, mx);
+    }
+    if (MODE & 2) {
+        tap2<BORDER, MM>(c, T.a0, xv, 2, sec, sadj, sum, mn, mx);
+        tap2<BORDER, MM>(c, T.b0, xv, 2, sec, sadj, sum, mn, mx);
+        tap2<BORDER, MM>(c, T.a1, xv, 1, sec, sadj, sum, mn, mx);
+        tap2<BORDER, MM>(c, T.b1, xv, 1, sec, sadj, sum, mn, mx);
+    }
+    const int y = xv + ((8 + sum - (sum < 0)) >> 4);
+    return MM ? clip3(mn, mx, y) : y;
+}
+
+template <bool BORDER>
+__device__ __forceinline__ void filter_two(const int16_t* cp, int xv0, int xv1, const Taps& T, int pri, int sec,
+                                           int padj, int sadj, int pt0, int pt1, int& out0, int& out1) {
+    if (pri && sec) {
+        out0 = filter_px<BORDER, 3>(cp, xv0, T, pri, sec, padj, sadj, pt0, pt1);
+        out1 = filter_px<BORDER, 3>(cp + 1, xv1, T, pri, sec, padj, sadj, pt0, pt1);
+    } else if (pri) {
+        out0 = filter_px<BORDER, 1>(cp, xv0, T, pri, sec, padj, sadj, pt0, pt1);
+        out1 = filter_px<BORDER, 1>(cp + 1, xv1, T, pri, sec, padj, sadj, pt0, pt1);
+    } else if (sec) {
+        out0 = filter_px<BORDER, 2>(cp, xv0, T, pri, sec, padj, sadj, pt0, pt1);
+        out1 = filter_px<BORDER, 2>(cp + 1, xv1, T, pri, sec, padj, sadj, pt0, pt1);
+    }
 }
 
 __global__ void __launch_bounds__(kCdefThreads, 4) cdef_kernel(const FrameDev* __restrict__ frames,
@@ -333,13 +368,8 @@ __global__ void __launch_bounds__(kCdefThreads, 4) cdef_kernel(const FrameDev* _
                     const int padj = p ? padj_uv : b.padj_y;
                     const Taps T = taps_of(toff, p ? b.uvdir : b.ydir);
                     const int prow = (pri >> cs) & 1, pt0 = prow ? 3 : 4, pt1 = prow ? 3 : 2;
-                    if (border) {
-                        out0 = filter_px<true>(cp, xv0, T, pri, sec, padj, sadj, pt0, pt1);
-                        out1 = filter_px<true>(cp + 1, xv1, T, pri, sec, padj, sadj, pt0, pt1);
-                    } else {
-                        out0 = filter_px<false>(cp, xv0, T, pri, sec, padj, sadj, pt0, pt1);
-                        out1 = filter_px<false>(cp + 1, xv1, T, pri, sec, padj, sadj, pt0, pt1);
-                    }
+                    if (border) filter_two<true>(cp, xv0, xv1, T, pri, sec, padj, sadj, pt0, pt1, out0, out1);
+                    else filter_two<false>(cp, xv0, xv1, T, pri, sec, padj, sadj, pt0, pt1, out0, out1);
                 }
                 if (gx + 1 < dw) {  // gx is even: one aligned 2- or 4-byte store
                     uint8_t* row = D.p + (size_t)gy * D.stride;
