@@ -705,19 +705,23 @@ def stream_frame(tpl, k):
 
 
 def _fetch_digest(lib, h, ticket):
-    """(status, SHA-256 of the frame's planes, latency ms); the digest is
-    taken on the engine's pinned output buffer, then the ticket is freed."""
-    import hashlib
+    """(status, digest of the frame's planes, latency ms); the digest (CRC-32
+    and byte length of each plane: an equality check between two decodes of
+    the same stream, at ~4 GB/s per client thread so that checking does not
+    bound the measured rate) is taken on the engine's pinned output buffer,
+    then the ticket is freed."""
+    import zlib
     o = abi.FrameOut()
     st = lib.av1g_fetch_output(h, ticket, C.byref(o))
-    m = hashlib.sha256()
+    dg = []
     if st == abi.AV1G_OK and o.shown:
         for p in range(o.num_planes):
             pl = o.planes[p]
-            m.update(memoryview((C.c_uint8 * (pl.stride * pl.height)).from_address(pl.data)))
+            n = pl.stride * pl.height
+            dg.append((zlib.crc32(memoryview((C.c_uint8 * n).from_address(pl.data))), n))
     lat = o.latency_ms
     lib.av1g_release_output(h, ticket)
-    return st, m.hexdigest(), lat
+    return st, tuple(dg), lat
 
 
 def drive(eng, templates, sbs, streams, clients=8, window=2):
@@ -733,6 +737,7 @@ def drive(eng, templates, sbs, streams, clients=8, window=2):
     hs = [eng.open_stream(synth.stream_seq(templates[t], sbs[t])) for t, _ in streams]
     assert all(h is not None for h in hs), "budget too small for the stream set"
     groups = [list(range(g, len(streams), clients)) for g in range(min(clients, len(streams)))]
+    failures = []  # (stream, frame, poll result, fetch status)
 
     def client(group):
         inflight = deque()
@@ -744,7 +749,9 @@ def drive(eng, templates, sbs, streams, clients=8, window=2):
             i, t = inflight.popleft()
             r = eng.poll(t, 300.0)
             st, dg, lat = _fetch_digest(lib, hs[i].h, t)
-            ok &= r == abi.AV1G_OK and st == abi.AV1G_OK
+            if r != abi.AV1G_OK or st != abi.AV1G_OK:
+                ok = False
+                failures.append((i, len(digests[i]), r, st))
             digests[i].append(dg)
             lats.append(lat)
 
@@ -781,6 +788,9 @@ def drive(eng, templates, sbs, streams, clients=8, window=2):
         digests.update(d)
         lats += l
         ok &= o
+    if failures:
+        sys.stderr.write(f"drive: {len(failures)} frames failed, first {failures[:4]}: "
+                         f"{lib.av1g_last_error().decode(errors='replace')}\n")
     return sum(n for _, n in streams) / dt, [digests[i] for i in range(len(streams))], lats, ok
 
 
@@ -823,7 +833,7 @@ def run_batching(args, local):
     launch path), both on the same number of lanes (worker threads with
     their own CUDA streams) and the same 8 client threads, so the ratio is
     the batching alone.  Every stream's output must equal its template
-    decoded alone (SHA-256 per frame)."""
+    decoded alone (a CRC-32 of every plane of every frame)."""
     from oxideav_av1_b200 import engine
     rng = np.random.default_rng(11)
     specs, sbs = [], []
@@ -854,7 +864,8 @@ def run_batching(args, local):
                         f"cycles its template's inter frames",
            "template_generation_s": gen_s,
            "timing": "host wall clock, first submit to last fetch; 8 client threads each owning a group of streams "
-                     "(at most 2 frames of a stream in flight), digests of every output frame taken by the clients",
+                     "(at most 2 frames of a stream in flight), a CRC-32 per plane of every output frame taken by "
+                     "the clients",
            **_host_info()}
     warm = [(t, 3) for t in range(len(templates))]
     ok_all = True

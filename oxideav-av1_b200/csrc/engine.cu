@@ -93,9 +93,13 @@ struct Ticket {
     // host copy of the descriptor
     av1g_frame_header hdr = {};
     av1g_quant_params quant = {};
-    std::vector<uint8_t> grid[9];
-    std::vector<int8_t> cdef_idx;
-    std::vector<av1g_lr_unit> lr_units[3];
+    // the device-bound arrays (grids 0-8, CDEF indices 9, LR units 10-12,
+    // coefficients 13), laid out at submit in one pinned block that the
+    // frame's step copies to its allocation with one cudaMemcpyAsync; the
+    // block goes back to the pool when that step has finished
+    uint8_t* blob = nullptr;
+    size_t blob_bytes = 0;
+    size_t blob_off[14] = {}, blob_len[14] = {};
     std::vector<av1g_inter_pred> preds;
     std::vector<av1g_obmc_neighbour> nbs;
     std::vector<av1g_warp_ctx> warps;
@@ -122,6 +126,7 @@ struct Step {
     // order) and the ticket of each of its jobs
     int32_t* intra_status = nullptr;
     std::vector<std::shared_ptr<Ticket>> intra_tickets;
+    std::vector<uint8_t*> blobs;  // the frames' pinned descriptor blocks
     size_t work_bytes = 0;
     Clock::time_point t_enqueued;
 };
@@ -236,23 +241,10 @@ int lr_unit_count(const av1g_frame_header& h, int p) {
 }
 
 // Layout: [uploaded blob: grids | cdef_idx | lr units | coeffs] [planes]
-size_t plan_frame(const Ticket& t, FrameBufs& B, std::vector<size_t>& blob_off) {
+size_t plan_frame(const Ticket& t, FrameBufs& B) {
     const av1g_frame_header& h = t.hdr;
     const int bps = h.bit_depth > 8 ? 2 : 1, np = h.num_planes;
-    size_t off = 0;
-    blob_off.assign(14, 0);
-    for (int g = 0; g < 9; g++) {
-        blob_off[g] = off;
-        off = align256(off + t.grid[g].size());
-    }
-    blob_off[9] = off;
-    off = align256(off + t.cdef_idx.size());
-    for (int p = 0; p < 3; p++) {
-        blob_off[10 + p] = off;
-        off = align256(off + t.lr_units[p].size() * sizeof(av1g_lr_unit));
-    }
-    blob_off[13] = off;
-    off = align256(off + t.coeffs.size() * sizeof(int32_t));
+    size_t off = t.blob_bytes;
     B.host_bytes = off;
     bool sr = h.use_superres && h.upscaled_width > h.frame_width;
     auto plane = [&](av1g_plane& pl, int w, int hh) {
@@ -283,7 +275,7 @@ size_t plan_frame(const Ticket& t, FrameBufs& B, std::vector<size_t>& blob_off) 
     return off;
 }
 
-void rebase(FrameBufs& B, const std::vector<size_t>& blob_off, const Ticket& t) {
+void rebase(FrameBufs& B, const Ticket& t) {
     auto fix = [&](av1g_plane* a) {
         for (int p = 0; p < 3; p++)
             if (a[p].width) a[p].data = B.dev + (size_t)a[p].data;
@@ -296,18 +288,17 @@ void rebase(FrameBufs& B, const std::vector<size_t>& blob_off, const Ticket& t) 
     fix(B.lr);
     fix(B.out);
     fix(B.side);
-    for (int g = 0; g < 9; g++) B.grid[g] = t.grid[g].empty() ? nullptr : B.dev + blob_off[g];
-    B.cdef_idx = t.cdef_idx.empty() ? nullptr : (int8_t*)(B.dev + blob_off[9]);
+    for (int g = 0; g < 9; g++) B.grid[g] = t.blob_len[g] ? B.dev + t.blob_off[g] : nullptr;
+    B.cdef_idx = t.blob_len[9] ? (int8_t*)(B.dev + t.blob_off[9]) : nullptr;
     for (int p = 0; p < 3; p++)
-        B.lr_units[p] = t.lr_units[p].empty() ? nullptr : (av1g_lr_unit*)(B.dev + blob_off[10 + p]);
-    B.coeffs = t.coeffs.empty() ? nullptr : (int32_t*)(B.dev + blob_off[13]);
+        B.lr_units[p] = t.blob_len[10 + p] ? (av1g_lr_unit*)(B.dev + t.blob_off[10 + p]) : nullptr;
+    B.coeffs = t.blob_len[13] ? (int32_t*)(B.dev + t.blob_off[13]) : nullptr;
 }
 
 // What a step does for one ticket.
 struct Work {
     std::shared_ptr<Ticket> t;
     FrameBufs B;
-    std::vector<size_t> blob_off;
     std::shared_ptr<SlotBuf> shown_slot;  // show_existing source
     av1g_ref_frame refs[7] = {};
     av1g_frame_header pf_hdr = {};        // header the post-filter chain sees
@@ -388,7 +379,7 @@ void enqueue_step(av1g_engine* E, cudaStream_t cs, std::vector<std::shared_ptr<T
             }
         }
         if (w.run_chain) {
-            plan_frame(t, w.B, w.blob_off);
+            plan_frame(t, w.B);
             cudaError_t e = cudaMallocAsync((void**)&w.B.dev, w.B.bytes, cs);
             if (e != cudaSuccess) {
                 w.B.dev = nullptr;
@@ -396,22 +387,11 @@ void enqueue_step(av1g_engine* E, cudaStream_t cs, std::vector<std::shared_ptr<T
                 continue;
             }
             step.work_bytes += w.B.bytes;
-            rebase(w.B, w.blob_off, t);
-            // the frame's grids, CDEF indices, LR units and coefficients,
-            // assembled straight into the pinned staging block
-            e = upload_with(w.B.dev, w.B.host_bytes, cs, [&](uint8_t* blob) {
-                // the arrays cover the blob but for alignment gaps (and arrays
-                // a frame does not have), which nothing reads
-                for (int g = 0; g < 9; g++)
-                    if (!t.grid[g].empty()) memcpy(blob + w.blob_off[g], t.grid[g].data(), t.grid[g].size());
-                if (!t.cdef_idx.empty()) memcpy(blob + w.blob_off[9], t.cdef_idx.data(), t.cdef_idx.size());
-                for (int p = 0; p < 3; p++)
-                    if (!t.lr_units[p].empty())
-                        memcpy(blob + w.blob_off[10 + p], t.lr_units[p].data(),
-                               t.lr_units[p].size() * sizeof(av1g_lr_unit));
-                if (!t.coeffs.empty())
-                    memcpy(blob + w.blob_off[13], t.coeffs.data(), t.coeffs.size() * sizeof(int32_t));
-            });
+            rebase(w.B, t);
+            // the frame's grids, CDEF indices, LR units and coefficients: the
+            // pinned block submit filled, in one copy (the block is returned
+            // to the pool once the step has finished)
+            if (t.blob_bytes) e = cudaMemcpyAsync(w.B.dev, t.blob, t.blob_bytes, cudaMemcpyHostToDevice, cs);
             // CurrFrame starts at zero, like the walker's fresh planes
             for (int p = 0; e == cudaSuccess && p < t.hdr.num_planes; p++)
                 e = cudaMemsetAsync(w.B.recon[p].data, 0, (size_t)w.B.recon[p].stride * w.B.recon[p].height, cs);
@@ -674,6 +654,8 @@ void worker_loop(av1g_engine* E, Lane* L) {
                     if (E->inflight_bytes + extra == 0 && batch.empty()) {
                         // can never fit: fail it
                         S->pending.pop_front();
+                        E->pinned_put(t->blob);
+                        t->blob = nullptr;
                         t->status = AV1G_ENOMEM_BUDGET;
                         t->err = "frame work memory exceeds the engine budget";
                         t->done = true;
@@ -701,18 +683,17 @@ void worker_loop(av1g_engine* E, Lane* L) {
         cudaEventRecord(step.ev0, L->cs);
         double part[6] = {};
         enqueue_step(E, L->cs, batch, step, part);
-        // the descriptor copies have been staged; keep only the outputs
+        // the descriptor copies have been staged; keep only the outputs (the
+        // pinned blocks of the device-bound arrays go with the step)
         for (auto& t : batch) {
-            for (auto& g : t->grid) std::vector<uint8_t>().swap(g);
-            std::vector<int8_t>().swap(t->cdef_idx);
-            for (auto& u : t->lr_units) std::vector<av1g_lr_unit>().swap(u);
+            if (t->blob) step.blobs.push_back(t->blob);
+            t->blob = nullptr;
             std::vector<av1g_inter_pred>().swap(t->preds);
             std::vector<av1g_obmc_neighbour>().swap(t->nbs);
             std::vector<av1g_warp_ctx>().swap(t->warps);
             std::vector<av1g_tu>().swap(t->inter_tus);
             std::vector<av1g_intra_tu>().swap(t->intra_tus);
             std::vector<uint8_t>().swap(t->maps);
-            std::vector<int32_t>().swap(t->coeffs);
         }
         step.tickets = batch;
         step.work_bytes = extra;
@@ -761,6 +742,8 @@ void completer_loop(av1g_engine* E) {
                     }
                 }
                 if (step.intra_status && !expired) E->pinned_put((uint8_t*)step.intra_status);
+                if (!expired)
+                    for (uint8_t* b : step.blobs) E->pinned_put(b);
                 for (auto& t : step.tickets) {
                     if (q != cudaSuccess && t->status == AV1G_OK) {
                         t->status = expired ? AV1G_TIMEOUT : AV1G_EDEVICE;
@@ -887,7 +870,10 @@ void av1g_engine_destroy(av1g_engine* E) {
         for (auto& sl : S->slots) sl.reset();
         delete S;
     }
-    for (auto& kv : E->tickets) E->pinned_put(kv.second->host_out);
+    for (auto& kv : E->tickets) {
+        E->pinned_put(kv.second->host_out);
+        E->pinned_put(kv.second->blob);  // never enqueued
+    }
     E->tickets.clear();
     for (auto& L : E->lanes) cudaStreamSynchronize(L->cs);
     for (auto& kv : E->pinned_free) cudaFreeHost(kv.second - sizeof(size_t));
@@ -997,17 +983,33 @@ av1g_status av1g_submit_frame(av1g_stream* S, const av1g_frame_desc* d, uint64_t
     size_t blob = 0;
     if (!d->show_existing_frame) {
         size_t M = (size_t)h.mi_rows * h.mi_cols;
-        const uint8_t* g[9] = {d->grid.mi_size, d->grid.skip, d->grid.is_inter, (const uint8_t*)d->grid.ref_frame0,
-                               d->grid.y_mode, (const uint8_t*)d->grid.segment_id, (const uint8_t*)d->grid.delta_lf,
-                               d->grid.tx_size, d->grid.inter_tx_size};
-        for (int k = 0; k < 9; k++) {
-            copy_in(t->grid[k], g[k], (int64_t)(k == 6 ? 4 * M : M));
-            blob += t->grid[k].size() + 256;
-        }
-        size_t ncdef = (size_t)((h.mi_rows + 15) >> 4) * ((h.mi_cols + 15) >> 4);
-        copy_in(t->cdef_idx, d->cdef_idx, (int64_t)ncdef);
+        const void* src[14] = {d->grid.mi_size, d->grid.skip, d->grid.is_inter, d->grid.ref_frame0, d->grid.y_mode,
+                               d->grid.segment_id, d->grid.delta_lf, d->grid.tx_size, d->grid.inter_tx_size,
+                               d->cdef_idx, d->lr_units[0], d->lr_units[1], d->lr_units[2], d->coeffs};
+        size_t len[14] = {};
+        for (int k = 0; k < 9; k++) len[k] = src[k] ? (k == 6 ? 4 * M : M) : 0;
+        len[9] = d->cdef_idx ? (size_t)((h.mi_rows + 15) >> 4) * ((h.mi_cols + 15) >> 4) : 0;
         for (int p = 0; p < 3; p++)
-            if (h.uses_lr && p < h.num_planes && h.lr_type[p]) copy_in(t->lr_units[p], d->lr_units[p], lr_unit_count(h, p));
+            if (h.uses_lr && p < h.num_planes && h.lr_type[p] && d->lr_units[p])
+                len[10 + p] = (size_t)lr_unit_count(h, p) * sizeof(av1g_lr_unit);
+        len[13] = d->coeffs && d->num_coeffs > 0 ? (size_t)d->num_coeffs * sizeof(int32_t) : 0;
+        size_t off = 0;
+        for (int k = 0; k < 14; k++) {
+            t->blob_off[k] = off;
+            t->blob_len[k] = len[k];
+            off = align256(off + len[k]);
+        }
+        t->blob_bytes = off;
+        if (off) {
+            {
+                DeviceGuard g(S->eng->device);
+                t->blob = S->eng->pinned_get(off);
+            }
+            if (!t->blob) return AV1G_EDEVICE;
+            // the arrays cover the block but for alignment gaps, which nothing reads
+            for (int k = 0; k < 14; k++)
+                if (len[k]) memcpy(t->blob + t->blob_off[k], src[k], len[k]);
+        }
         copy_in(t->preds, d->inter_preds, d->num_inter_preds);
         for (const av1g_inter_pred& pr : t->preds) t->has_interintra |= pr.kind == AV1G_INTER_INTRA;
         copy_in(t->nbs, d->neighbours, d->num_neighbours);
@@ -1015,8 +1017,7 @@ av1g_status av1g_submit_frame(av1g_stream* S, const av1g_frame_desc* d, uint64_t
         copy_in(t->inter_tus, d->inter_tus, d->num_inter_tus);
         copy_in(t->intra_tus, d->intra_tus, d->num_intra_tus);
         copy_in(t->maps, d->palette_maps, d->palette_map_bytes);
-        copy_in(t->coeffs, d->coeffs, d->num_coeffs);
-        blob += t->cdef_idx.size() + t->coeffs.size() * 4 + 4096;
+        blob = off + 9 * 256 + 4096;
         t->work_bytes = work_estimate(h, blob);
     } else {
         av1g_frame_header hh = {};
@@ -1032,7 +1033,10 @@ av1g_status av1g_submit_frame(av1g_stream* S, const av1g_frame_desc* d, uint64_t
     }
     av1g_engine* E = S->eng;
     std::lock_guard<std::mutex> lk(E->mu);
-    if (S->closing) return AV1G_EINVAL;
+    if (S->closing) {
+        E->pinned_put(t->blob);
+        return AV1G_EINVAL;
+    }
     t->id = E->next_id++;
     t->t_submit = Clock::now();
     E->tickets[t->id] = t;
