@@ -392,8 +392,9 @@ def run_gpu(args):
         line["extra_stages"] = run_extra_stages(args, dev, stream)
         line["motion_field"] = run_motion_field(args, dev, stream)
     if rank == 0 and world == 1 and not args.no_serving:
-        line["batching"] = run_batching(args, local)
-        line["serving"] = run_serving(args, local)
+        mix = mix_templates()
+        line["batching"] = run_batching(args, local, mix)
+        line["serving"] = run_serving(args, local, mix)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         k = args.cpu_sample
         dt = cpu_time_frames(frames[:k], 1)
@@ -513,7 +514,18 @@ def run_recon_stages(args, dev, stream):
 
     fi = synth.make_intra_frame(9003, WIDTH, HEIGHT, **kw)
     d = postfilter.DeviceIntra(fi, device=dev)
-    ms, hms = _device_ms(stream, lambda: postfilter.run_intra([d], stream=stream))
+    ms, _ = _device_ms(stream, lambda: postfilter.run_intra([d], stream=stream))
+    # av1g_run_intra returns once its launch has finished (it reads the
+    # per-frame wait status), so its host share is the call's wall time on an
+    # idle stream less the device time
+    import torch
+    walls = []
+    for _ in range(5):
+        torch.cuda.synchronize()
+        h0 = time.perf_counter()
+        postfilter.run_intra([d], stream=stream)
+        walls.append((time.perf_counter() - h0) * 1e3)
+    hms = max(0.0, min(walls) - ms)
     area = int((tw[fi.tus["tx_size"]] * th[fi.tus["tx_size"]]).sum())
     out["intra"] = {"kernels": ["intra_res_kernel", "intra_kernel"], "ms_per_frame": ms, "host_ms_per_call": hms,
                     "tus": len(fi.tus), "tus_per_us": len(fi.tus) / (ms * 1e3),
@@ -681,10 +693,11 @@ TEMPLATE_FRAMES = 3
 
 
 def _make_template(spec):
-    """One stream template; runs in a spawned worker process."""
+    """One stream template; runs in a spawned worker process.  3840x2160
+    streams use the full-reconstruction configuration's 2 x 2 tile grid."""
     seed, w, h, bd, ss, grain, sb = spec
     return synth.make_stream(seed, n_frames=TEMPLATE_FRAMES, width=w, height=h, bit_depth=bd, ssx=ss, ssy=ss,
-                             film_grain=grain, sb_size=sb)
+                             film_grain=grain, sb_size=sb, tiles=(1, 1) if w >= 3840 else (0, 0))
 
 
 def make_templates(specs):
@@ -825,7 +838,29 @@ def _host_info():
     return {"host_cpus": len(os.sched_getaffinity(0)), "host_load_avg_1min": os.getloadavg()[0]}
 
 
-def run_batching(args, local):
+def mix_templates():
+    """The stream-batching mix's templates: every resolution x bit depth (8,
+    10) x chroma format (4:2:0, 4:4:4), index = shape * 4 + depth * 2 + format;
+    returns (templates, superblock sizes, generation seconds)."""
+    specs, sbs = [], []
+    for w, h in BATCH_SHAPES:
+        for bd in (8, 10):
+            for ss in (1, 0):
+                sb = 128 if w >= 3840 else 64
+                specs.append((900 + len(specs), w, h, bd, ss, False, sb))
+                sbs.append(sb)
+    t0 = time.perf_counter()
+    templates = make_templates(specs)
+    return templates, sbs, time.perf_counter() - t0
+
+
+def _draw_mix_template(rng):
+    shape_of = [si for si, wgt in enumerate(BATCH_WEIGHTS) for _ in range(wgt)]
+    si = shape_of[int(rng.integers(0, len(shape_of)))]
+    return si * 4 + int(rng.integers(0, 2)) * 2 + int(rng.integers(0, 2))
+
+
+def run_batching(args, local, mix):
     """The stream-batching configuration through the engine: 256 streams of
     uneven shape decoded by the engine batching one frame of every ready
     stream per step (one launch per stage across the streams of a lane)
@@ -836,33 +871,21 @@ def run_batching(args, local):
     decoded alone (a CRC-32 of every plane of every frame)."""
     from oxideav_av1_b200 import engine
     rng = np.random.default_rng(11)
-    specs, sbs = [], []
-    for si, (w, h) in enumerate(BATCH_SHAPES):
-        for bd in (8, 10):
-            for ss in (1, 0):
-                sb = 128 if w >= 3840 else 64
-                specs.append((900 + len(specs), w, h, bd, ss, False, sb))
-                sbs.append(sb)
-    t0 = time.perf_counter()
-    templates = make_templates(specs)
-    gen_s = time.perf_counter() - t0
+    templates, sbs, gen_s = mix
     # stream i: shape by weight, bit depth and chroma format uniform, 8-60 frames
-    shape_of = [si for si, wgt in enumerate(BATCH_WEIGHTS) for _ in range(wgt)]
-    streams = []
-    for _ in range(args.batch_streams):
-        si = shape_of[int(rng.integers(0, len(shape_of)))]
-        t = si * 4 + int(rng.integers(0, 2)) * 2 + int(rng.integers(0, 2))
-        streams.append((t, int(rng.integers(8, 61))))
+    streams = [(_draw_mix_template(rng), int(rng.integers(8, 61))) for _ in range(args.batch_streams)]
     lengths = [max([n for t_, n in streams if t_ == t] + [1]) for t in range(len(templates))]
     ref = _alone_digests(local, templates, sbs, lengths)
     frames = sum(n for _, n in streams)
+    desc_bytes = sum(_desc_bytes(stream_frame(templates[t], k)) for t, n in streams for k in range(n))
     out = {"streams": len(streams), "frames": frames,
            "mix": "640x360 / 1280x720 / 1920x1080 / 3840x2160 weighted 4:3:2:1, 8- or 10-bit, 4:2:0 or 4:4:4 "
-                  "(uniform), 8-60 frames per stream (uniform); 128x128 superblocks at 3840x2160",
+                  "(uniform), 8-60 frames per stream (uniform); 128x128 superblocks and 2 x 2 tiles at 3840x2160",
            "templates": f"{len(templates)} synthetic streams (a key frame with palette blocks, then inter frames with "
                         f"every inter tool, intra blocks and residuals, the post-filter chain); a longer stream "
                         f"cycles its template's inter frames",
            "template_generation_s": gen_s,
+           "descriptor_bytes_per_frame": desc_bytes / frames,
            "timing": "host wall clock, first submit to last fetch; 8 client threads each owning a group of streams "
                      "(at most 2 frames of a stream in flight), a CRC-32 per plane of every output frame taken by "
                      "the clients",
@@ -885,41 +908,32 @@ def run_batching(args, local):
     return out
 
 
-def run_serving(args, local):
-    """The serving configuration through the engine: 3840x2160 10-bit 4:2:0
-    streams of 30-300 frames (uniform), 25 % with film grain, admitted by a
-    120 GB HBM budget.  Capacity is measured closed-loop (every stream open at
-    once) on the batching engine and on the per-frame path at the same lane
-    count; then streams arrive as a Poisson process at 30 %, 60 % and 90 % of
-    the batched capacity, and the per-frame path at the 60 % arrival rate.
-    A client thread takes each arrival, opens the stream (waiting while the
-    budget is full), decodes it with two frames in flight and checks every
-    frame against the template decoded alone.  The stated mean rate of 40
-    streams/s is reported as the offered load it is against the capacity."""
+def _desc_bytes(fr):
+    """Bytes of one frame's host descriptor (what av1g_submit_frame copies)."""
+    n = 0
+    for a in [fr.preds, fr.neighbours, fr.warps, fr.inter_tus, fr.intra_tus, fr.coeffs, fr.palette_maps,
+              fr.cdef_idx] + list(fr.lr_units or []) + list((fr.grid or {}).values()):
+        if a is not None:
+            n += np.asarray(a).nbytes
+    return n
+
+
+def _serve_variant(args, local, templates, sbs, draw, mean_len, label):
+    """One serving run: closed-loop capacity of the batching engine and of the
+    per-frame path (same lanes, budget and clients), then Poisson arrivals at
+    30 %, 60 % and 90 % of the batched capacity, and the per-frame path at the
+    60 % arrival rate.  A client thread takes each arrival, opens the stream
+    (waiting while the budget is full), decodes it with two frames in flight
+    and checks every frame against the template decoded alone."""
     import queue
     import threading
     from oxideav_av1_b200 import engine
     rng = np.random.default_rng(17)
-    w, h, bd = SERVE_SHAPE
-    specs = [(950 + i, w, h, bd, 1, grain, 128) for i, grain in enumerate([False, False, True, True])]
-    sbs = [128] * len(specs)
-    t0 = time.perf_counter()
-    templates = make_templates(specs)
-    gen_s = time.perf_counter() - t0
-
-    def draw():
-        grain = rng.random() < 0.25
-        return (2 if grain else 0) + int(rng.integers(0, 2)), int(rng.integers(30, 301))
-
     ref = _alone_digests(local, templates, sbs, [300] * len(templates))
-    mean_len = (30 + 300) / 2
-    out = {"shape": f"{w}x{h} {bd}-bit 4:2:0, 128x128 superblocks, 30-300 frames per stream, 25 % with film grain",
-           "budget_bytes": SERVE_BUDGET, "lanes": args.serve_lanes, "template_generation_s": gen_s,
+    out = {"what": label, "budget_bytes": SERVE_BUDGET, "lanes": args.serve_lanes,
            "timing": "host wall clock; per-frame latency = the engine's submit-to-completion time", **_host_info()}
     ok_all = True
-
-    # closed-loop capacity
-    cap_streams = [draw() for _ in range(args.serve_cap_streams)]
+    cap_streams = [draw(rng) for _ in range(args.serve_cap_streams)]
     for name, mb in [("batched", 64), ("per_frame", 1)]:
         eng = engine.Engine(device=local, max_batch=mb, lanes=args.serve_lanes, budget_bytes=SERVE_BUDGET)
         drive(eng, templates, sbs, [(t, 3) for t in range(len(templates))])
@@ -942,7 +956,7 @@ def run_serving(args, local):
             t += rng.exponential(1.0 / lam)
             if t > args.serve_seconds:
                 break
-            arrivals.append((t, draw()))
+            arrivals.append((t, draw(rng)))
         eng = engine.Engine(device=local, max_batch=mb, lanes=args.serve_lanes, budget_bytes=SERVE_BUDGET)
         drive(eng, templates, sbs, [(t_, 3) for t_ in range(len(templates))])
         s0 = eng.stats()
@@ -957,10 +971,11 @@ def run_serving(args, local):
                     return
                 t_arr, (tpl, n) = item
                 w0 = time.perf_counter()
-                hnd = eng.open_stream(synth.stream_seq(templates[tpl], 128))
+                seq = synth.stream_seq(templates[tpl], sbs[tpl])
+                hnd = eng.open_stream(seq)
                 while hnd is None:  # admitted once the budget frees up
                     time.sleep(0.001)
-                    hnd = eng.open_stream(synth.stream_seq(templates[tpl], 128))
+                    hnd = eng.open_stream(seq)
                 wait = (time.perf_counter() - w0) * 1e3
                 pend, dg, ls, ok = [], [], [], True
                 for k in range(n):
@@ -1024,6 +1039,43 @@ def run_serving(args, local):
     ok_all &= ok
     out["poisson_per_frame_path"] = r
     out["bit_exact_alone_vs_mixed"] = bool(ok_all)
+    return out
+
+
+def run_serving(args, local, mix):
+    """The serving configuration through the engine: Poisson arrivals of
+    streams of 30-300 frames (uniform), 25 % with film grain, admitted by a
+    120 GB HBM budget; the stated mean rate (40 streams/s) is reported as the
+    offered load it is against the measured capacity.  Two stream mixes: the
+    batching configuration's resolutions, bit depths and chroma formats, and
+    3840x2160 10-bit 4:2:0 only (the full-reconstruction configuration's
+    shape)."""
+    templates, sbs, gen_s = mix
+    # each mix template also with film grain on every frame (index + 16)
+    grained = [synth.with_film_grain(t, 77 + i) for i, t in enumerate(templates)]
+    mix_t, mix_sb = templates + grained, sbs + sbs
+
+    def draw_mix(rng):
+        t = _draw_mix_template(rng) + (len(templates) if rng.random() < 0.25 else 0)
+        return t, int(rng.integers(30, 301))
+
+    out = {"mix": _serve_variant(args, local, mix_t, mix_sb, draw_mix, (30 + 300) / 2,
+                                 "the batching mix (640x360 / 1280x720 / 1920x1080 / 3840x2160 weighted 4:3:2:1, "
+                                 "8- or 10-bit, 4:2:0 or 4:4:4), 30-300 frames per stream, 25 % with film grain")}
+    w, h, bd = SERVE_SHAPE
+    specs = [(950 + i, w, h, bd, 1, grain, 128) for i, grain in enumerate([False, False, True, True])]
+    t0 = time.perf_counter()
+    uhd = make_templates(specs)
+    gen_uhd = time.perf_counter() - t0
+
+    def draw_uhd(rng):
+        grain = rng.random() < 0.25
+        return (2 if grain else 0) + int(rng.integers(0, 2)), int(rng.integers(30, 301))
+
+    out["uhd"] = _serve_variant(args, local, uhd, [128] * len(uhd), draw_uhd, (30 + 300) / 2,
+                                f"{w}x{h} {bd}-bit 4:2:0, 128x128 superblocks, 2 x 2 tiles, 30-300 frames per "
+                                f"stream, 25 % with film grain")
+    out["template_generation_s"] = gen_s + gen_uhd
     return out
 
 
@@ -1186,7 +1238,7 @@ def main():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--batch-streams", type=int, default=256)
     ap.add_argument("--serve-cap-streams", type=int, default=12)
-    ap.add_argument("--serve-seconds", type=float, default=12.0)
+    ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--serve-clients", type=int, default=32)
     ap.add_argument("--serve-lanes", type=int, default=8)
     ap.add_argument("--section", default="all",
@@ -1202,7 +1254,7 @@ def main():
         abi.load()
         if args.section in ("batching", "serving"):
             fn = run_batching if args.section == "batching" else run_serving
-            print(json.dumps({args.section: fn(args, 0)}), flush=True)
+            print(json.dumps({args.section: fn(args, 0, mix_templates())}), flush=True)
             return 0
         stream = torch.cuda.Stream()
         fn = {"chain": run_chain, "recon": run_recon_stages, "extra": run_extra_stages, "motion_field": run_motion_field}[args.section]

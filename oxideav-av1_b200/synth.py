@@ -987,6 +987,23 @@ def make_stream(seed, n_frames=4, width=176, height=144, bit_depth=8, ssx=1, ssy
     return frames
 
 
+def with_film_grain(frames, seed):
+    """The same stream with film grain on every frame: each frame a shallow
+    copy sharing the descriptors, with its own header carrying seeded grain
+    parameters (a new grain_seed per frame)."""
+    import copy
+    rng = np.random.default_rng(seed)
+    out = []
+    for fr in frames:
+        g = copy.copy(fr)
+        h = abi.FrameHeader()
+        C.memmove(C.addressof(h), C.addressof(fr.hdr), C.sizeof(h))
+        _film_grain(rng, h.film_grain, h.bit_depth, h.num_planes == 1)
+        g.hdr = h
+        out.append(g)
+    return out
+
+
 def stream_seq(frames, sb_size=64):
     h = frames[0].hdr
     return {"max_width": h.upscaled_width, "max_height": h.frame_height, "bit_depth": h.bit_depth,
