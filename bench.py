@@ -391,6 +391,8 @@ def run_gpu(args):
         line["recon_stages"] = run_recon_stages(args, dev, stream)
         line["extra_stages"] = run_extra_stages(args, dev, stream)
         line["motion_field"] = run_motion_field(args, dev, stream)
+    if rank == 0 and world == 1:
+        line["decode"] = run_decode(args, local)
     if rank == 0 and world == 1 and not args.no_serving:
         mix = mix_templates()
         line["batching"] = run_batching(args, local, mix)
@@ -531,6 +533,14 @@ def run_recon_stages(args, dev, stream):
                     "tus": len(fi.tus), "tus_per_us": len(fi.tus) / (ms * 1e3),
                     "bound": "latency: the TU dependency chain of the superblock wavefront",
                     "algorithmic_bytes": fi.coeffs.nbytes + 2 * area * S}
+    # the full-reconstruction configuration's key frame: 3840x2160 10-bit,
+    # 128x128 superblocks, 2 x 2 tiles (the tiles' wavefronts run side by side)
+    fu = synth.make_intra_frame(9004, 3840, 2160, bit_depth=10, sb_size=128, tiles=(1, 1))
+    du = postfilter.DeviceIntra(fu, device=dev)
+    msu, _ = _device_ms(stream, lambda: postfilter.run_intra([du], stream=stream), reps=3)
+    out["intra_uhd"] = {"kernels": ["intra_res_kernel", "intra_kernel"], "frame": "3840x2160 10-bit 4:2:0, "
+                        "128x128 superblocks, 2 x 2 tiles", "ms_per_frame": msu, "tus": len(fu.tus),
+                        "tus_per_us": len(fu.tus) / (msu * 1e3)}
     return out
 
 
@@ -836,6 +846,78 @@ def _alone_digests(local, templates, sbs, lengths):
 
 def _host_info():
     return {"host_cpus": len(os.sched_getaffinity(0)), "host_load_avg_1min": os.getloadavg()[0]}
+
+
+def run_decode(args, local, passes=16):
+    """Real AV1 bitstreams end to end: the 110 IVF streams the reference's
+    tests/fixture_conformance.rs decodes (carried in
+    tests/golden/framing_fixtures.json.gz with the SHA-256 of their decoded
+    planes), each through the registry-style stream decoder: the host tile
+    walk (symbols, contexts, motion vector prediction) and the GPU engine for
+    every pixel stage, whole IVF file in, shown frames out.  8 client threads
+    each decode their share of the corpus, `passes` times over, on one
+    engine; every stream's digest is checked against the reference's on
+    every pass.  The CPU arm decodes the corpus once on one host thread with
+    the same walk and the oracle (the C restatement of the reference's pixel
+    path).  The streams are small (64x64 to 320x240, 478 shown frames), so
+    per-frame fixed costs dominate both arms."""
+    import base64
+    import gzip
+    import threading
+    from oxideav_av1_b200 import decoder, engine
+    streams = json.load(gzip.open(ROOT / "tests" / "golden" / "framing_fixtures.json.gz"))["ivf_streams"]
+    ivfs = [base64.b64decode(x["ivf"]) for x in streams]
+    eng = engine.Engine(device=local, lanes=8)
+    for b in ivfs[:8]:   # warm-up: pinned pools, memory pool
+        decoder.decode(b, eng)
+    lock = threading.Lock()
+    res = {"frames": 0, "walk_ms": 0.0, "ok": True}
+
+    def client(ids):
+        n, walk, ok = 0, 0.0, True
+        for _ in range(passes):
+            for i in ids:
+                dec = decoder.Av1Decoder(eng)
+                try:
+                    dec.send_packet(ivfs[i])
+                    dec.flush()
+                    frames = dec.drain()
+                    walk += dec.host_ms()
+                finally:
+                    dec.close()
+                ok &= decoder.digest(frames) == streams[i]["sha256"] and len(frames) == streams[i]["shown_frames"]
+                n += len(frames)
+        with lock:
+            res["frames"] += n
+            res["walk_ms"] += walk
+            res["ok"] &= ok
+
+    # largest streams first, spread over the clients
+    order = sorted(range(len(ivfs)), key=lambda i: -len(ivfs[i]))
+    threads = [threading.Thread(target=client, args=(order[k::8],)) for k in range(8)]
+    t0 = time.perf_counter()
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    wall = time.perf_counter() - t0
+    eng.close()
+    out = {"streams": len(ivfs), "passes": passes, "frames": res["frames"], "value": res["frames"] / wall,
+           "unit": UNIT, "wall_s": wall, "walk_host_ms_per_frame": res["walk_ms"] / max(1, res["frames"]),
+           "digests_match_reference": bool(res["ok"]),
+           "path": "av1g_decoder_send_packet (whole IVF) / av1g_decoder_receive_frame, one engine, 8 client "
+                   "threads", **_host_info()}
+    if not args.no_cpu_baseline:
+        import oracle
+        t0 = time.perf_counter()
+        n = 0
+        for b in ivfs:
+            _, frames = decoder.parse_stream(b)
+            n += sum(1 for o in oracle.decode_stream(frames) if o is not None)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": n / dt, "unit": UNIT, "cores": 1, "kind": "port",
+                               "sample": f"the whole corpus once ({n} shown frames): host walk + oracle, one thread"}
+    return out
 
 
 def mix_templates():
@@ -1242,7 +1324,7 @@ def main():
     ap.add_argument("--serve-clients", type=int, default=32)
     ap.add_argument("--serve-lanes", type=int, default=8)
     ap.add_argument("--section", default="all",
-                    choices=["all", "recon", "extra", "motion_field", "chain", "batching", "serving"],
+                    choices=["all", "recon", "extra", "motion_field", "chain", "decode", "batching", "serving"],
                     help="recon / extra: only that section (one GPU), printed as its own JSON object; "
                          "for profiling a row's kernels")
     args = ap.parse_args()
@@ -1252,6 +1334,9 @@ def main():
         import torch
         torch.cuda.set_device(0)
         abi.load()
+        if args.section == "decode":
+            print(json.dumps({"decode": run_decode(args, 0)}), flush=True)
+            return 0
         if args.section in ("batching", "serving"):
             fn = run_batching if args.section == "batching" else run_serving
             print(json.dumps({args.section: fn(args, 0, mix_templates())}), flush=True)
