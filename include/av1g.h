@@ -655,6 +655,11 @@ typedef struct av1g_config {
                                     stream of frames stays on one lane; 0 = 4     */
     const char* autotune_cache;  /* NULL, or a file av1g_autotune_postfilter
                                     wrote: loaded at create                       */
+    int64_t max_step_samples;    /* a step takes frames until their luma samples
+                                    would pass this (at least one frame):
+                                    small frames batch, large ones pipeline;
+                                    0 = 4,194,304 (two 1080p frames), < 0 =
+                                    no limit                                      */
 } av1g_config;
 
 /* What a stream's sequence header fixes: the largest upscaled frame and the

@@ -174,7 +174,8 @@ INTER_SINGLE, INTER_COMPOUND, INTER_INTRA = 0, 1, 2
 
 class Config(C.Structure):
     _fields_ = [("device", C.c_int32), ("max_batch", C.c_int32), ("hbm_budget_bytes", C.c_int64),
-                ("max_inflight_steps", C.c_int32), ("lanes", C.c_int32), ("autotune_cache", C.c_char_p)]
+                ("max_inflight_steps", C.c_int32), ("lanes", C.c_int32), ("autotune_cache", C.c_char_p),
+                ("max_step_samples", C.c_int64)]
 
 
 class SeqInfo(C.Structure):

@@ -10,7 +10,8 @@
 //
 // Worker threads ("lanes", each with its own CUDA stream; a stream of frames
 // belongs to one lane) form steps: a lane takes the oldest pending frame of
-// each of its streams that has one (up to max_batch frames, round robin), and
+// each of its streams that has one (up to max_batch frames, round robin, and
+// while their luma samples stay within max_step_samples), and
 // enqueues for the whole step one inter launch, one residual launch, the
 // intra wavefront and the post-filter chain (one launch per stage), then the
 // slot refreshes and the output copies, on its CUDA stream; lanes overlap
@@ -158,6 +159,7 @@ struct av1g_engine {
     int device = 0;
     size_t budget = 0, reserved = 0, inflight_bytes = 0;
     int max_batch = 64, max_steps = 3;
+    int64_t max_step_samples = 4194304;  // < 0: no limit
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::vector<av1g_stream*> streams;
@@ -169,9 +171,15 @@ struct av1g_engine {
     uint64_t next_id = 1;
     int64_t frames_done = 0, steps_done = 0;
     double host_ms = 0, device_ms = 0, host_stage_ms[6] = {};
-    // pinned output blocks by size
+    // pinned host blocks (descriptor blobs, outputs, status words) by
+    // capacity.  Blocks come from slabs of up to eight blocks of one capacity
+    // class (cudaHostAlloc pins pages and is slow and serialising, so it runs
+    // once per slab, not per block); a block returns to the free list and the
+    // slabs are freed with the engine.
+    static constexpr size_t kPinHeader = 256;  // keeps blocks 256-byte aligned
     std::mutex pin_mu;
     std::multimap<size_t, uint8_t*> pinned_free;
+    std::vector<uint8_t*> pinned_slabs;
 
     uint8_t* pinned_get(size_t n) {
         // power-of-two capacities (from 256 KiB), so buffers recycle across
@@ -185,15 +193,23 @@ struct av1g_engine {
             pinned_free.erase(it);
             return p;
         }
-        uint8_t* p = nullptr;
-        if (cudaHostAlloc((void**)&p, cap + sizeof(size_t), cudaHostAllocPortable) != cudaSuccess) return nullptr;
-        *(size_t*)p = cap;
-        return p + sizeof(size_t);
+        const size_t blk = cap + kPinHeader;
+        size_t k = ((size_t)64 << 20) / cap;
+        k = k < 1 ? 1 : (k > 8 ? 8 : k);
+        uint8_t* slab = nullptr;
+        if (cudaHostAlloc((void**)&slab, k * blk, cudaHostAllocPortable) != cudaSuccess) {
+            k = 1;  // retry with one block
+            if (cudaHostAlloc((void**)&slab, blk, cudaHostAllocPortable) != cudaSuccess) return nullptr;
+        }
+        pinned_slabs.push_back(slab);
+        for (size_t j = 0; j < k; j++) *(size_t*)(slab + j * blk) = cap;
+        for (size_t j = 1; j < k; j++) pinned_free.emplace(cap, slab + j * blk + kPinHeader);
+        return slab + kPinHeader;
     }
     void pinned_put(uint8_t* p) {
         if (!p) return;
         std::lock_guard<std::mutex> lk(pin_mu);
-        pinned_free.emplace(*(size_t*)(p - sizeof(size_t)), p);
+        pinned_free.emplace(*(size_t*)(p - kPinHeader), p);
     }
 };
 
@@ -635,6 +651,7 @@ void worker_loop(av1g_engine* E, Lane* L) {
     while (!E->stop) {
         std::vector<std::shared_ptr<Ticket>> batch;
         size_t extra = 0;
+        int64_t samples = 0;  // luma samples of the frames taken
         if ((int)L->steps.size() < E->max_steps) {
             size_t n = E->streams.size();
             for (size_t k = 0; k < n && (int)batch.size() < E->max_batch; k++) {
@@ -650,6 +667,10 @@ void worker_loop(av1g_engine* E, Lane* L) {
                 }
                 if (S->pending.empty()) continue;
                 std::shared_ptr<Ticket> t = S->pending.front();
+                // a step's host preparation is serial: bound its size so that
+                // large frames pipeline instead of waiting for each other
+                const int64_t tpx = (int64_t)t->hdr.upscaled_width * t->hdr.frame_height;
+                if (!batch.empty() && E->max_step_samples > 0 && samples + tpx > E->max_step_samples) break;
                 if (E->reserved + E->inflight_bytes + extra + t->work_bytes > E->budget) {
                     if (E->inflight_bytes + extra == 0 && batch.empty()) {
                         // can never fit: fail it
@@ -667,6 +688,7 @@ void worker_loop(av1g_engine* E, Lane* L) {
                 S->pending.pop_front();
                 S->inflight++;
                 extra += t->work_bytes;
+                samples += tpx;
                 batch.push_back(t);
             }
             if (n) rr = (rr + 1) % n;
@@ -808,6 +830,7 @@ av1g_status av1g_engine_create(const av1g_config* cfg, av1g_engine** out) {
     auto* E = new av1g_engine();
     E->device = cfg->device;
     E->max_batch = cfg->max_batch > 0 ? cfg->max_batch : 64;
+    E->max_step_samples = cfg->max_step_samples != 0 ? cfg->max_step_samples : 4194304;
     E->max_steps = cfg->max_inflight_steps > 0 ? cfg->max_inflight_steps : 3;
     int nl = cfg->lanes > 0 ? cfg->lanes : 4;
     size_t free_b = 0, total_b = 0;
@@ -876,7 +899,7 @@ void av1g_engine_destroy(av1g_engine* E) {
     }
     E->tickets.clear();
     for (auto& L : E->lanes) cudaStreamSynchronize(L->cs);
-    for (auto& kv : E->pinned_free) cudaFreeHost(kv.second - sizeof(size_t));
+    for (uint8_t* slab : E->pinned_slabs) cudaFreeHost(slab);
     for (auto& L : E->lanes) cudaStreamDestroy(L->cs);
     delete E;
 }

@@ -15,9 +15,9 @@ def _p(a):
 
 
 class Engine:
-    def __init__(self, device=0, max_batch=0, budget_bytes=0, max_inflight_steps=0, lanes=0):
+    def __init__(self, device=0, max_batch=0, budget_bytes=0, max_inflight_steps=0, lanes=0, max_step_samples=0):
         self.lib = abi.load()
-        cfg = abi.Config(device, max_batch, budget_bytes, max_inflight_steps, lanes)
+        cfg = abi.Config(device, max_batch, budget_bytes, max_inflight_steps, lanes, None, max_step_samples)
         h = C.c_void_p()
         abi.check(self.lib.av1g_engine_create(C.byref(cfg), C.byref(h)))
         self.h = h
