@@ -91,6 +91,11 @@ __device__ void box_coeffs(Smem& s, int th, int tw, int bd, int eps, int y0) {
     const long long n2e = (long long)n * n * eps;
     const unsigned sm = (unsigned)(((1LL << 20) + n2e / 2) / n2e);
     constexpr int one_over_n = ((1 << 12) + n / 2) / n;
+    // z = (p * sm + 2^19) >> 20 reaches 255 (a2 = 256) once p * sm >= zsat;
+    // clamping p to the first such value keeps every product below 2^32
+    // (zsat + sm) and leaves a2 unchanged, so z is computed in 32 bits
+    constexpr unsigned zsat = (255u << 20) - (1u << 19);
+    const unsigned pcap = (zsat + sm - 1) / sm;
     const int sa = 2 * (bd - 8), sb = bd - 8;
     const int vw = tw + 2 * H3;
     const int rows = th + 2;
@@ -159,12 +164,14 @@ __device__ void box_coeffs(Smem& s, int th, int tw, int bd, int eps, int y0) {
             int dr = sb ? (b + (1 << (sb - 1))) >> sb : b;
             int p = ar * n - dr * dr;
             if (p < 0) p = 0;
-            unsigned z = (unsigned)(((unsigned long long)(unsigned)p * sm + (1u << 19)) >> 20);
+            const unsigned z = (min((unsigned)p, pcap) * sm + (1u << 19)) >> 20;
             int a2 = z >= 255 ? 256 : s.a2lut[z];
-            // b2 uses the raw box sum b, as the reference does (loop_restoration.rs:660-661)
-            long long b2 = (long long)((256 - a2) * b) * one_over_n;
+            // b2 uses the raw box sum b, as the reference does
+            // (loop_restoration.rs:660-661); (256 - a2) * b * one_over_n
+            // stays below 2^32 at every bit depth (b <= 25 * 4095)
+            const unsigned b2 = (unsigned)(256 - a2) * (unsigned)b * (unsigned)one_over_n;
             ao[t] = (uint16_t)a2;
-            bo[t] = (int)((b2 + (1 << 11)) >> 12);
+            bo[t] = (int)((b2 + (1u << 11)) >> 12);
             b += c1[t + 2 * R + 1] - c1[t];
             a += c2[t + 2 * R + 1] - c2[t];
         }
