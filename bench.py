@@ -19,6 +19,15 @@ oracle (a C restatement of the reference's CPU path) on a bounded sample.
 
 `--impl reference` times the reference's CPU implementation of the path (the
 same C restatement — the Rust crate does not build here) on all host cores.
+
+Further sections in the same line (rank 0, one GPU): `recon_stages` (inter
+residuals, inter prediction, the intra wavefront at 1080p and at 3840x2160
+tiled), `extra_stages` (superres, film grain), `motion_field`, `decode` (the
+reference's conformance streams through the stream decoder, digests checked),
+`batching` (256 mixed streams through the serving engine, batched against the
+per-frame path at equal lanes) and `serving` (Poisson arrivals of 30-300
+frame streams at three loads, for the batching mix and for 3840x2160 10-bit).
+`--section NAME` runs one of them alone; `--no-serving` skips the last two.
 """
 import argparse
 import concurrent.futures as cf

@@ -663,8 +663,9 @@ typedef struct av1g_config {
 } av1g_config;
 
 /* What a stream's sequence header fixes: the largest upscaled frame and the
- * sample format.  The engine reserves eight reference slots of that size in
- * its budget when the stream opens. */
+ * sample format.  When the stream opens, the engine reserves in its budget
+ * nine slot payloads of that size (the eight reference slots and the one a
+ * refresh writes before it replaces an older one). */
 typedef struct av1g_seq_info {
     int32_t max_width;
     int32_t max_height;

@@ -54,14 +54,20 @@ class Dispatcher:
 
 
 def required_slot_bytes(seq):
-    """The eight reference slots an engine reserves for a stream (the
-    admission unit): cropped planes of the largest frame, u8 or u16."""
+    """What an engine reserves for a stream when it opens (the admission
+    unit, av1g_stream_open): nine slot payloads of the largest frame — the
+    eight reference slots and the one a refresh writes before it replaces an
+    older one — each the cropped planes, u8 or u16, rows padded to 64 bytes
+    and planes to 256."""
     w, h = seq["max_width"], seq["max_height"]
     bps = 1 if seq["bit_depth"] == 8 else 2
-    luma = w * h
-    chroma = 0 if seq["num_planes"] == 1 else 2 * ((w + seq["subsampling_x"]) >> seq["subsampling_x"]) * \
-        ((h + seq["subsampling_y"]) >> seq["subsampling_y"])
-    return 8 * (luma + chroma) * bps
+    total = 0
+    for p in range(seq["num_planes"]):
+        sx = seq["subsampling_x"] if p else 0
+        sy = seq["subsampling_y"] if p else 0
+        pitch = (((w + sx) >> sx) * bps + 63) // 64 * 64
+        total += (pitch * ((h + sy) >> sy) + 255) // 256 * 256
+    return 9 * total
 
 
 __all__ = ["Dispatcher", "required_slot_bytes", "abi"]

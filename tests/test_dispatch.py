@@ -1,7 +1,7 @@
 """The multi-GPU stream dispatcher: placement by free HBM budget (CPU, fake engines).
 
 Each fake engine stands for one GPU's serving engine: a budget, the bytes its
-open streams reserve (eight reference slots each) and a refusal
+open streams reserve (nine slot payloads each, as av1g_stream_open) and a refusal
 (AV1G_ENOMEM_BUDGET -> None) when a stream does not fit, as the engine's own
 admission does.  The dispatcher must put each new stream on the engine with
 the most free budget, skip engines that refuse it, and return None when no
@@ -40,8 +40,13 @@ class FakeEngine:
 
 
 def test_slot_bytes():
-    assert required_slot_bytes(SEQ_1080) == 8 * (1920 * 1080 + 2 * 960 * 540)
-    assert required_slot_bytes(SEQ_4K10) == 8 * 2 * (3840 * 2160 + 2 * 1920 * 1080)
+    # nine payloads; rows padded to 64 bytes, planes to 256 (1920 = 30 x 64,
+    # 960 = 15 x 64; every plane here is a multiple of 256 bytes)
+    assert required_slot_bytes(SEQ_1080) == 9 * (1920 * 1080 + 2 * 960 * 540)
+    assert required_slot_bytes(SEQ_4K10) == 9 * 2 * (3840 * 2160 + 2 * 1920 * 1080)
+    odd = dict(SEQ_1080, max_width=130, max_height=70)
+    # luma 192 x 70 = 13440 -> 13568; chroma 128 x 35 = 4480 -> 4608 each
+    assert required_slot_bytes(odd) == 9 * (13568 + 2 * 4608)
 
 
 def test_streams_go_to_the_engine_with_most_free_budget():
