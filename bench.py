@@ -756,7 +756,17 @@ def _fetch_digest(lib, h, ticket):
     return st, tuple(dg), lat
 
 
-def drive(eng, templates, sbs, streams, clients=8, window=2):
+def _fetch_only(lib, h, ticket):
+    """(status, None, latency ms): the frame fetched (its planes are already
+    in host memory) and freed, without checking its samples."""
+    o = abi.FrameOut()
+    st = lib.av1g_fetch_output(h, ticket, C.byref(o))
+    lat = o.latency_ms
+    lib.av1g_release_output(h, ticket)
+    return st, None, lat
+
+
+def drive(eng, templates, sbs, streams, clients=8, window=2, check=True):
     """Decodes `streams` [(template index, frame count)] through the engine.
     `clients` threads each own a group of streams, as a server's connections
     would: a client submits frame k of each of its streams in turn, keeps at
@@ -780,7 +790,7 @@ def drive(eng, templates, sbs, streams, clients=8, window=2):
             nonlocal ok
             i, t = inflight.popleft()
             r = eng.poll(t, 300.0)
-            st, dg, lat = _fetch_digest(lib, hs[i].h, t)
+            st, dg, lat = (_fetch_digest if check else _fetch_only)(lib, hs[i].h, t)
             if r != abi.AV1G_OK or st != abi.AV1G_OK:
                 ok = False
                 failures.append((i, len(digests[i]), r, st))
@@ -978,8 +988,9 @@ def run_batching(args, local, mix):
            "template_generation_s": gen_s,
            "descriptor_bytes_per_frame": desc_bytes / frames,
            "timing": "host wall clock, first submit to last fetch; 8 client threads each owning a group of streams "
-                     "(at most 2 frames of a stream in flight), a CRC-32 per plane of every output frame taken by "
-                     "the clients",
+                     "(at most 2 frames of a stream in flight); a first run checks a CRC-32 per plane of every "
+                     "output frame against the streams decoded alone, two more fetch every frame unhashed and "
+                     "the faster is reported",
            **_host_info()}
     # warm-up: every stream for a few frames, so that the engine's pinned
     # pools and the device memory pool reach the run's working set first
@@ -989,17 +1000,22 @@ def run_batching(args, local, mix):
         eng = engine.Engine(device=local, max_batch=mb, lanes=args.serve_lanes)
         drive(eng, templates, sbs, warm)
         runs = []
-        for _ in range(2):  # the host is shared: two runs, the faster one reported
+        # run 1 checks every output frame (CRC-32 per plane on the client
+        # threads); runs 2 and 3 fetch every frame into host memory without
+        # hashing it, so that the check's host work does not compete with the
+        # engine's; the faster of those two is reported
+        for check in (True, False, False):
             s0 = eng.stats()
-            fps, dg, lats, ok = drive(eng, templates, sbs, streams)
+            fps, dg, lats, ok = drive(eng, templates, sbs, streams, check=check)
             s1 = eng.stats()
-            exact = all(d == ref[t][:len(d)] and len(d) == n for d, (t, n) in zip(dg, streams))
-            ok_all &= ok and exact
+            ok_all &= ok
+            if check:
+                ok_all &= all(d == ref[t][:len(d)] and len(d) == n for d, (t, n) in zip(dg, streams))
             runs.append({"value": fps, "unit": UNIT, "max_frames_per_step": mb, "lanes": args.serve_lanes,
                          "p50_ms": _pct(lats, 0.5), "p99_ms": _pct(lats, 0.99), **_engine_parts(s0, s1)})
         eng.close()
-        best = max(runs, key=lambda r: r["value"])
-        out[name] = dict(best, runs_value=[r["value"] for r in runs])
+        best = max(runs[1:], key=lambda r: r["value"])
+        out[name] = dict(best, checked_run_value=runs[0]["value"], runs_value=[r["value"] for r in runs[1:]])
     out["batched_over_per_frame"] = out["batched"]["value"] / out["per_frame"]["value"]
     out["bit_exact_alone_vs_mixed"] = bool(ok_all)
     return out
