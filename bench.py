@@ -987,7 +987,8 @@ def run_batching(args, local, mix):
                         f"cycles its template's inter frames",
            "template_generation_s": gen_s,
            "descriptor_bytes_per_frame": desc_bytes / frames,
-           "timing": "host wall clock, first submit to last fetch; 8 client threads each owning a group of streams "
+           "clients": args.batch_clients,
+           "timing": "host wall clock, first submit to last fetch; client threads each owning a group of streams "
                      "(at most 2 frames of a stream in flight); a first run checks a CRC-32 per plane of every "
                      "output frame against the streams decoded alone, two more fetch every frame unhashed and "
                      "the faster is reported",
@@ -998,7 +999,7 @@ def run_batching(args, local, mix):
     ok_all = True
     for name, mb in [("batched", 64), ("per_frame", 1)]:
         eng = engine.Engine(device=local, max_batch=mb, lanes=args.serve_lanes)
-        drive(eng, templates, sbs, warm)
+        drive(eng, templates, sbs, warm, clients=args.batch_clients)
         runs = []
         # run 1 checks every output frame (CRC-32 per plane on the client
         # threads); runs 2 and 3 fetch every frame into host memory without
@@ -1006,7 +1007,7 @@ def run_batching(args, local, mix):
         # engine's; the faster of those two is reported
         for check in (True, False, False):
             s0 = eng.stats()
-            fps, dg, lats, ok = drive(eng, templates, sbs, streams, check=check)
+            fps, dg, lats, ok = drive(eng, templates, sbs, streams, clients=args.batch_clients, check=check)
             s1 = eng.stats()
             ok_all &= ok
             if check:
@@ -1350,6 +1351,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--batch-streams", type=int, default=256)
+    ap.add_argument("--batch-clients", type=int, default=8)
     ap.add_argument("--serve-cap-streams", type=int, default=12)
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--serve-clients", type=int, default=32)
