@@ -542,8 +542,19 @@ def run_recon_stages(args, dev, stream):
                     "tus": len(fi.tus), "tus_per_us": len(fi.tus) / (ms * 1e3),
                     "bound": "latency: the TU dependency chain of the superblock wavefront",
                     "algorithmic_bytes": fi.coeffs.nbytes + 2 * area * S}
-    # the full-reconstruction configuration's key frame: 3840x2160 10-bit,
-    # 128x128 superblocks, 2 x 2 tiles (the tiles' wavefronts run side by side)
+    # the full-reconstruction configuration's shape: 3840x2160 10-bit 4:2:0,
+    # 128x128 superblocks — an inter frame's residual and prediction passes,
+    # and a key frame with 2 x 2 tiles (the tiles' wavefronts run side by side)
+    ru = synth.make_recon_frame(9011, 3840, 2160, bit_depth=10)
+    du = postfilter.DeviceRecon(ru, device=dev)
+    msu, hmsu = _device_ms(stream, lambda: postfilter.run_recon([du], stream=stream), reps=3)
+    out["residual_uhd"] = {"kernel": "recon_kernel", "frame": "3840x2160 10-bit 4:2:0", "ms_per_frame": msu,
+                           "host_ms_per_call": hmsu, "tus": len(ru.tus)}
+    iu = synth.make_inter_frame(9012, 3840, 2160, bit_depth=10, sb_size=128)
+    du = postfilter.DeviceInter(iu, device=dev)
+    msu, hmsu = _device_ms(stream, lambda: postfilter.run_inter([du], stream=stream), reps=3)
+    out["inter_uhd"] = {"kernel": "inter_kernel", "frame": "3840x2160 10-bit 4:2:0, 128x128 superblocks",
+                        "ms_per_frame": msu, "host_ms_per_call": hmsu, "calls": len(iu.preds)}
     fu = synth.make_intra_frame(9004, 3840, 2160, bit_depth=10, sb_size=128, tiles=(1, 1))
     du = postfilter.DeviceIntra(fu, device=dev)
     msu, _ = _device_ms(stream, lambda: postfilter.run_intra([du], stream=stream), reps=3)
