@@ -94,7 +94,6 @@ int slots_for(int tx) {
 // Host side of av1g_run_recon: validation, bucketing, upload, launch.
 av1g_status recon_run(const av1g_recon_job* jobs, int n, cudaStream_t s, std::string& err) {
     std::vector<ReconFrame> frames(n);
-    std::vector<TuDev> all;
     size_t total = 0;
     for (int i = 0; i < n; i++) total += jobs[i].num_tus > 0 ? jobs[i].num_tus : 0;
     // TUs bucketed by (size, type) so the threads of a warp run one butterfly
@@ -138,23 +137,17 @@ av1g_status recon_run(const av1g_recon_job* jobs, int n, cudaStream_t s, std::st
         }
     }
     if (total == 0) return AV1G_OK;
-    for (int k = 1; k <= kKeys; k++) count[k] += count[k - 1];
-    all.resize(total);
-    for (int i = 0; i < n; i++)
-        for (int k = 0; k < jobs[i].num_tus; k++) {
-            const av1g_tu& t = jobs[i].tus[k];
-            all[count[t.tx_size * 16 + t.tx_type]++] = TuDev{t, i};
-        }
+    for (int k = 1; k <= kKeys; k++) count[k] += count[k - 1];  // count[key]: TUs with a smaller key
+    // tasks: runs of at most slots_for(tx) TUs of one size; keys are
+    // size-major, so the TUs of size tx are [count[16 tx], count[16 tx + 16])
     std::vector<Task> tasks;
-    for (size_t k = 0; k < all.size();) {
-        int tx = all[k].tu.tx_size, cap = slots_for(tx);
-        size_t e = k;
-        while (e < all.size() && all[e].tu.tx_size == tx && (int)(e - k) < cap) e++;
-        tasks.push_back(Task{(int32_t)k, (int32_t)(e - k), tx, 0});
-        k = e;
+    for (int tx = 0; tx < 19; tx++) {
+        const int first = (int)count[tx * 16], len = (int)(count[tx * 16 + 16] - count[tx * 16]);
+        const int cap = slots_for(tx);
+        for (int k = 0; k < len; k += cap) tasks.push_back(Task{first + k, len - k < cap ? len - k : cap, tx, 0});
     }
     size_t off_tus = (sizeof(ReconFrame) * n + 255) & ~(size_t)255;
-    size_t off_tasks = (off_tus + sizeof(TuDev) * all.size() + 255) & ~(size_t)255;
+    size_t off_tasks = (off_tus + sizeof(TuDev) * total + 255) & ~(size_t)255;
     size_t bytes = off_tasks + sizeof(Task) * tasks.size();
     uint8_t* dev = nullptr;
     cudaError_t e = cudaMallocAsync((void**)&dev, bytes, s);
@@ -162,9 +155,16 @@ av1g_status recon_run(const av1g_recon_job* jobs, int n, cudaStream_t s, std::st
         err = std::string("cudaMallocAsync: ") + cudaGetErrorString(e);
         return AV1G_EDEVICE;
     }
+    // the TU records bucketed straight into the pinned staging block (a
+    // counting sort, stable in (job, decode order))
     e = upload_with(dev, bytes, s, [&](uint8_t* host) {
         memcpy(host, frames.data(), sizeof(ReconFrame) * n);
-        memcpy(host + off_tus, all.data(), sizeof(TuDev) * all.size());
+        TuDev* dst = reinterpret_cast<TuDev*>(host + off_tus);
+        for (int i = 0; i < n; i++)
+            for (int k = 0; k < jobs[i].num_tus; k++) {
+                const av1g_tu& t = jobs[i].tus[k];
+                dst[count[t.tx_size * 16 + t.tx_type]++] = TuDev{t, i};
+            }
         memcpy(host + off_tasks, tasks.data(), sizeof(Task) * tasks.size());
     });
     if (e == cudaSuccess) {
