@@ -644,6 +644,21 @@ def run_chain(args, dev, stream):
             "launches_per_step": 4}
 
 
+def run_e2e_section(args, dev, stream):
+    """The end-to-end leg alone, on the main line's frames and launch shapes:
+    pinned-host inputs and outputs copied every step around the chain, through
+    av1g_run_postfilter and through replays of captured chain graphs."""
+    from oxideav_av1_b200 import postfilter
+    lib = abi.load()
+    frames = make_frames(0, args.frames, args.bit_depth)
+    dframes = [postfilter.DeviceFrame(f, device=dev) for f in frames]
+    jobs = postfilter.jobs_array(dframes)
+    run_autotune(lib, jobs, len(dframes), stream, args.bit_depth > 8)
+    out = run_e2e(args, frames, dframes, jobs, stream, dev, 1, graphs=False)
+    out["graph_variant"] = run_e2e(args, frames, dframes, jobs, stream, dev, 1, graphs=True)
+    return out
+
+
 def run_motion_field(args, dev, stream, frames=16):
     """Row f2 on 1920x1080 frames (mi 270 x 480): §7.19 storage of `frames`
     decoded frames in one launch, then the §7.9 projection of `frames`
@@ -1281,6 +1296,7 @@ def run_e2e(args, frames, dframes, jobs, stream, dev, world, chunks=8, graphs=Tr
     ev_comp = [torch.cuda.Event() for _ in groups]   # group's kernels done (inputs free)
     ev_d2h = [torch.cuda.Event() for _ in groups]    # group's outputs copied out (outputs free)
     ev_in = [torch.cuda.Event() for _ in groups]
+    call_s = [0.0, 0]  # host seconds inside the library's entry point, calls
 
     def step():
         for gi in range(len(groups)):
@@ -1290,10 +1306,14 @@ def run_e2e(args, frames, dframes, jobs, stream, dev, world, chunks=8, graphs=Tr
                 ev_in[gi].record(s_in)
             stream.wait_event(ev_in[gi])
             stream.wait_event(ev_d2h[gi])
+            t0 = time.perf_counter()
             if graphs:
-                abi.check(lib.av1g_chain_graph_launch(ggraph[gi], sp))
+                rc = lib.av1g_chain_graph_launch(ggraph[gi], sp)
             else:
-                abi.check(lib.av1g_run_postfilter(gjobs[gi], len(groups[gi]), abi.MODE_BATCHED, sp, None))
+                rc = lib.av1g_run_postfilter(gjobs[gi], len(groups[gi]), abi.MODE_BATCHED, sp, None)
+            call_s[0] += time.perf_counter() - t0
+            call_s[1] += 1
+            abi.check(rc)
             ev_comp[gi].record(stream)
             with torch.cuda.stream(s_out):
                 s_out.wait_event(ev_comp[gi])
@@ -1306,12 +1326,20 @@ def run_e2e(args, frames, dframes, jobs, stream, dev, world, chunks=8, graphs=Tr
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     s_in.wait_event(e0)
+    call_s[0], call_s[1] = 0.0, 0
+    h0 = time.perf_counter()
     for _ in range(args.steps):
         step()
     stream.wait_stream(s_out)
     e1.record(stream)
+    host_ms = (time.perf_counter() - h0) * 1e3 / args.steps
     torch.cuda.synchronize()
     ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, dev)
+    host = {"enqueue_ms_per_step": host_ms, "entry_point_ms_per_call": call_s[0] * 1e3 / max(call_s[1], 1),
+            "calls_per_step": len(groups),
+            "note": "host wall time to enqueue one step (all groups' copies, chain calls and events) and the "
+                    "mean host time inside the library call; enqueue time near ms_per_step means the step is "
+                    "bound by the host, not the GPU"}
     for gh in ggraph:
         abi.check(lib.av1g_chain_graph_destroy(gh))
 
@@ -1344,7 +1372,7 @@ def run_e2e(args, frames, dframes, jobs, stream, dev, world, chunks=8, graphs=Tr
             "note": "the step's pinned copies alone (same buffers and streams, no kernels): h2d and d2h each "
                     "alone, then both at once; floor = the slowest of the three"}
     return {"value": job_rate(world, n, ms), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-            "ms_per_step": ms, "pcie": pcie,
+            "ms_per_step": ms, "pcie": pcie, "host": host,
             "path": f"{'av1g_chain_graph_launch (one captured chain per group)' if graphs else 'av1g_run_postfilter'}"
                     f" with pinned-host inputs/outputs copied every step, {len(groups)} groups of frames (one copy "
                     f"in and one copy out per group) pipelined over copy-in / compute / copy-out streams"}
@@ -1368,7 +1396,8 @@ def main():
     ap.add_argument("--serve-clients", type=int, default=32)
     ap.add_argument("--serve-lanes", type=int, default=8)
     ap.add_argument("--section", default="all",
-                    choices=["all", "recon", "extra", "motion_field", "chain", "decode", "batching", "serving"],
+                    choices=["all", "recon", "extra", "motion_field", "chain", "e2e", "decode", "batching",
+                             "serving"],
                     help="recon / extra: only that section (one GPU), printed as its own JSON object; "
                          "for profiling a row's kernels")
     args = ap.parse_args()
@@ -1386,7 +1415,8 @@ def main():
             print(json.dumps({args.section: fn(args, 0, mix_templates())}), flush=True)
             return 0
         stream = torch.cuda.Stream()
-        fn = {"chain": run_chain, "recon": run_recon_stages, "extra": run_extra_stages, "motion_field": run_motion_field}[args.section]
+        fn = {"chain": run_chain, "e2e": run_e2e_section, "recon": run_recon_stages, "extra": run_extra_stages,
+              "motion_field": run_motion_field}[args.section]
         print(json.dumps({args.section: fn(args, torch.device("cuda", 0), stream)}), flush=True)
         return 0
     return run_gpu(args)
