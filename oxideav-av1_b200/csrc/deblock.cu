@@ -31,7 +31,11 @@ __constant__ AV1T_TX_HEIGHT_TYPE c_txh AV1T_TX_HEIGHT_DIMS = AV1T_TX_HEIGHT_INIT
 
 namespace {
 
-constexpr int TILE = 64, HALO = 16, WIN = TILE + 2 * HALO, PITCH = WIN + 1, CELLS = WIN / 4;
+// window rows hold u16 samples at an odd number of 32-bit words per row
+// (49), so a warp walking down a column touches 32 distinct banks; a row
+// starts on a 4-byte (not always 8-byte) boundary, so the window is moved in
+// 32-bit words
+constexpr int TILE = 64, HALO = 16, WIN = TILE + 2 * HALO, PITCH = WIN + 2, CELLS = WIN / 4;
 constexpr int kDbThreads = 256;  // deblock_kernel's CTA size
 static_assert(WIN * (WIN / 4) % kDbThreads == 0, "window groups split evenly over the CTA");
 constexpr int BLOCK_SIZES = 22, BLOCK_INVALID = 22;
@@ -162,7 +166,7 @@ __device__ __forceinline__ int f4clamp(int v, int bd) { return clip3(-(1 << (bd 
 // i in [-n, n) from taps j in [-n, n] weighted 2 for |j| <= n2 else 1, source
 // positions clamped to [-(n + 1), n].  All indices are compile-time.
 template <int N, int LOG2, int N2>
-__device__ __forceinline__ void wide(int* b, int st) {
+__device__ __forceinline__ void wide(uint16_t* b, int st) {
     int v[2 * N + 2];
 #pragma unroll
     for (int k = 0; k < 2 * N + 2; k++) v[k] = b[(k - N - 1) * st];
@@ -178,12 +182,12 @@ __device__ __forceinline__ void wide(int* b, int st) {
         o[i + N] = (t + (1 << (LOG2 - 1))) >> LOG2;
     }
 #pragma unroll
-    for (int i = -N; i < N; i++) b[i * st] = o[i + N];
+    for (int i = -N; i < N; i++) b[i * st] = (uint16_t)o[i + N];
 }
 
 // sample_filtering + filter_mask + narrow/wide filters (loop_filter.rs:582-822)
 // on a line of shared-memory samples; b points at q0, st is the step.
-__device__ void filter_line(int* b, int st, uint32_t prm, int plane, int bd) {
+__device__ void filter_line(uint16_t* b, int st, uint32_t prm, int plane, int bd) {
     int fs = prm & 0xff;
     int limit = (prm >> 8) & 0xff, blimit = (prm >> 16) & 0xff, thresh = prm >> 24;
     int bds = bd - 8;
@@ -221,12 +225,12 @@ __device__ void filter_line(int* b, int st, uint32_t prm, int plane, int bd) {
         f = f4clamp(f + 3 * (qs0 - ps0), bd);
         int f1 = f4clamp(f + 4, bd) >> 3;
         int f2 = f4clamp(f + 3, bd) >> 3;
-        b[0] = f4clamp(qs0 - f1, bd) + half;
-        b[-st] = f4clamp(ps0 + f2, bd) + half;
+        b[0] = (uint16_t)(f4clamp(qs0 - f1, bd) + half);
+        b[-st] = (uint16_t)(f4clamp(ps0 + f2, bd) + half);
         if (!hev) {
             int ff = (f1 + 1) >> 1;
-            b[st] = f4clamp(qs1 - ff, bd) + half;
-            b[-2 * st] = f4clamp(ps1 + ff, bd) + half;
+            b[st] = (uint16_t)(f4clamp(qs1 - ff, bd) + half);
+            b[-2 * st] = (uint16_t)(f4clamp(ps1 + ff, bd) + half);
         }
         return;
     }
@@ -238,9 +242,9 @@ __device__ void filter_line(int* b, int st, uint32_t prm, int plane, int bd) {
     }
 }
 
-__global__ void __launch_bounds__(kDbThreads, 5) deblock_kernel(const FrameDev* __restrict__ frames,
+__global__ void __launch_bounds__(kDbThreads, 6) deblock_kernel(const FrameDev* __restrict__ frames,
                                                       const int32_t* __restrict__ starts, int n, int total) {
-    __shared__ int win[WIN * PITCH];
+    __shared__ __align__(16) uint16_t win[WIN * PITCH];
     __shared__ uint32_t ev[CELLS * CELLS], eh[CELLS * CELLS];
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
         int f = find_frame(starts, n, t);
@@ -277,8 +281,9 @@ __global__ void __launch_bounds__(kDbThreads, 5) deblock_kernel(const FrameDev* 
 #pragma unroll
                 for (int q = 0; q < PER; q++) {
                     const int i = threadIdx.x + q * kDbThreads, r = i / G, c = (i - r * G) * 4;
-                    int* w = &win[r * PITCH + c];
-                    w[0] = v[q].x & 0xffff; w[1] = v[q].x >> 16; w[2] = v[q].y & 0xffff; w[3] = v[q].y >> 16;
+                    uint32_t* w = reinterpret_cast<uint32_t*>(&win[r * PITCH + c]);  // 4-byte aligned
+                    w[0] = v[q].x;
+                    w[1] = v[q].y;
                 }
             } else {
                 uint32_t v[PER];
@@ -290,27 +295,31 @@ __global__ void __launch_bounds__(kDbThreads, 5) deblock_kernel(const FrameDev* 
 #pragma unroll
                 for (int q = 0; q < PER; q++) {
                     const int i = threadIdx.x + q * kDbThreads, r = i / G, c = (i - r * G) * 4;
-                    int* w = &win[r * PITCH + c];
-                    w[0] = v[q] & 0xff; w[1] = (v[q] >> 8) & 0xff; w[2] = (v[q] >> 16) & 0xff; w[3] = v[q] >> 24;
+                    uint32_t* w = reinterpret_cast<uint32_t*>(&win[r * PITCH + c]);  // 4-byte aligned
+                    w[0] = __byte_perm(v[q], 0u, 0x4140);
+                    w[1] = __byte_perm(v[q], 0u, 0x4342);
                 }
             }
         } else
         for (int i = threadIdx.x; i < WIN * (WIN / 4); i += blockDim.x) {
             int r = i / (WIN / 4), c = (i % (WIN / 4)) * 4;
             int gy = clip3(0, S.h - 1, gy0 + r), gx = gx0 + c;
-            int* w = &win[r * PITCH + c];
+            uint16_t* w = &win[r * PITCH + c];
             const uint8_t* row = S.p + (size_t)gy * S.stride;
             if (gx >= 0 && gx + 3 < S.w) {
+                uint32_t* w32 = reinterpret_cast<uint32_t*>(w);  // 4-byte aligned
                 if (hbd) {
-                    uint2 v = *reinterpret_cast<const uint2*>(row + 2 * gx);
-                    w[0] = v.x & 0xffff; w[1] = v.x >> 16; w[2] = v.y & 0xffff; w[3] = v.y >> 16;
+                    const uint2 v = *reinterpret_cast<const uint2*>(row + 2 * gx);
+                    w32[0] = v.x;
+                    w32[1] = v.y;
                 } else {
-                    uint32_t v = *reinterpret_cast<const uint32_t*>(row + gx);
-                    w[0] = v & 0xff; w[1] = (v >> 8) & 0xff; w[2] = (v >> 16) & 0xff; w[3] = v >> 24;
+                    const uint32_t v = *reinterpret_cast<const uint32_t*>(row + gx);
+                    w32[0] = __byte_perm(v, 0u, 0x4140);
+                    w32[1] = __byte_perm(v, 0u, 0x4342);
                 }
             } else {
 #pragma unroll
-                for (int k = 0; k < 4; k++) w[k] = ld_px(S, hbd, gy, clip3(0, S.w - 1, gx + k));
+                for (int k = 0; k < 4; k++) w[k] = (uint16_t)ld_px(S, hbd, gy, clip3(0, S.w - 1, gx + k));
             }
         }
         const int cy0 = gy0 / 4, cx0 = gx0 / 4;  // gx0,gy0 are multiples of 4 (may be negative)
@@ -360,15 +369,13 @@ __global__ void __launch_bounds__(kDbThreads, 5) deblock_kernel(const FrameDev* 
             int r = i / (TILE / 4), c = (i % (TILE / 4)) * 4;
             int gy = ty * TILE + r, gx = tx * TILE + c;
             if (gy >= dh) continue;
-            const int* w = &win[(r + HALO) * PITCH + c + HALO];
+            const uint16_t* w = &win[(r + HALO) * PITCH + c + HALO];
             uint8_t* row = D.p + (size_t)gy * D.stride;
             if (gx + 3 < dw) {
-                if (hbd)
-                    *reinterpret_cast<uint2*>(row + 2 * gx) =
-                        make_uint2((uint32_t)w[0] | ((uint32_t)w[1] << 16), (uint32_t)w[2] | ((uint32_t)w[3] << 16));
-                else
-                    *reinterpret_cast<uint32_t*>(row + gx) =
-                        (uint32_t)w[0] | ((uint32_t)w[1] << 8) | ((uint32_t)w[2] << 16) | ((uint32_t)w[3] << 24);
+                const uint32_t* w32 = reinterpret_cast<const uint32_t*>(w);  // 4-byte aligned
+                const uint2 v = make_uint2(w32[0], w32[1]);
+                if (hbd) *reinterpret_cast<uint2*>(row + 2 * gx) = v;
+                else *reinterpret_cast<uint32_t*>(row + gx) = __byte_perm(v.x, v.y, 0x6420);
             } else {
                 for (int k = 0; k < 4 && gx + k < dw; k++) st_px(D, hbd, gy, gx + k, w[k]);
             }
