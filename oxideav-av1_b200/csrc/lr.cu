@@ -84,7 +84,7 @@ __device__ __forceinline__ int count_units(int us, int sz) {
 // the rows and row sums slide along the columns, so each sum costs two loads
 // instead of 2R + 1; the runs have fixed lengths so the loops unroll and the
 // coefficient arithmetic of neighbouring positions overlaps.
-template <int R>
+template <int R, bool HBD>
 __device__ void box_coeffs(Smem& s, int th, int tw, int bd, int eps, int y0) {
     constexpr bool ODD = R == 2;
     constexpr int n = (2 * R + 1) * (2 * R + 1);
@@ -160,8 +160,9 @@ __device__ void box_coeffs(Smem& s, int th, int tw, int bd, int eps, int y0) {
 #pragma unroll
         for (int t = 0; t < CRUN; t++) {
             if (ja + t >= jb) break;
-            int ar = sa ? (a + (1 << (sa - 1))) >> sa : a;
-            int dr = sb ? (b + (1 << (sb - 1))) >> sb : b;
+            // 8-bit: both shifts are 0 (the branch is decided at compile time)
+            const int ar = HBD ? (a + (1 << (sa - 1))) >> sa : a;
+            const int dr = HBD ? (b + (1 << (sb - 1))) >> sb : b;
             int p = ar * n - dr * dr;
             if (p < 0) p = 0;
             const unsigned z = (min((unsigned)p, pcap) * sm + (1u << 19)) >> 20;
@@ -286,10 +287,21 @@ __global__ void __launch_bounds__(kLrThreads) lr_kernel(const FrameDev* __restri
             u = F.lr_units[plane][ur * F.lr_unit_cols[plane] + uc];
         __syncthreads();
         if (u.type != 1 && u.type != 2) {
-            for (int k = threadIdx.x; k < th * TW; k += blockDim.x) {
-                int i = k >> 6, j = k & (TW - 1);
-                if (j >= tw) continue;
-                st_px(O, hbd, y0 + i, x0 + j, ld_px(C, hbd, y0 + i, x0 + j));
+            // RESTORE_NONE: copied through, four samples per thread (x0 is a
+            // multiple of 32 and plane rows start on 16-byte boundaries, so
+            // each group of four is one aligned load and store)
+            for (int k = threadIdx.x; k < th * (TW / 4); k += blockDim.x) {
+                const int i = k >> 4, j0 = (k & 15) * 4;
+                if (j0 >= tw) continue;
+                const int y = y0 + i, x = x0 + j0;
+                if (j0 + 4 <= tw) {
+                    const uint8_t* src = C.p + (size_t)y * C.stride;
+                    uint8_t* dst = O.p + (size_t)y * O.stride;
+                    if (hbd) *reinterpret_cast<uint2*>(dst + 2 * x) = *reinterpret_cast<const uint2*>(src + 2 * x);
+                    else *reinterpret_cast<uint32_t*>(dst + x) = *reinterpret_cast<const uint32_t*>(src + x);
+                } else {
+                    for (int e = 0; e < 4 && j0 + e < tw; e++) st_px(O, hbd, y, x + e, ld_px(C, hbd, y, x + e));
+                }
             }
             continue;
         }
@@ -441,7 +453,8 @@ __global__ void __launch_bounds__(kLrThreads) lr_kernel(const FrameDev* __restri
         // outputs in runs of four along a row
         constexpr int Q = TW / 4;
         if (r0) {
-            box_coeffs<2>(s, th, tw, bd, e0, y0);  // r0 is 2 in every set that has it
+            if (bd > 8) box_coeffs<2, true>(s, th, tw, bd, e0, y0);  // r0 is 2 in every set that has it
+            else box_coeffs<2, false>(s, th, tw, bd, e0, y0);
             // rows of one parity run together (the odd-row and even-row
             // weightings differ), so a warp's two rows share a code path
             const int n_odd = (th + ((y0 & 1) ? 1 : 0)) >> 1;      // rows i with (y0 + i) odd
@@ -459,7 +472,10 @@ __global__ void __launch_bounds__(kLrThreads) lr_kernel(const FrameDev* __restri
             }
             __syncthreads();
         }
-        if (r1) box_coeffs<1>(s, th, tw, bd, e1, y0);  // r1 is 1 in every set that has it
+        if (r1) {  // r1 is 1 in every set that has it
+            if (bd > 8) box_coeffs<1, true>(s, th, tw, bd, e1, y0);
+            else box_coeffs<1, false>(s, th, tw, bd, e1, y0);
+        }
         for (int k = threadIdx.x; k < th * Q; k += blockDim.x) {
             int i = k / Q, j0 = (k - i * Q) * 4;
             if (j0 >= tw) continue;
