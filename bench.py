@@ -309,10 +309,11 @@ def run_gpu(args):
     ev_start = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ev_stage = [[torch.cuda.Event(enable_timing=True) for _ in stages] for _ in range(args.steps)]
     with torch.cuda.stream(stream):
-        # a ~20 ms spin ahead of the first event keeps the stream busy while
-        # the host enqueues the first steps, so a host pause there cannot open
-        # an idle gap inside the timed region (the spin itself is not timed)
-        torch.cuda._sleep(40_000_000)
+        # a ~100 ms spin ahead of the first event keeps the stream busy while
+        # the host enqueues the steps, so a host pause there cannot open an
+        # idle gap inside the timed region (the spin itself is not timed; a
+        # 20 ms spin was once outlasted by a ~45 ms host stall)
+        torch.cuda._sleep(200_000_000)
         for k in range(args.steps):
             ev_start[k].record(stream)
             step(ev_stage[k])
