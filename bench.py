@@ -806,7 +806,7 @@ def drive(eng, templates, sbs, streams, clients=8, window=2, check=True):
     hs = [eng.open_stream(synth.stream_seq(templates[t], sbs[t])) for t, _ in streams]
     assert all(h is not None for h in hs), "budget too small for the stream set"
     groups = [list(range(g, len(streams), clients)) for g in range(min(clients, len(streams)))]
-    failures = []  # (stream, frame, poll result, fetch status)
+    failures = []  # (stream, frame, poll result, fetch status, error text)
 
     def client(group):
         inflight = deque()
@@ -820,7 +820,7 @@ def drive(eng, templates, sbs, streams, clients=8, window=2, check=True):
             st, dg, lat = (_fetch_digest if check else _fetch_only)(lib, hs[i].h, t)
             if r != abi.AV1G_OK or st != abi.AV1G_OK:
                 ok = False
-                failures.append((i, len(digests[i]), r, st))
+                failures.append((i, len(digests[i]), r, st, lib.av1g_last_error().decode(errors="replace")))
             digests[i].append(dg)
             lats.append(lat)
 
@@ -858,9 +858,19 @@ def drive(eng, templates, sbs, streams, clients=8, window=2, check=True):
         lats += l
         ok &= o
     if failures:
-        sys.stderr.write(f"drive: {len(failures)} frames failed, first {failures[:4]}: "
-                         f"{lib.av1g_last_error().decode(errors='replace')}\n")
+        sys.stderr.write(f"drive: {len(failures)} frames failed, first {failures[:4]}\n")
+        FRAME_FAILURES.extend(failures)
     return sum(n for _, n in streams) / dt, [digests[i] for i in range(len(streams))], lats, ok
+
+
+# Frames the engine failed during the current section (drive appends; the
+# batching and serving sections report them in their results rather than
+# stopping the run).
+FRAME_FAILURES = []
+
+
+def _failures_summary():
+    return {"count": len(FRAME_FAILURES), "first": [list(f) for f in FRAME_FAILURES[:4]]}
 
 
 def _pct(xs, q):
@@ -886,7 +896,8 @@ def _alone_digests(local, templates, sbs, lengths):
     _, dg, _, ok = drive(solo, templates, sbs, [(t, lengths[t]) for t in range(len(templates))],
                          clients=len(templates))
     solo.close()
-    assert ok, "a template failed to decode alone"
+    # a frame that failed alone is in FRAME_FAILURES, and every stream frame
+    # compared with it counts as a mismatch
     return dg
 
 
@@ -1003,6 +1014,7 @@ def run_batching(args, local, mix):
     # stream i: shape by weight, bit depth and chroma format uniform, 8-60 frames
     streams = [(_draw_mix_template(rng), int(rng.integers(8, 61))) for _ in range(args.batch_streams)]
     lengths = [max([n for t_, n in streams if t_ == t] + [1]) for t in range(len(templates))]
+    FRAME_FAILURES.clear()
     ref = _alone_digests(local, templates, sbs, lengths)
     frames = sum(n for _, n in streams)
     desc_bytes = sum(_desc_bytes(stream_frame(templates[t], k)) for t, n in streams for k in range(n))
@@ -1046,6 +1058,7 @@ def run_batching(args, local, mix):
         out[name] = dict(best, checked_run_value=runs[0]["value"], runs_value=[r["value"] for r in runs[1:]])
     out["batched_over_per_frame"] = out["batched"]["value"] / out["per_frame"]["value"]
     out["bit_exact_alone_vs_mixed"] = bool(ok_all)
+    out["failed_frames"] = _failures_summary()
     return out
 
 
@@ -1070,6 +1083,7 @@ def _serve_variant(args, local, templates, sbs, draw, mean_len, label):
     import threading
     from oxideav_av1_b200 import engine
     rng = np.random.default_rng(17)
+    FRAME_FAILURES.clear()
     ref = _alone_digests(local, templates, sbs, [300] * len(templates))
     out = {"what": label, "budget_bytes": SERVE_BUDGET, "lanes": args.serve_lanes,
            "timing": "host wall clock; per-frame latency = the engine's submit-to-completion time", **_host_info()}
@@ -1180,6 +1194,7 @@ def _serve_variant(args, local, templates, sbs, draw, mean_len, label):
     ok_all &= ok
     out["poisson_per_frame_path"] = r
     out["bit_exact_alone_vs_mixed"] = bool(ok_all)
+    out["failed_frames"] = _failures_summary()  # the alone and capacity runs (Poisson runs count in bit_exact)
     return out
 
 

@@ -762,7 +762,9 @@ av1g_status av1g_submit_frame(av1g_stream* s, const av1g_frame_desc* d, uint64_t
  * *result = the frame's status once finished, AV1G_TIMEOUT (timeout > 0) or
  * AV1G_ENOTREADY (timeout 0) otherwise. */
 av1g_status av1g_poll(av1g_engine* e, uint64_t ticket, int64_t timeout_ns, av1g_status* result);
-/* The finished frame of a ticket (its status is returned). */
+/* The finished frame of a ticket (its status is returned).  When a frame
+ * failed, av1g_poll and av1g_fetch_output leave the reason in the calling
+ * thread's av1g_last_error(). */
 av1g_status av1g_fetch_output(av1g_stream* s, uint64_t ticket, av1g_frame_out* out);
 /* Frees a finished ticket and its output buffer. */
 av1g_status av1g_release_output(av1g_stream* s, uint64_t ticket);

@@ -20,11 +20,15 @@ namespace av1g {
 namespace {
 
 std::mutex g_mu;
+// What the autotuner picks on a 64 x 1080p batch on B200: grids several
+// times the resident CTAs (deblock 6, CDEF and LR 4 per SM), so the tiles'
+// uneven work evens out over many small CTAs instead of ending in a partial
+// last wave.
 StageShape g_shape[ST_COUNT][2] = {
-    {{6, 0}, {6, 0}},      // deblock
-    {{6, 0}, {6, 0}},      // CDEF
+    {{16, 0}, {16, 0}},    // deblock
+    {{16, 0}, {16, 0}},    // CDEF
     {{16, 512}, {16, 512}},  // superres
-    {{4, 0}, {4, 0}},      // loop restoration
+    {{8, 0}, {8, 0}},      // loop restoration
     {{8, 0}, {8, 0}},      // film grain blend
 };
 

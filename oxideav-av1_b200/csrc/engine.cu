@@ -46,6 +46,7 @@ av1g_status intra_run_status(const av1g_intra_job* jobs, int n, cudaStream_t s, 
 av1g_status inter_run(const av1g_inter_job* jobs, int n, cudaStream_t s, std::string& err);
 av1g_status postfilter_run(const av1g_frame_job* jobs, int n, cudaStream_t s, std::string& err);
 av1g_status postfilter_result_planes(const av1g_frame_job& j, PlaneDev pre[3], PlaneDev out[3], std::string& err);
+void set_last_error_text(const std::string& s);  // the C ABI's thread-local error text (api.cu)
 }  // namespace av1g
 
 using namespace av1g;
@@ -1079,6 +1080,7 @@ av1g_status av1g_poll(av1g_engine* E, uint64_t id, int64_t timeout_ns, av1g_stat
         E->cv_done.wait_for(lk, std::chrono::nanoseconds(timeout_ns), [&] { return t->done; });
     if (!t->done) return timeout_ns > 0 ? AV1G_TIMEOUT : AV1G_ENOTREADY;
     if (result) *result = t->status;
+    if (t->status != AV1G_OK) set_last_error_text(t->err);  // why the frame failed
     return AV1G_OK;
 }
 
@@ -1096,6 +1098,7 @@ av1g_status av1g_fetch_output(av1g_stream* S, uint64_t id, av1g_frame_out* o) {
     o->bit_depth = t.show_existing ? t.st->seq.bit_depth : t.hdr.bit_depth;
     for (int p = 0; p < 3; p++) o->planes[p] = t.out_planes[p];
     o->latency_ms = std::chrono::duration<double, std::milli>(t.t_done - t.t_submit).count();
+    if (t.status != AV1G_OK) set_last_error_text(t.err);
     return t.status;
 }
 

@@ -953,6 +953,27 @@ void plan_fault_wait(IntraPlan& plan, int f) {
         return;
     }
 }
+
+// The most dynamic shared memory any launch asks for: the fixed part, the TU
+// window and the largest superblock copy (128x128, three full planes, u16).
+constexpr size_t kMaxDynSmem = kSharedBytes + kTuWin * sizeof(av1g_intra_tu) + 3 * 128 * 128 * sizeof(uint16_t);
+static_assert(kMaxDynSmem <= 227 * 1024, "intra_kernel's shared memory exceeds an SM's");
+
+// The kernel's dynamic shared memory limit is a per-device attribute that
+// every launch on the device shares, and engine lanes launch concurrently
+// with different sizes: it is raised once per device to the largest size,
+// so no launch can find it lowered by another thread between its own
+// setting and its launch.
+cudaError_t ensure_intra_smem_limit(int dev) {
+    static std::mutex mu;
+    static bool done[256];
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev >= 0 && dev < 256 && done[dev]) return cudaSuccess;
+    const cudaError_t e =
+        cudaFuncSetAttribute(intra_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxDynSmem);
+    if (e == cudaSuccess && dev >= 0 && dev < 256) done[dev] = true;
+    return e;
+}
 }  // namespace
 
 // Host side of av1g_run_intra: the plan (intra_plan.cu), its upload, one
@@ -1033,7 +1054,8 @@ av1g_status intra_run_status(const av1g_intra_job* jobs, int n, cudaStream_t st,
         e = cudaGetLastError();
     }
     const size_t smem = kSharedBytes + kTuWin * sizeof(av1g_intra_tu) + plan.cache_bytes;
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(intra_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess && smem > kMaxDynSmem) e = cudaErrorInvalidValue;  // cannot happen: cache_bytes is bounded
+    if (e == cudaSuccess) e = ensure_intra_smem_limit(dev);
     int per_sm = 0;
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, intra_kernel, kT, smem);
     if (e == cudaSuccess) {

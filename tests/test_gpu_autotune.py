@@ -73,7 +73,7 @@ def test_forced_shapes_keep_parity(tmp_path, tile, ctas):
         _run_and_check([synth.make_frame(**c) for c in FRAMES])
     finally:  # back to the defaults for the tests that follow
         cache.write_text("".join(f"{st} {h} {c} {t}\n" for st, c, t in
-                                 [(0, 6, 0), (1, 6, 0), (2, 16, 512), (3, 4, 0), (4, 8, 0)] for h in range(2)))
+                                 [(0, 16, 0), (1, 16, 0), (2, 16, 512), (3, 8, 0), (4, 8, 0)] for h in range(2)))
         abi.check(lib.av1g_autotune_load(str(cache).encode()))
 
 

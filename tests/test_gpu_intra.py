@@ -89,3 +89,41 @@ def test_intra_rejects_palette_index_out_of_range():
     d = postfilter.DeviceIntra(f)
     with pytest.raises(abi.Av1gError):
         postfilter.run_intra([d])
+
+
+def test_concurrent_launches_with_different_shared_memory_sizes():
+    """Two host threads (as engine lanes do) run av1g_run_intra on their own
+    streams at the same time, one with 64x64 4:2:0 superblocks (a small
+    shared-memory copy) and one with 128x128 4:4:4 superblocks (the largest):
+    the kernel's shared-memory limit is a per-device attribute, so neither
+    thread's launches may fail because of the other's, and both frames come
+    out equal to the oracle."""
+    import ctypes as C
+    import threading
+
+    lib = abi.load()
+    fa = synth.make_intra_frame(seed=98, width=176, height=144)
+    fb = synth.make_intra_frame(seed=99, width=256, height=192, sb_size=128, ssx=0, ssy=0, bit_depth=10)
+    da, db = postfilter.DeviceIntra(fa), postfilter.DeviceIntra(fb)
+    torch.cuda.synchronize()
+    errors = []
+
+    def worker(d):
+        torch.cuda.set_device(0)
+        s = torch.cuda.Stream()
+        jobs = (abi.IntraJob * 1)(d.job())
+        for _ in range(40):  # a frame re-run from its inputs gives the same samples
+            rc = lib.av1g_run_intra(jobs, 1, C.c_void_p(s.cuda_stream))
+            if rc != abi.AV1G_OK:
+                errors.append((rc, lib.av1g_last_error()))
+                break
+        s.synchronize()
+
+    ts = [threading.Thread(target=worker, args=(d,)) for d in (da, db)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    assert not errors
+    _check(fa, da)
+    _check(fb, db)

@@ -77,7 +77,10 @@ def test_engine_fails_only_the_timed_out_frame(hook):
             assert st == abi.AV1G_OK
             for g, e in zip(planes, w):
                 assert np.array_equal(g.astype(np.int64), e)
-        for t in ta:
+        st, _, _ = sa.fetch(ta[0])
+        assert st == abi.AV1G_EDEVICE
+        assert b"dependency wait ran out of time" in lib.av1g_last_error()  # the failed frame's reason
+        for t in ta[1:]:
             sa.fetch(t)
         sa.close()
         sb.close()

@@ -122,6 +122,33 @@ def test_noalloc_draws_nothing_from_the_device_memory_pool():
     assert _pool_attr(8) > used
 
 
+def test_noalloc_rejects_a_batch_whose_scratch_exceeds_the_array():
+    """Sixteen 10240x10240 monochrome grain frames need about 139 KB of grain
+    scratch each (templates, LUTs and one offset byte per 32x32 block of each
+    stripe), 2.2 MB in all: more than the static array holds, so the call is
+    refused on the host before anything is enqueued.  The jobs point at real
+    planes of that size."""
+    lib = abi.load()
+    small = postfilter.DeviceFrame(synth.make_frame(seed=330, width=64, height=64, mono=True, **GRAIN_ONLY))
+    hdr = type(small.hdr).from_buffer_copy(small.hdr)
+    side = 10240
+    hdr.frame_width = hdr.upscaled_width = hdr.frame_height = side
+    hdr.mi_cols = hdr.mi_rows = 2 * ((side + 7) >> 3)
+    big_in = torch.zeros((side, side), dtype=torch.uint8, device="cuda")
+    big_out = torch.zeros((side, side), dtype=torch.uint8, device="cuda")
+    job = small.job()
+    job.hdr = C.pointer(hdr)
+    job.recon[0] = abi.Plane(big_in.data_ptr(), side, side, side)
+    job.out[0] = abi.Plane(big_out.data_ptr(), side, side, side)
+    n = abi.NOALLOC_MAX_FRAMES
+    jobs = (abi.FrameJob * n)(*([job] * n))
+    rc = lib.av1g_run_film_grain_noalloc(jobs, n, None)
+    assert rc == abi.AV1G_EINVAL
+    assert b"static array" in lib.av1g_last_error()
+    torch.cuda.synchronize()
+    assert int(big_out.count_nonzero()) == 0  # nothing ran
+
+
 def test_noalloc_rejects_batches_beyond_its_limit():
     lib = abi.load()
     frames = [postfilter.DeviceFrame(f) for f in _batch([dict(seed=310, width=64, height=64)])]
