@@ -27,7 +27,10 @@ reference's conformance streams through the stream decoder, digests checked),
 `batching` (256 mixed streams through the serving engine, batched against the
 per-frame path at equal lanes) and `serving` (Poisson arrivals of 30-300
 frame streams at three loads, for the batching mix and for 3840x2160 10-bit).
-`--section NAME` runs one of them alone; `--no-serving` skips the last two.
+`--section NAME` runs one of them alone (`recon`, `extra`, `motion_field`,
+`decode`, `batching`, `serving`, and also `chain`: the chain alone at the
+default launch shapes, and `e2e`: the end-to-end leg alone); `--no-serving`
+skips the last two of the line.
 """
 import argparse
 import concurrent.futures as cf
