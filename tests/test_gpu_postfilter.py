@@ -112,8 +112,10 @@ def test_chain_matches_oracle_chain(lib, case):
 
 
 def test_mixed_batch_equals_single(lib):
-    """One launch per stage over frames of mixed size / depth / format gives each frame's solo result."""
-    cases = [CASES[0], CASES[1], CASES[2], CASES[3], CASES[5], CASES[6], CASES[9]]
+    """One launch per stage over frames of mixed size / depth / format gives
+    each frame's solo result (8- and 10-bit frames take CDEF's half-precision
+    path and the 12-bit one its integer path, in the same launch)."""
+    cases = [CASES[0], CASES[1], CASES[2], CASES[3], CASES[5], CASES[6], CASES[7], CASES[9]]
     frames = [synth.make_frame(**c) for c in cases]
     batch = [postfilter.DeviceFrame(f) for f in frames]
     launches = postfilter.run_postfilter(batch, mode=abi.MODE_BATCHED)
