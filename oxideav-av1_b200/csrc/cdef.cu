@@ -30,10 +30,12 @@
 // round-to-nearest addition of 1536 to an exactly computed value whose
 // fraction cannot be a tie.  The maximum with zero that ends constrain turns
 // a NaN (unavailable) tap into a zero contribution and the clip range's min
-// / max skip NaNs, which is the reference's CdefAvailable == 0 arm.  Threads
-// of one warp take one 8x8 luma block (two adjacent samples each), so the
-// block's direction and strengths are warp-uniform.  12-bit frames keep the
-// 32-bit integer path (their sums pass 2048).
+// / max skip NaNs, which is the reference's CdefAvailable == 0 arm.  A warp
+// filters 64 consecutive samples of a row (8 luma blocks, each with its own
+// direction); in interior tiles a luma tap is one aligned 32-bit load from
+// the window or from a copy of it shifted by one sample (per-block byte
+// offsets), elsewhere two aligned words and a byte permute.  12-bit frames
+// keep the 32-bit integer path (their sums pass 2048).
 #include <cuda_fp16.h>
 
 #include "common.cuh"
@@ -230,21 +232,18 @@ __device__ __forceinline__ __half2 constrain_h(__half2 x, __half2 xv, const Half
     return u2h(h2u(__hmin2(ad, m)) | (h2u(d) & kSign2));
 }
 
-// The two samples at base + o, base + o + 1 (base even).  UNIFORM: o's
-// parity is the same in every lane of the warp (one branch); otherwise two
-// aligned words and a byte permute in every lane.
-template <bool UNIFORM>
+// The two samples at base + o, base + o + 1 (base even): two aligned words
+// and a byte permute (o's parity differs between lanes).
 __device__ __forceinline__ __half2 ld_pair(const uint16_t* base, int o) {
     const uint32_t* w = reinterpret_cast<const uint32_t*>(base + (o & ~1));
-    if (UNIFORM && !(o & 1)) return u2h(w[0]);
     return u2h(__byte_perm(w[0], w[1], (o & 1) ? 0x5432 : 0x3210));
 }
 
 // One tap pair (+o and -o) of weight w for two samples, with the clip range.
-template <bool BORDER, bool MINMAX, bool UNIFORM>
+template <bool BORDER, bool MINMAX>
 __device__ __forceinline__ void tap2_h(const uint16_t* cp, int o, __half2 xv, uint32_t w, const HalfStrength& S,
                                        __half2& sum, __half2& mn, __half2& mx) {
-    const __half2 x0 = ld_pair<UNIFORM>(cp, o), x1 = ld_pair<UNIFORM>(cp, -o);
+    const __half2 x0 = ld_pair(cp, o), x1 = ld_pair(cp, -o);
     sum = __hfma2(u2h(w), __hadd2(constrain_h<BORDER>(x0, xv, S), constrain_h<BORDER>(x1, xv, S)), sum);
     if (MINMAX) {
         mx = __hmax2(mx, __hmax2(x0, x1));
@@ -254,20 +253,20 @@ __device__ __forceinline__ void tap2_h(const uint16_t* cp, int o, __half2 xv, ui
 
 // cdef_filter (cdef.rs:465-590) of two adjacent samples; MODE as filter_px.
 // Returns the two filtered samples as half-precision bits 0x6400 | value.
-template <bool BORDER, int MODE, bool UNIFORM>
+template <bool BORDER, int MODE>
 __device__ __forceinline__ uint32_t filter_pair_h(const uint16_t* cp, __half2 xv, const Taps& T, const HalfStrength& P,
                                                   uint32_t pw0, uint32_t pw1, const HalfStrength& Sc) {
     constexpr bool MM = MODE == 3;
     __half2 sum = u2h(0u), mn = xv, mx = xv;
     if (MODE & 1) {
-        tap2_h<BORDER, MM, UNIFORM>(cp, T.p0, xv, pw0, P, sum, mn, mx);
-        tap2_h<BORDER, MM, UNIFORM>(cp, T.p1, xv, pw1, P, sum, mn, mx);
+        tap2_h<BORDER, MM>(cp, T.p0, xv, pw0, P, sum, mn, mx);
+        tap2_h<BORDER, MM>(cp, T.p1, xv, pw1, P, sum, mn, mx);
     }
     if (MODE & 2) {
-        tap2_h<BORDER, MM, UNIFORM>(cp, T.a0, xv, 0x40004000u, Sc, sum, mn, mx);  // weight 2
-        tap2_h<BORDER, MM, UNIFORM>(cp, T.b0, xv, 0x40004000u, Sc, sum, mn, mx);
-        tap2_h<BORDER, MM, UNIFORM>(cp, T.a1, xv, 0x3C003C00u, Sc, sum, mn, mx);  // weight 1
-        tap2_h<BORDER, MM, UNIFORM>(cp, T.b1, xv, 0x3C003C00u, Sc, sum, mn, mx);
+        tap2_h<BORDER, MM>(cp, T.a0, xv, 0x40004000u, Sc, sum, mn, mx);  // weight 2
+        tap2_h<BORDER, MM>(cp, T.b0, xv, 0x40004000u, Sc, sum, mn, mx);
+        tap2_h<BORDER, MM>(cp, T.a1, xv, 0x3C003C00u, Sc, sum, mn, mx);  // weight 1
+        tap2_h<BORDER, MM>(cp, T.b1, xv, 0x3C003C00u, Sc, sum, mn, mx);
     }
     // (8 + sum - (sum < 0)) >> 4: sum / 16 + copysign(1/32, sum) is exact and
     // never a half-integer; adding 1536 rounds it to the reference's offset
@@ -277,14 +276,14 @@ __device__ __forceinline__ uint32_t filter_pair_h(const uint16_t* cp, __half2 xv
     return h2u(y);
 }
 
-template <bool BORDER, bool UNIFORM>
+template <bool BORDER>
 __device__ __forceinline__ uint32_t filter_pair_modes(const uint16_t* cp, __half2 xv, const Taps& T, int mode,
                                                       const HalfStrength& P, uint32_t pw0, uint32_t pw1,
                                                       const HalfStrength& Sc) {
     switch (mode) {
-        case 3: return filter_pair_h<BORDER, 3, UNIFORM>(cp, xv, T, P, pw0, pw1, Sc);
-        case 1: return filter_pair_h<BORDER, 1, UNIFORM>(cp, xv, T, P, pw0, pw1, Sc);
-        case 2: return filter_pair_h<BORDER, 2, UNIFORM>(cp, xv, T, P, pw0, pw1, Sc);
+        case 3: return filter_pair_h<BORDER, 3>(cp, xv, T, P, pw0, pw1, Sc);
+        case 1: return filter_pair_h<BORDER, 1>(cp, xv, T, P, pw0, pw1, Sc);
+        case 2: return filter_pair_h<BORDER, 2>(cp, xv, T, P, pw0, pw1, Sc);
         default: return h2u(xv);
     }
 }
@@ -638,8 +637,8 @@ __global__ void __launch_bounds__(kCdefThreads, 4) cdef_kernel(const FrameDev* _
                             out = filter_pair_eo_modes(cp, xv, eo, mode, P, pw0, pw1, Sc);
                         } else {
                             const Taps T = taps_of(toff, p ? b.uvdir : b.ydir);
-                            out = border ? filter_pair_modes<true, false>(cp, xv, T, mode, P, pw0, pw1, Sc)
-                                         : filter_pair_modes<false, false>(cp, xv, T, mode, P, pw0, pw1, Sc);
+                            out = border ? filter_pair_modes<true>(cp, xv, T, mode, P, pw0, pw1, Sc)
+                                         : filter_pair_modes<false>(cp, xv, T, mode, P, pw0, pw1, Sc);
                         }
                     }
                     // out holds 0x6400 | value per lane
